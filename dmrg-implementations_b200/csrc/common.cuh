@@ -1,0 +1,87 @@
+// Shared scalar types, error handling and small device helpers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+
+namespace dmrg2 {
+
+typedef long long ll;
+
+struct __align__(16) zc {
+  double re, im;
+};
+
+__host__ __device__ inline zc mkz(double r, double i) { zc z; z.re = r; z.im = i; return z; }
+__host__ __device__ inline zc operator+(zc a, zc b) { return mkz(a.re + b.re, a.im + b.im); }
+__host__ __device__ inline zc operator-(zc a, zc b) { return mkz(a.re - b.re, a.im - b.im); }
+__host__ __device__ inline zc operator*(zc a, zc b) {
+  return mkz(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re);
+}
+__host__ __device__ inline zc operator*(double s, zc a) { return mkz(s * a.re, s * a.im); }
+
+// Scalar traits: real double or complex double (interleaved re, im).
+template <typename T> struct ST;
+template <> struct ST<double> {
+  static constexpr bool cplx = false;
+  __host__ __device__ static double zero() { return 0.0; }
+  __host__ __device__ static double one() { return 1.0; }
+  __host__ __device__ static double conj(double a) { return a; }
+  __host__ __device__ static double re(double a) { return a; }
+  __host__ __device__ static double im(double) { return 0.0; }
+  __host__ __device__ static double abs2(double a) { return a * a; }
+  __host__ __device__ static double make(double r, double) { return r; }
+  __host__ __device__ static double mul(double a, double b) { return a * b; }
+  __host__ __device__ static double add(double a, double b) { return a + b; }
+  __host__ __device__ static double scale(double s, double a) { return s * a; }
+  // conj(a) * b
+  __host__ __device__ static double cmul(double a, double b) { return a * b; }
+};
+template <> struct ST<zc> {
+  static constexpr bool cplx = true;
+  __host__ __device__ static zc zero() { return mkz(0, 0); }
+  __host__ __device__ static zc one() { return mkz(1, 0); }
+  __host__ __device__ static zc conj(zc a) { return mkz(a.re, -a.im); }
+  __host__ __device__ static double re(zc a) { return a.re; }
+  __host__ __device__ static double im(zc a) { return a.im; }
+  __host__ __device__ static double abs2(zc a) { return a.re * a.re + a.im * a.im; }
+  __host__ __device__ static zc make(double r, double i) { return mkz(r, i); }
+  __host__ __device__ static zc mul(zc a, zc b) { return a * b; }
+  __host__ __device__ static zc add(zc a, zc b) { return a + b; }
+  __host__ __device__ static zc scale(double s, zc a) { return mkz(s * a.re, s * a.im); }
+  __host__ __device__ static zc cmul(zc a, zc b) {
+    return mkz(a.re * b.re + a.im * b.im, a.re * b.im - a.im * b.re);
+  }
+};
+
+struct CudaError : public std::runtime_error {
+  explicit CudaError(const std::string& s) : std::runtime_error(s) {}
+};
+
+#define DMRG2_CUDA(call)                                                              \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess) {                                                          \
+      throw ::dmrg2::CudaError(std::string("CUDA error ") + cudaGetErrorString(e_) +  \
+                               " at " + __FILE__ + ":" + std::to_string(__LINE__) +   \
+                               " (" #call ")");                                       \
+    }                                                                                 \
+  } while (0)
+
+// Every kernel launch of the library goes through DMRG2_CHECK_LAUNCH, which
+// also counts it (reported through dmrg2_get_launch_count).
+long long& launch_counter();
+#define DMRG2_CHECK_LAUNCH()            \
+  do {                                  \
+    DMRG2_CUDA(cudaGetLastError());     \
+    ++::dmrg2::launch_counter();        \
+  } while (0)
+
+inline int ceil_div(ll a, ll b) { return (int)((a + b - 1) / b); }
+
+}  // namespace dmrg2

@@ -1,0 +1,188 @@
+#include "contract.cuh"
+
+namespace dmrg2 {
+
+template <typename T>
+void heff_apply(const T* Lenv, const T* Renv, const T* WWt, const T* in, T* out, T* X, T* Y, int cL,
+                int cR, int d, int Dl, int Dr, const int* skip, cudaStream_t s) {
+  const ll dd = (ll)d * d;
+  {
+    Gemm<T> g;
+    g.M = cL; g.N = (int)(dd * cR); g.K = cL;
+    g.A = Lenv; g.lda = (ll)Dl * cL; g.sA1 = cL;
+    g.B = in; g.ldb = dd * cR; g.sB1 = 0;
+    g.C = X; g.ldc = (ll)Dl * dd * cR; g.sC1 = dd * cR;
+    g.nb1 = Dl; g.skip = skip;
+    launch_gemm(g, s);
+  }
+  {
+    Gemm<T> g;
+    g.M = (int)(dd * Dr); g.N = cR; g.K = (int)(Dl * dd);
+    g.A = WWt; g.lda = Dl * dd; g.sA1 = 0;
+    g.B = X; g.ldb = cR; g.sB1 = (ll)Dl * dd * cR;
+    g.C = Y; g.ldc = cR; g.sC1 = dd * Dr * cR;
+    g.nb1 = cL; g.skip = skip;
+    launch_gemm(g, s);
+  }
+  {
+    Gemm<T> g;
+    g.tb = true;
+    g.M = (int)(cL * dd); g.N = cR; g.K = Dr * cR;
+    g.A = Y; g.lda = (ll)Dr * cR;
+    g.B = Renv; g.ldb = (ll)Dr * cR;
+    g.C = out; g.ldc = cR;
+    g.skip = skip;
+    launch_gemm(g, s);
+  }
+}
+
+double heff_flops(int cL, int cR, int d, int Dl, int Dr, bool cplx) {
+  double dd = (double)d * d;
+  double f = 2.0 * Dl * cL * (dd * cR) * cL + 2.0 * cL * (dd * Dr) * cR * (Dl * dd) +
+             2.0 * (cL * dd) * cR * ((double)Dr * cR);
+  return cplx ? 4.0 * f : f;
+}
+
+double env_flops(int ci, int co, int d, int Dl, int Dr, bool cplx) {
+  double f = 2.0 * ((double)ci * Dl) * ((double)d * co) * ci + 2.0 * ci * ((double)d * Dr) * co * (Dl * d) +
+             2.0 * co * ((double)Dr * co) * ((double)ci * d);
+  return cplx ? 4.0 * f : f;
+}
+
+template <typename T>
+void env_left(const T* Lenv, const T* A, const T* WmixL, T* Lnew, T* X, T* Y, int cL, int cO, int d,
+              int Dl, int Dr, cudaStream_t s) {
+  {
+    Gemm<T> g;
+    g.M = cL * Dl; g.N = d * cO; g.K = cL;
+    g.A = Lenv; g.lda = cL;
+    g.B = A; g.ldb = (ll)d * cO;
+    g.C = X; g.ldc = (ll)d * cO;
+    launch_gemm(g, s);
+  }
+  {
+    Gemm<T> g;
+    g.M = d * Dr; g.N = cO; g.K = Dl * d;
+    g.A = WmixL; g.lda = (ll)Dl * d; g.sA1 = 0;
+    g.B = X; g.ldb = cO; g.sB1 = (ll)Dl * d * cO;
+    g.C = Y; g.ldc = cO; g.sC1 = (ll)d * Dr * cO;
+    g.nb1 = cL;
+    launch_gemm(g, s);
+  }
+  {
+    Gemm<T> g;
+    g.ta = true; g.ca = true;
+    g.M = cO; g.N = Dr * cO; g.K = cL * d;
+    g.A = A; g.lda = cO;
+    g.B = Y; g.ldb = (ll)Dr * cO;
+    g.C = Lnew; g.ldc = (ll)Dr * cO;
+    launch_gemm(g, s);
+  }
+}
+
+template <typename T>
+void env_right(const T* Renv, const T* B, const T* WmixR, T* Rnew, T* X, T* Y, int cI, int cO,
+               int d, int Dl, int Dr, cudaStream_t s) {
+  {
+    Gemm<T> g;
+    g.tb = true;
+    g.M = cI * Dr; g.N = cO; g.K = cI;
+    g.A = Renv; g.lda = cI; g.sA1 = 0;
+    g.B = B; g.ldb = (ll)d * cI; g.sB1 = cI;
+    g.C = X; g.ldc = (ll)d * cO; g.sC1 = cO;
+    g.nb1 = d;
+    launch_gemm(g, s);
+  }
+  {
+    Gemm<T> g;
+    g.M = Dl; g.N = cO; g.K = Dr * d;
+    g.A = WmixR; g.lda = (ll)Dr * d; g.sA1 = 0; g.sA2 = (ll)Dl * Dr * d;
+    g.B = X; g.ldb = cO; g.sB1 = (ll)Dr * d * cO; g.sB2 = 0;
+    g.C = Y; g.ldc = cO; g.sC1 = (ll)Dl * cO; g.sC2 = (ll)cI * Dl * cO;
+    g.nb1 = cI; g.nb2 = d;
+    launch_gemm(g, s);
+  }
+  {
+    Gemm<T> g;
+    g.ca = true;
+    g.M = cO; g.N = Dl * cO; g.K = d * cI;
+    g.A = B; g.lda = (ll)d * cI;
+    g.B = Y; g.ldb = (ll)Dl * cO;
+    g.C = Rnew; g.ldc = (ll)Dl * cO;
+    launch_gemm(g, s);
+  }
+}
+
+template <typename T>
+void theta_form(const T* A, const T* B, T* theta, int cL, int cM, int cR, int d, cudaStream_t s) {
+  Gemm<T> g;
+  g.M = cL * d; g.N = d * cR; g.K = cM;
+  g.A = A; g.lda = cM;
+  g.B = B; g.ldb = (ll)d * cR;
+  g.C = theta; g.ldc = (ll)d * cR;
+  launch_gemm(g, s);
+}
+
+template <typename T>
+void build_wwt(const T* WL, const T* WR, int Dl, int Dm, int Dr, int d, std::vector<T>& out) {
+  // WWt[(p,q,n)][(w,s,r)] = sum_m WL[w][m][s][p] WR[m][n][r][q]
+  const int rows = d * d * Dr, cols = Dl * d * d;
+  out.assign((size_t)rows * cols, ST<T>::zero());
+  for (int p = 0; p < d; ++p)
+    for (int q = 0; q < d; ++q)
+      for (int n = 0; n < Dr; ++n)
+        for (int w = 0; w < Dl; ++w)
+          for (int s = 0; s < d; ++s)
+            for (int r = 0; r < d; ++r) {
+              T acc = ST<T>::zero();
+              for (int m = 0; m < Dm; ++m) {
+                T a = WL[(((size_t)w * Dm + m) * d + s) * d + p];
+                T b = WR[(((size_t)m * Dr + n) * d + r) * d + q];
+                acc = acc + ST<T>::mul(a, b);
+              }
+              size_t row = ((size_t)p * d + q) * Dr + n;
+              size_t col = ((size_t)w * d + s) * d + r;
+              out[row * cols + col] = acc;
+            }
+}
+
+template <typename T>
+void build_wmix_left(const T* W, int Dl, int Dr, int d, std::vector<T>& out) {
+  // WmixL[(t,w')][(w,s)] = W[w][w'][s][t]
+  const int rows = d * Dr, cols = Dl * d;
+  out.assign((size_t)rows * cols, ST<T>::zero());
+  for (int t = 0; t < d; ++t)
+    for (int wp = 0; wp < Dr; ++wp)
+      for (int w = 0; w < Dl; ++w)
+        for (int s = 0; s < d; ++s)
+          out[((size_t)t * Dr + wp) * cols + (size_t)w * d + s] = W[(((size_t)w * Dr + wp) * d + s) * d + t];
+}
+
+template <typename T>
+void build_wmix_right(const T* W, int Dl, int Dr, int d, std::vector<T>& out) {
+  // WmixR[t][w'][(w,s)] = W[w'][w][s][t]   (w' left index in Dl, w right index in Dr)
+  const int cols = Dr * d;
+  out.assign((size_t)d * Dl * cols, ST<T>::zero());
+  for (int t = 0; t < d; ++t)
+    for (int wp = 0; wp < Dl; ++wp)
+      for (int w = 0; w < Dr; ++w)
+        for (int s = 0; s < d; ++s)
+          out[((size_t)t * Dl + wp) * cols + (size_t)w * d + s] = W[(((size_t)wp * Dr + w) * d + s) * d + t];
+}
+
+#define INST(T)                                                                                 \
+  template void heff_apply<T>(const T*, const T*, const T*, const T*, T*, T*, T*, int, int, int, \
+                              int, int, const int*, cudaStream_t);                               \
+  template void env_left<T>(const T*, const T*, const T*, T*, T*, T*, int, int, int, int, int,  \
+                            cudaStream_t);                                                       \
+  template void env_right<T>(const T*, const T*, const T*, T*, T*, T*, int, int, int, int, int, \
+                             cudaStream_t);                                                      \
+  template void theta_form<T>(const T*, const T*, T*, int, int, int, int, cudaStream_t);         \
+  template void build_wwt<T>(const T*, const T*, int, int, int, int, std::vector<T>&);          \
+  template void build_wmix_left<T>(const T*, int, int, int, std::vector<T>&);                   \
+  template void build_wmix_right<T>(const T*, int, int, int, std::vector<T>&);
+INST(double)
+INST(zc)
+#undef INST
+
+}  // namespace dmrg2

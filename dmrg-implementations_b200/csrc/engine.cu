@@ -1,0 +1,479 @@
+// Two-site DMRG sweep engine.
+//
+// Mirrors the algorithm of the reference driver (gpu-rocm/dmrg2-gpu/src/dmrg2_gpu_impl.h):
+// build environments (941-964), then per sweep a left-to-right and a
+// right-to-left half sweep (1366-1413); each bond forms theta (583-600), finds
+// the ground state of H_eff with Lanczos (971-1160), splits it by a truncated
+// SVD (1167-1343) and updates one environment (787-934). The sweep energy is
+// the eigenvalue of the last bond optimised and the run stops at |dE| < tol
+// (1440-1447).
+//
+// Differences by design (all device-resident, no library calls):
+//  * any MPS can be loaded (set_mps); it is right-canonicalised on the device
+//    before the environments are built, so first-sweep energies are variational;
+//  * per-sweep chi schedule, cutoff, Krylov cap and restarts;
+//  * per-sweep energy, truncation error (discarded weight) and timings.
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <random>
+
+#include "contract.cuh"
+#include "engine.h"
+#include "lanczos_driver.cuh"
+
+namespace dmrg2 {
+
+namespace {
+ll ipow_cap(int d, int e, ll cap) {
+  ll v = 1;
+  for (int i = 0; i < e; ++i) {
+    v *= d;
+    if (v >= cap) return cap;
+  }
+  return v;
+}
+}  // namespace
+
+template <typename T>
+class Engine final : public EngineBase {
+ public:
+  explicit Engine(const EngineConfig& c) : cfg_(c) {
+    if (cfg_.L < 2) throw std::runtime_error("L must be >= 2");
+    if (cfg_.d < 1) throw std::runtime_error("d must be >= 1");
+    if (cfg_.chi_max < 1) throw std::runtime_error("chi_max must be >= 1");
+    if (cfg_.krylov_max < 2) cfg_.krylov_max = 2;
+    L_ = cfg_.L;
+    d_ = cfg_.d;
+    DMRG2_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+    cap_.resize(L_ + 1);
+    for (int i = 0; i <= L_; ++i) cap_[i] = (int)ipow_cap(d_, std::min(i, L_ - i), cfg_.chi_max);
+    dims_.assign(L_ + 1, 1);
+    mps_.assign(L_, nullptr);
+    for (int i = 0; i < L_; ++i) mps_[i] = dalloc((ll)cap_[i] * d_ * cap_[i + 1]);
+    nmax_ = 1;
+    for (int i = 0; i + 1 < L_; ++i) nmax_ = std::max(nmax_, (ll)cap_[i] * d_ * d_ * cap_[i + 2]);
+    qmax_ = 1;
+    for (int i = 0; i + 1 < L_; ++i) {
+      ll m = (ll)cap_[i] * d_, n = (ll)d_ * cap_[i + 2];
+      qmax_ = std::max(qmax_, std::max(m, n));
+    }
+    for (int i = 0; i < L_; ++i) qmax_ = std::max(qmax_, (ll)d_ * cap_[i + 1]);
+    theta_ = dalloc(nmax_);
+    svdX_ = dalloc(nmax_);
+    svdQ_ = dalloc(qmax_ * qmax_);
+    tmp_ = dalloc((ll)cfg_.chi_max * cfg_.chi_max);
+    lw_.init(cfg_.krylov_max, nmax_);
+    bytes_ += lw_.bytes(nmax_);
+    sigma_ = (double*)dalloc_bytes(sizeof(double) * qmax_);
+    perm_ = (int*)dalloc_bytes(sizeof(int) * qmax_);
+    svdout_ = (SvdOut*)dalloc_bytes(sizeof(SvdOut));
+    jctl_ = (JacobiCtl*)dalloc_bytes(sizeof(JacobiCtl));
+    dscal_ = (double*)dalloc_bytes(sizeof(double) * 16);
+    red_.nblk = vec_blocks(nmax_);
+    red_.part = (double*)dalloc_bytes(sizeof(double) * (size_t)red_.nblk * 2 * (KRYLOV_CAP + 2));
+    red_.counter = (unsigned*)dalloc_bytes(sizeof(unsigned) * 4);
+    DMRG2_CUDA(cudaMemset(red_.counter, 0, sizeof(unsigned) * 4));
+    DMRG2_CUDA(cudaMallocHost(&h_svd_, sizeof(SvdOut)));
+    DMRG2_CUDA(cudaEventCreate(&ev_c_));
+    DMRG2_CUDA(cudaEventCreate(&ev_d_));
+    DMRG2_CUDA(cudaEventCreate(&ev_s0_));
+    DMRG2_CUDA(cudaEventCreate(&ev_s1_));
+  }
+
+  ~Engine() override {
+    cudaStreamSynchronize(st_);
+    free_tmp();
+    free_mpo();
+    for (void* p : allocs_) cudaFree(p);
+    cudaFreeHost(h_svd_);
+    lw_.release();
+    cudaEventDestroy(ev_c_);
+    cudaEventDestroy(ev_d_);
+    cudaEventDestroy(ev_s0_);
+    cudaEventDestroy(ev_s1_);
+    cudaStreamDestroy(st_);
+  }
+
+  EngineConfig& config() override { return cfg_; }
+  double energy() const override { return energy_; }
+  double env_build_s() const override { return env_build_s_; }
+  const std::vector<int>& bond_dims() const override { return dims_; }
+  size_t device_bytes() const override { return bytes_ + bytes_mpo_; }
+
+  // --------------------------------------------------------------------------
+  void set_mpo(const std::vector<const void*>& W, const std::vector<int>& Dl,
+               const std::vector<int>& Dr) override {
+    if ((int)W.size() != L_ || (int)Dl.size() != L_ || (int)Dr.size() != L_)
+      throw std::runtime_error("set_mpo: expected L tensors and bond dims");
+    if (Dl[0] != 1 || Dr[L_ - 1] != 1)
+      throw std::runtime_error("set_mpo: boundary MPO bonds must be 1 (Dl[0] = Dr[L-1] = 1)");
+    for (int i = 0; i + 1 < L_; ++i)
+      if (Dr[i] != Dl[i + 1]) throw std::runtime_error("set_mpo: Dr[i] != Dl[i+1]");
+    for (int i = 0; i < L_; ++i)
+      if (Dl[i] < 1 || Dr[i] < 1 || Dl[i] > 4096 || Dr[i] > 4096)
+        throw std::runtime_error("set_mpo: bad MPO bond dimension");
+    DMRG2_CUDA(cudaStreamSynchronize(st_));
+    free_mpo();
+    Dl_ = Dl;
+    Dr_ = Dr;
+    Db_.assign(L_ + 1, 1);
+    for (int i = 0; i < L_; ++i) Db_[i] = Dl[i];
+    Db_[L_] = Dr[L_ - 1];
+    hW_.assign(L_, {});
+    for (int i = 0; i < L_; ++i) {
+      size_t n = (size_t)Dl[i] * Dr[i] * d_ * d_;
+      hW_[i].resize(n);
+      std::memcpy(hW_[i].data(), W[i], n * sizeof(T));
+    }
+    wml_.assign(L_, nullptr);
+    wmr_.assign(L_, nullptr);
+    wwt_.assign(L_ - 1, nullptr);
+    std::vector<T> tmp;
+    for (int i = 0; i < L_; ++i) {
+      build_wmix_left(hW_[i].data(), Dl[i], Dr[i], d_, tmp);
+      wml_[i] = upload(tmp);
+      build_wmix_right(hW_[i].data(), Dl[i], Dr[i], d_, tmp);
+      wmr_[i] = upload(tmp);
+    }
+    for (int i = 0; i + 1 < L_; ++i) {
+      build_wwt(hW_[i].data(), hW_[i + 1].data(), Dl[i], Dr[i], Dr[i + 1], d_, tmp);
+      wwt_[i] = upload(tmp);
+    }
+    lenv_.assign(L_ + 1, nullptr);
+    renv_.assign(L_ + 1, nullptr);
+    for (int i = 0; i <= L_; ++i) {
+      ll n = (ll)cap_[i] * cap_[i] * Db_[i];
+      lenv_[i] = dalloc_mpo(n);
+      renv_[i] = dalloc_mpo(n);
+    }
+    // contraction scratch
+    ll xs = 1;
+    const ll dd = (ll)d_ * d_;
+    for (int i = 0; i + 1 < L_; ++i) {
+      ll cL = cap_[i], cR = cap_[i + 2];
+      xs = std::max(xs, cL * Db_[i] * dd * cR);
+      xs = std::max(xs, cL * dd * Db_[i + 2] * cR);
+    }
+    for (int i = 0; i < L_; ++i) {
+      ll a = cap_[i], b = cap_[i + 1];
+      xs = std::max(xs, a * Dl[i] * d_ * b);
+      xs = std::max(xs, a * d_ * Dr[i] * b);
+      xs = std::max(xs, b * Dr[i] * d_ * a);
+      xs = std::max(xs, (ll)d_ * b * Dl[i] * a);
+    }
+    X_ = dalloc_mpo(xs);
+    Y_ = dalloc_mpo(xs);
+    mpo_set_ = true;
+    envs_valid_ = false;
+  }
+
+  void set_mps(const std::vector<const void*>& A, const std::vector<int>& dims) override {
+    if ((int)A.size() != L_ || (int)dims.size() != L_ + 1)
+      throw std::runtime_error("set_mps: expected L tensors and L+1 bond dims");
+    if (dims[0] != 1 || dims[L_] != 1) throw std::runtime_error("set_mps: boundary bonds must be 1");
+    for (int i = 0; i <= L_; ++i)
+      if (dims[i] < 1 || dims[i] > cap_[i])
+        throw std::runtime_error("set_mps: bond " + std::to_string(i) + " dimension " +
+                                 std::to_string(dims[i]) + " exceeds min(chi_max, d^min(i,L-i)) = " +
+                                 std::to_string(cap_[i]));
+    DMRG2_CUDA(cudaStreamSynchronize(st_));
+    dims_ = dims;
+    for (int i = 0; i < L_; ++i) {
+      size_t n = (size_t)dims[i] * d_ * dims[i + 1];
+      DMRG2_CUDA(cudaMemcpy(mps_[i], A[i], n * sizeof(T), cudaMemcpyHostToDevice));
+    }
+    mps_set_ = true;
+    canonical_ = false;
+    envs_valid_ = false;
+  }
+
+  void get_mps(std::vector<void*>& out) override {
+    DMRG2_CUDA(cudaStreamSynchronize(st_));
+    for (int i = 0; i < L_; ++i) {
+      size_t n = (size_t)dims_[i] * d_ * dims_[i + 1];
+      DMRG2_CUDA(cudaMemcpy(out[i], mps_[i], n * sizeof(T), cudaMemcpyDeviceToHost));
+    }
+  }
+
+  // --------------------------------------------------------------------------
+  std::vector<SweepStats> run(const std::vector<int>& schedule) override {
+    if (!mpo_set_) throw std::runtime_error("run: MPO not set");
+    if (!mps_set_) throw std::runtime_error("run: MPS not set");
+    for (int c : schedule)
+      if (c < 1 || c > cfg_.chi_max) throw std::runtime_error("run: schedule chi outside [1, chi_max]");
+    auto t0 = std::chrono::steady_clock::now();
+    right_canonicalize();
+    build_right_envs();
+    DMRG2_CUDA(cudaStreamSynchronize(st_));
+    env_build_s_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+
+    envs_valid_ = true;
+    return sweeps(schedule, true);
+  }
+
+  std::vector<SweepStats> resume(const std::vector<int>& schedule) override {
+    if (!envs_valid_) throw std::logic_error("resume: no previous run on this MPS/MPO");
+    for (int c : schedule)
+      if (c < 1 || c > cfg_.chi_max) throw std::runtime_error("resume: schedule chi outside [1, chi_max]");
+    return sweeps(schedule, false);
+  }
+
+  std::vector<SweepStats> sweeps(const std::vector<int>& schedule, bool stop_rule) {
+    std::vector<SweepStats> out;
+    double e_prev = energy_;
+    for (size_t sw = 0; sw < schedule.size(); ++sw) {
+      SweepStats ss;
+      ss.sweep = (int)sw;
+      ss.chi_max = schedule[sw];
+      auto ts = std::chrono::steady_clock::now();
+      DMRG2_CUDA(cudaEventRecord(ev_s0_, st_));
+      double e = 0.0;
+      for (int i = 0; i + 1 < L_; ++i) e = optimize_bond(i, 'R', schedule[sw], ss);
+      for (int i = L_ - 2; i >= 0; --i) e = optimize_bond(i, 'L', schedule[sw], ss);
+      DMRG2_CUDA(cudaEventRecord(ev_s1_, st_));
+      DMRG2_CUDA(cudaStreamSynchronize(st_));
+      float ms = 0.f;
+      DMRG2_CUDA(cudaEventElapsedTime(&ms, ev_s0_, ev_s1_));
+      ss.device_s = ms * 1e-3;
+      ss.wall_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - ts).count();
+      ss.energy = e;
+      ss.max_bond = *std::max_element(dims_.begin(), dims_.end());
+      energy_ = e;
+      out.push_back(ss);
+      if (stop_rule && (int)sw + 1 >= cfg_.min_sweeps && std::fabs(e - e_prev) < cfg_.tol) break;
+      e_prev = e;
+    }
+    canonical_ = true;
+    return out;
+  }
+
+  // <O_i> for all sites; valid on a right-canonical MPS with its norm on site 0
+  void expect_local(const void* op, std::vector<double>& re, std::vector<double>& im) override {
+    if (!mps_set_) throw std::runtime_error("expect_local: MPS not set");
+    if (!mpo_set_) throw std::runtime_error("expect_local: MPO not set (scratch buffers)");
+    if (!canonical_) right_canonicalize();
+    const ll cm = cfg_.chi_max;
+    T* E = dalloc_tmp(cm * cm);
+    T* E2 = dalloc_tmp(cm * cm);
+    T* F = dalloc_tmp(cm * cm);
+    T* opd = dalloc_tmp((ll)d_ * d_);
+    T* idd = dalloc_tmp((ll)d_ * d_);
+    double* res = (double*)dalloc_tmp_bytes(sizeof(double) * 2 * (L_ + 1));
+    std::vector<T> hid((size_t)d_ * d_, ST<T>::zero());
+    for (int i = 0; i < d_; ++i) hid[(size_t)i * d_ + i] = ST<T>::one();
+    DMRG2_CUDA(cudaMemcpyAsync(opd, op, sizeof(T) * d_ * d_, cudaMemcpyHostToDevice, st_));
+    DMRG2_CUDA(cudaMemcpyAsync(idd, hid.data(), sizeof(T) * d_ * d_, cudaMemcpyHostToDevice, st_));
+    T one = ST<T>::one();
+    DMRG2_CUDA(cudaMemcpyAsync(E, &one, sizeof(T), cudaMemcpyHostToDevice, st_));
+    for (int i = 0; i < L_; ++i) {
+      int a = dims_[i], b = dims_[i + 1];
+      env_left(E, mps_[i], opd, F, X_, Y_, a, b, d_, 1, 1, st_);
+      trace_real(F, b, b, res + 2 * i, res + 2 * i + 1, st_);
+      env_left(E, mps_[i], idd, E2, X_, Y_, a, b, d_, 1, 1, st_);
+      if (i == 0) trace_real(E2, b, b, res + 2 * L_, res + 2 * L_ + 1, st_);
+      std::swap(E, E2);
+    }
+    std::vector<double> h(2 * (L_ + 1));
+    DMRG2_CUDA(cudaMemcpyAsync(h.data(), res, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st_));
+    DMRG2_CUDA(cudaStreamSynchronize(st_));
+    free_tmp();
+    double nrm = h[2 * L_];
+    re.resize(L_);
+    im.resize(L_);
+    for (int i = 0; i < L_; ++i) {
+      re[i] = h[2 * i] / nrm;
+      im[i] = h[2 * i + 1] / nrm;
+    }
+  }
+
+ private:
+  // ---------------------------------------------------------------- memory
+  T* dalloc(ll n) { return (T*)dalloc_bytes(sizeof(T) * (size_t)std::max<ll>(n, 1)); }
+  void* dalloc_bytes(size_t b) {
+    void* p = nullptr;
+    DMRG2_CUDA(cudaMalloc(&p, b));
+    allocs_.push_back(p);
+    bytes_ += b;
+    return p;
+  }
+  T* dalloc_mpo(ll n) {
+    void* p = nullptr;
+    size_t b = sizeof(T) * (size_t)std::max<ll>(n, 1);
+    DMRG2_CUDA(cudaMalloc(&p, b));
+    mpo_allocs_.push_back(p);
+    bytes_mpo_ += b;
+    return (T*)p;
+  }
+  T* dalloc_tmp(ll n) { return (T*)dalloc_tmp_bytes(sizeof(T) * (size_t)std::max<ll>(n, 1)); }
+  void* dalloc_tmp_bytes(size_t b) {
+    void* p = nullptr;
+    DMRG2_CUDA(cudaMalloc(&p, b));
+    tmp_allocs_.push_back(p);
+    return p;
+  }
+  void free_tmp() {
+    for (void* p : tmp_allocs_) cudaFree(p);
+    tmp_allocs_.clear();
+  }
+  void free_mpo() {
+    for (void* p : mpo_allocs_) cudaFree(p);
+    mpo_allocs_.clear();
+    bytes_mpo_ = 0;
+  }
+  T* upload(const std::vector<T>& h) {
+    T* p = dalloc_mpo((ll)h.size());
+    DMRG2_CUDA(cudaMemcpy(p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+    return p;
+  }
+
+  // rotation threshold on |<x_p,x_q>| / (|x_p||x_q|): len * eps, as LAPACK's
+  // one-sided Jacobi (dgesvj) uses; below that the computed inner products are noise
+  double jacobi_tol(ll len) const { return 2.2e-16 * std::max<double>(16.0, (double)len); }
+
+  // ---------------------------------------------------------------- setup
+  void right_canonicalize() {
+    envs_valid_ = false;
+    for (int i = L_ - 1; i >= 1; --i) {
+      const int cl = dims_[i], cr = dims_[i + 1];
+      const ll nc = (ll)d_ * cr;
+      transpose(mps_[i], svdX_, cl, nc, st_);
+      norm2(svdX_, (ll)cl * nc, dscal_, red_, st_);
+      set_identity(svdQ_, (int)nc, st_);
+      svd_jacobi(svdX_, svdQ_, (int)nc, (ll)cl, jctl_, cfg_.jacobi_max_sweeps, jacobi_tol(cl), dscal_,
+                 st_);
+      svd_sort_truncate(svdX_, (int)nc, (ll)cl, sigma_, perm_, svdout_,
+                        std::min(cfg_.chi_max, cap_[i]), 1e-14, true, jctl_, st_);
+      int k = read_svd().k;
+      svd_gather(svdX_, svdQ_, perm_, (int)nc, (ll)cl, k, 1, tmp_, mps_[i], st_);
+      scale_inplace(tmp_, (ll)cl * k, &svdout_->sigma_max2, st_);
+      {  // A[i-1] <- A[i-1] . (U S / sigma_max)
+        Gemm<T> g;
+        g.M = dims_[i - 1] * d_; g.N = k; g.K = cl;
+        g.A = mps_[i - 1]; g.lda = cl;
+        g.B = tmp_; g.ldb = k;
+        g.C = theta_; g.ldc = k;
+        launch_gemm(g, st_);
+      }
+      DMRG2_CUDA(cudaMemcpyAsync(mps_[i - 1], theta_, sizeof(T) * (size_t)dims_[i - 1] * d_ * k,
+                                 cudaMemcpyDeviceToDevice, st_));
+      dims_[i] = k;
+    }
+    const ll n0 = (ll)d_ * dims_[1];
+    norm2(mps_[0], n0, dscal_, red_, st_);
+    scale_inplace(mps_[0], n0, dscal_, st_);
+    canonical_ = true;
+  }
+
+  void build_right_envs() {
+    T one = ST<T>::one();
+    DMRG2_CUDA(cudaMemcpyAsync(lenv_[0], &one, sizeof(T), cudaMemcpyHostToDevice, st_));
+    DMRG2_CUDA(cudaMemcpyAsync(renv_[L_], &one, sizeof(T), cudaMemcpyHostToDevice, st_));
+    for (int i = L_ - 1; i >= 2; --i)
+      env_right(renv_[i + 1], mps_[i], wmr_[i], renv_[i], X_, Y_, dims_[i + 1], dims_[i], d_, Dl_[i],
+                Dr_[i], st_);
+  }
+
+  SvdOut read_svd() {
+    DMRG2_CUDA(cudaMemcpyAsync(h_svd_, svdout_, sizeof(SvdOut), cudaMemcpyDeviceToHost, st_));
+    DMRG2_CUDA(cudaStreamSynchronize(st_));
+    if (h_svd_->jacobi_err) throw std::runtime_error("Jacobi SVD barrier timed out");
+    return *h_svd_;
+  }
+
+  // ---------------------------------------------------------------- sweep
+  double optimize_bond(int i, char dir, int chi, SweepStats& ss) {
+    const int cL = dims_[i], cM = dims_[i + 1], cR = dims_[i + 2];
+    const ll n = (ll)cL * d_ * d_ * cR;
+    theta_form(mps_[i], mps_[i + 1], theta_, cL, cM, cR, d_, st_);
+    double e = lanczos(i, n, ss);
+    svd_split(i, dir, chi, ss);
+    if (dir == 'R')
+      env_left(lenv_[i], mps_[i], wml_[i], lenv_[i + 1], X_, Y_, dims_[i], dims_[i + 1], d_, Dl_[i],
+               Dr_[i], st_);
+    else
+      env_right(renv_[i + 2], mps_[i + 1], wmr_[i + 1], renv_[i + 1], X_, Y_, dims_[i + 2],
+                dims_[i + 1], d_, Dl_[i + 1], Dr_[i + 1], st_);
+    return e;
+  }
+
+  double lanczos(int i, ll n, SweepStats& ss) {
+    const int cL = dims_[i], cR = dims_[i + 2];
+    const int Dl = Db_[i], Dr = Db_[i + 2];
+    const double fl = heff_flops(cL, cR, d_, Dl, Dr, ST<T>::cplx);
+    auto mv = [&](const T* in, T* out, const int* skip) {
+      heff_apply(lenv_[i], renv_[i + 2], wwt_[i], in, out, X_, Y_, cL, cR, d_, Dl, Dr, skip, st_);
+    };
+    LanczosResult r = lanczos_solve<T>(lw_, theta_, n, cfg_.krylov_max, cfg_.lanczos_tol,
+                                       cfg_.max_restarts, cfg_.seed + 7919u * (unsigned)i, mv, st_);
+    ss.heff_s += r.matvec_s;
+    ss.matvecs += r.matvecs;
+    ss.heff_flops += fl * r.matvecs;
+    ss.lanczos_iters += r.iters;
+    if (!r.converged) ss.lanczos_unconverged += 1;
+    return r.energy;
+  }
+
+  void svd_split(int i, char dir, int chi, SweepStats& ss) {
+    const int cL = dims_[i], cR = dims_[i + 2];
+    const ll m = (ll)cL * d_, nc = (ll)d_ * cR;
+    int nvec;
+    ll len;
+    DMRG2_CUDA(cudaEventRecord(ev_c_, st_));
+    if (dir == 'R') {
+      nvec = (int)m;
+      len = nc;
+      DMRG2_CUDA(cudaMemcpyAsync(svdX_, theta_, sizeof(T) * m * nc, cudaMemcpyDeviceToDevice, st_));
+    } else {
+      nvec = (int)nc;
+      len = m;
+      transpose(theta_, svdX_, m, nc, st_);
+    }
+    set_identity(svdQ_, nvec, st_);
+    svd_jacobi(svdX_, svdQ_, nvec, len, jctl_, cfg_.jacobi_max_sweeps, jacobi_tol(len), nullptr, st_);
+    svd_sort_truncate(svdX_, nvec, len, sigma_, perm_, svdout_, chi, cfg_.cutoff, false, jctl_, st_);
+    DMRG2_CUDA(cudaEventRecord(ev_d_, st_));
+    SvdOut o = read_svd();
+    float ms = 0.f;
+    DMRG2_CUDA(cudaEventElapsedTime(&ms, ev_c_, ev_d_));
+    ss.svd_s += ms * 1e-3;
+    ss.jacobi_sweeps_max = std::max(ss.jacobi_sweeps_max, o.jacobi_sweeps);
+    const int k = o.k;
+    svd_gather(svdX_, svdQ_, perm_, nvec, len, k, dir == 'R' ? 0 : 1, mps_[i], mps_[i + 1], st_);
+    dims_[i + 1] = k;
+    ss.trunc_err_max = std::max(ss.trunc_err_max, o.trunc_err);
+    ss.trunc_err_sum += o.trunc_err;
+  }
+
+  // ---------------------------------------------------------------- state
+  EngineConfig cfg_;
+  int L_ = 0, d_ = 0;
+  cudaStream_t st_ = nullptr;
+  std::vector<int> cap_, dims_, Dl_, Dr_, Db_;
+  std::vector<std::vector<T>> hW_;
+  std::vector<T*> mps_, lenv_, renv_, wwt_, wml_, wmr_;
+  T *theta_ = nullptr, *X_ = nullptr, *Y_ = nullptr, *svdX_ = nullptr,
+    *svdQ_ = nullptr, *tmp_ = nullptr;
+  LanczosWork<T> lw_;
+  double* sigma_ = nullptr;
+  int* perm_ = nullptr;
+  SvdOut* svdout_ = nullptr;
+  JacobiCtl* jctl_ = nullptr;
+  double* dscal_ = nullptr;
+  RedScratch red_;
+  SvdOut* h_svd_ = nullptr;
+  cudaEvent_t ev_c_ = nullptr, ev_d_ = nullptr, ev_s0_ = nullptr, ev_s1_ = nullptr;
+  bool envs_valid_ = false;
+  std::vector<void*> allocs_, mpo_allocs_, tmp_allocs_;
+  size_t bytes_ = 0, bytes_mpo_ = 0;
+  ll nmax_ = 0, qmax_ = 0;
+  bool mpo_set_ = false, mps_set_ = false, canonical_ = false;
+  double energy_ = 0.0, env_build_s_ = 0.0;
+};
+
+std::unique_ptr<EngineBase> make_engine(const EngineConfig& cfg) {
+  if (cfg.complex) return std::unique_ptr<EngineBase>(new Engine<zc>(cfg));
+  return std::unique_ptr<EngineBase>(new Engine<double>(cfg));
+}
+
+}  // namespace dmrg2

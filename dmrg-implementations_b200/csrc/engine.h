@@ -1,0 +1,69 @@
+// Two-site DMRG engine (host orchestration of the device kernels).
+//
+// B200-native counterpart of the reference's DMRG2GPU<Scalar> class
+// (gpu-rocm/dmrg2-gpu/src/dmrg2_gpu.h:24-203, dmrg2_gpu_impl.h).
+#pragma once
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace dmrg2 {
+
+struct EngineConfig {
+  int L = 0;
+  int d = 2;
+  int chi_max = 32;
+  bool complex = false;
+  double tol = 1e-10;          // sweep stop rule |dE| < tol (dmrg2_gpu.h:30)
+  int krylov_max = 100;        // Lanczos vectors per pass (dmrg2_gpu_impl.h:138: min(100, n))
+  double lanczos_tol = 1e-12;  // |dE| between Lanczos steps (dmrg2_gpu_impl.h:976)
+  int max_restarts = 0;        // explicit restarts from the Ritz vector
+  double cutoff = 1e-14;       // absolute singular-value cutoff (dmrg2_gpu_impl.h:1276)
+  int min_sweeps = 2;          // the stop rule applies from the second sweep on
+  int jacobi_max_sweeps = 40;
+  unsigned seed = 42;
+};
+
+struct SweepStats {
+  int sweep = 0;
+  int chi_max = 0;
+  double energy = 0.0;
+  double trunc_err_max = 0.0;
+  double trunc_err_sum = 0.0;
+  int max_bond = 0;
+  double wall_s = 0.0;
+  long long matvecs = 0;
+  double heff_s = 0.0;       // device time inside the H_eff contractions
+  double heff_flops = 0.0;   // algorithmic flops of those contractions
+  long long lanczos_iters = 0;
+  int lanczos_unconverged = 0;
+  double svd_s = 0.0;
+  int jacobi_sweeps_max = 0;
+  double device_s = 0.0;     // device time of the whole sweep (CUDA events on the engine stream)
+};
+
+class EngineBase {
+ public:
+  virtual ~EngineBase() = default;
+  virtual void set_mpo(const std::vector<const void*>& W, const std::vector<int>& Dl,
+                       const std::vector<int>& Dr) = 0;
+  virtual void set_mps(const std::vector<const void*>& A, const std::vector<int>& dims) = 0;
+  virtual std::vector<SweepStats> run(const std::vector<int>& schedule) = 0;
+  // continue sweeping from the current state (environments kept from the last run)
+  virtual std::vector<SweepStats> resume(const std::vector<int>& schedule) = 0;
+  virtual void get_mps(std::vector<void*>& out) = 0;
+  virtual void expect_local(const void* op, std::vector<double>& re, std::vector<double>& im) = 0;
+  virtual double energy() const = 0;
+  virtual double env_build_s() const = 0;
+  virtual const std::vector<int>& bond_dims() const = 0;
+  virtual EngineConfig& config() = 0;
+  virtual size_t device_bytes() const = 0;
+};
+
+std::unique_ptr<EngineBase> make_engine(const EngineConfig& cfg);
+
+}  // namespace dmrg2

@@ -1,0 +1,101 @@
+// Launchers for the Krylov, SVD and data-movement kernels.
+#pragma once
+
+#include "common.cuh"
+
+namespace dmrg2 {
+
+constexpr int KRYLOV_CAP = 128;   // hard cap on Krylov vectors per Lanczos pass
+constexpr int VEC_THREADS = 256;
+
+// Device-resident state of one Lanczos solve (one per engine).
+struct LanczosDev {
+  double alpha[KRYLOV_CAP];
+  double beta[KRYLOV_CAP];
+  double coef[2 * (KRYLOV_CAP + 1)];   // projection coefficients of the current pass (re, im)
+  double ritz[KRYLOV_CAP];             // Ritz coefficients (real: T is real symmetric)
+  double nrm2;                         // squared norm produced by the last reduction
+  double e_prev, e_cur;
+  double tol;
+  int done;                            // 1 once converged / broken down / Krylov space full
+  int converged;
+  int n_iter;                          // size of the tridiagonal matrix
+  int randomized;
+  int kmax;
+  int pad[3];
+};
+
+// Reduction scratch shared by the vector kernels.
+struct RedScratch {
+  double* part = nullptr;   // [nblk][ncoef*2]
+  unsigned* counter = nullptr;
+  int nblk = 0;
+};
+
+int vec_blocks(ll n);
+
+// w <- H v is done by the caller; these kernels implement one Lanczos step.
+template <typename T>
+void lz_dots(const T* V, int nv, ll n, const T* w, LanczosDev* st, RedScratch& r, cudaStream_t s);
+template <typename T>
+void lz_update_dots(const T* V, int nv, ll n, T* w, LanczosDev* st, RedScratch& r, cudaStream_t s);
+template <typename T>
+void lz_update_norm_check(const T* V, int nv, ll n, T* w, LanczosDev* st, RedScratch& r, int j,
+                          int kmax, cudaStream_t s);
+template <typename T>
+void lz_normalize_next(T* vnext, const T* w, ll n, LanczosDev* st, cudaStream_t s);
+// start: nrm(theta) -> (random fill if ~0) -> v0 = theta/|theta|
+template <typename T>
+void lz_start(T* theta, T* v0, ll n, LanczosDev* st, RedScratch& r, unsigned seed, double tol,
+              int kmax, cudaStream_t s);
+// Ritz vector out = sum_i ritz_i V_i, normalised.
+template <typename T>
+void lz_ritz(const T* V, ll n, T* out, LanczosDev* st, RedScratch& r, cudaStream_t s);
+
+// ---------------------------------------------------------------- SVD
+struct JacobiCtl {
+  unsigned bar_count;
+  unsigned bar_gen;
+  int err;
+  int sweeps;
+  int rotated[64];
+};
+
+struct SvdOut {
+  int k;            // kept rank
+  int nonzero;
+  double trunc_err; // sum of discarded sigma^2
+  double sigma_max;
+  double sigma_max2;
+  double fro2;
+  int jacobi_sweeps;
+  int jacobi_err;
+};
+
+template <typename T>
+void svd_jacobi(T* X, T* Q, int nvec, ll len, JacobiCtl* ctl, int max_sweeps, double tol,
+                const double* fro2_dev, cudaStream_t s);  // fro2_dev: |X|_F^2 on device, or null for 1
+template <typename T>
+void svd_sort_truncate(const T* X, int nvec, ll len, double* sigma, int* perm, SvdOut* out,
+                       int chi_max, double cutoff, bool relative_cutoff, const JacobiCtl* ctl,
+                       cudaStream_t s);
+// gather: left (rows x k) and right (k x cols) factors from X (rotated vectors) / Q.
+//   mode 0 ('R'): vectors were rows of theta: left = conj(Q^T) cols, right = X rows
+//   mode 1 ('L'): vectors were columns:       left = X^T,            right = conj(Q) rows
+template <typename T>
+void svd_gather(const T* X, const T* Q, const int* perm, int nvec, ll len, int k, int mode,
+                T* left, T* right, cudaStream_t s);
+
+// ---------------------------------------------------------------- misc
+template <typename T>
+void transpose(const T* in, T* out, ll rows, ll cols, cudaStream_t s);  // out[c][r] = in[r][c]
+template <typename T>
+void set_identity(T* Q, int n, cudaStream_t s);
+template <typename T>
+void scale_inplace(T* x, ll n, const double* inv_scale_dev, cudaStream_t s);
+template <typename T>
+void norm2(const T* x, ll n, double* out_dev, RedScratch& r, cudaStream_t s);
+template <typename T>
+void trace_real(const T* M, int n, ll ld, double* out_re, double* out_im, cudaStream_t s);
+
+}  // namespace dmrg2

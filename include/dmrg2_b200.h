@@ -1,0 +1,196 @@
+/*
+ * dmrg2_b200.h - C ABI of the B200-native two-site DMRG engine.
+ *
+ * The solver entry points replace the C++ class DMRG2GPU<Scalar> of the
+ * reference driver (gpu-rocm/dmrg2-gpu/src/dmrg2_gpu.h:24-203) with plain C
+ * functions: integer status codes instead of exceptions, caller-owned host
+ * buffers, handle-owned device memory. The op-level entry points replace the
+ * reference's numpy two-site primitives (cpu/pdmrg/pdmrg/numerics/*.py,
+ * cpu/pdmrg/pdmrg/environments/update.py) one for one and run them on the GPU.
+ *
+ * Scalars: DMRG2_F64 = double, DMRG2_C128 = interleaved (re, im) doubles,
+ * ABI-compatible with cuDoubleComplex / hipDoubleComplex / numpy complex128.
+ *
+ * Tensor layouts (DMRG2_LAYOUT_ROWMAJOR, the numpy C-order of the oracle):
+ *   MPS site   A[i]  shape (chi_i, d, chi_{i+1})          index (a*d + s)*chi_{i+1} + b
+ *   MPO site   W[i]  shape (Dl_i, Dr_i, d, d)              axes (mpo_l, mpo_r, s_in, s_out);
+ *                    the applied operator is O[s_out][s_in] = W[..., s_in, s_out];
+ *                    Dl_0 = Dr_{L-1} = 1.
+ *   local op   op    d x d row-major, op[s_out*d + s_in] = <s_out|O|s_in>
+ *   envs       (bra, mpo, ket)
+ * DMRG2_LAYOUT_REFERENCE is the column-major layout of the reference driver:
+ *   MPS  A[a + s*chi_l + b*chi_l*d]
+ *   MPO  W[w + s*D + sp*D*d + wp*D*d*d] with one padded D for all sites, the left
+ *        boundary picking row 0 of W[0] and the right boundary column D-1 of
+ *        W[L-1] (gpu-rocm/common/challenge_mpos.h:4-7).
+ *
+ * Threading: one handle per host thread; calls on one handle are not
+ * reentrant. All functions return DMRG2_OK (0) on success.
+ */
+#ifndef DMRG2_B200_H
+#define DMRG2_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DMRG2_ABI_VERSION 1
+
+enum dmrg2_status {
+  DMRG2_OK = 0,
+  DMRG2_ERR_ARG = 1,     /* invalid argument or shape */
+  DMRG2_ERR_CUDA = 2,    /* CUDA runtime error (message in dmrg2_last_error) */
+  DMRG2_ERR_STATE = 3,   /* call out of order (e.g. run before set_mpo) */
+  DMRG2_ERR_NUMERIC = 4, /* solver failure (e.g. Jacobi barrier timeout) */
+  DMRG2_ERR_INTERNAL = 5
+};
+
+enum dmrg2_dtype { DMRG2_F64 = 0, DMRG2_C128 = 1 };
+enum dmrg2_layout { DMRG2_LAYOUT_ROWMAJOR = 0, DMRG2_LAYOUT_REFERENCE = 1 };
+enum dmrg2_init_kind { DMRG2_INIT_RANDOM = 0, DMRG2_INIT_PRODUCT = 1, DMRG2_INIT_NEEL = 2 };
+
+typedef struct dmrg2_handle dmrg2_handle;
+
+/* Solver configuration. Fields left at 0 take the reference driver's defaults
+ * (dmrg2_gpu_impl.h:138,975-976,1276; dmrg2_gpu.h:30). */
+typedef struct dmrg2_config {
+  int L;              /* chain length */
+  int d;              /* local dimension */
+  int chi_max;        /* largest bond dimension any sweep may use */
+  int dtype;          /* dmrg2_dtype */
+  double tol;         /* sweep stop rule |E_sweep - E_prev| < tol (0 -> 1e-10) */
+  int krylov_max;     /* Lanczos vectors per pass (0 -> 100, capped at 128) */
+  double lanczos_tol; /* Lanczos stop rule on successive Ritz values (0 -> 1e-12) */
+  int max_restarts;   /* explicit Lanczos restarts from the Ritz vector (default 0) */
+  double cutoff;      /* absolute singular-value cutoff (0 -> 1e-14; <0 -> none) */
+  int min_sweeps;     /* sweeps before the stop rule applies (0 -> 2) */
+  int device;         /* CUDA device ordinal */
+  uint64_t seed;      /* seed for random initial states and Lanczos restarts */
+} dmrg2_config;
+
+/* One row per sweep (left-to-right + right-to-left half sweep). */
+typedef struct dmrg2_sweep_report {
+  int sweep;
+  int chi_max;             /* bond dimension cap of this sweep */
+  double energy;           /* eigenvalue of the last bond optimised */
+  double trunc_err_max;    /* largest discarded weight of any bond */
+  double trunc_err_sum;    /* summed discarded weight over the sweep */
+  int max_bond;            /* largest bond dimension after the sweep */
+  double wall_s;           /* host wall time of the sweep */
+  long long matvecs;       /* H_eff applications */
+  double heff_s;           /* device time inside the H_eff contractions */
+  double heff_flops;       /* algorithmic real flops of those contractions */
+  long long lanczos_iters; /* Krylov vectors built */
+  int lanczos_unconverged; /* bonds whose Lanczos hit the Krylov cap */
+  double svd_s;            /* device time of the SVD truncations */
+  int jacobi_sweeps_max;
+  double device_s;         /* device time of the whole sweep (CUDA events on the solver stream) */
+} dmrg2_sweep_report;
+
+/* ---------------------------------------------------------------- solver */
+
+/* DMRG2GPU<Scalar>::DMRG2GPU(L, d, chi_max, D_mpo, tol)  (dmrg2_gpu.h:30) */
+int dmrg2_create(const dmrg2_config* cfg, dmrg2_handle** out);
+/* DMRG2GPU<Scalar>::~DMRG2GPU()  (dmrg2_gpu_impl.h:265-343) */
+void dmrg2_destroy(dmrg2_handle* h);
+
+/* DMRG2GPU<Scalar>::set_mpo(const std::vector<Scalar*>&)  (dmrg2_gpu.h:38, impl:436-485).
+ * ROWMAJOR: Dl/Dr hold the per-site MPO bonds. REFERENCE: Dl points to the single
+ * padded D_mpo and Dr is ignored. Host buffers are copied; the caller keeps them. */
+int dmrg2_set_mpo(dmrg2_handle* h, const void* const* W, const int* Dl, const int* Dr, int layout);
+
+/* Load an MPS (no reference counterpart: the reference only has the initialisers
+ * below). bond_dims has L+1 entries with bond_dims[0] = bond_dims[L] = 1. */
+int dmrg2_set_mps(dmrg2_handle* h, const void* const* A, const int* bond_dims, int layout);
+
+/* DMRG2GPU<Scalar>::initialize_mps_random / _product / _neel  (dmrg2_gpu.h:34-36,
+ * impl:383-429). Random entries are 0.1*U[-1,1] from the seeded generator. */
+int dmrg2_init_mps(dmrg2_handle* h, int kind, uint64_t seed);
+
+/* DMRG2GPU<Scalar>::run(n_sweeps)  (dmrg2_gpu.h:32, impl:1427-1457).
+ * chi_schedule[s] is the bond cap of sweep s (NULL: chi_max for every sweep).
+ * Up to max_out reports are written; *n_out receives the number of sweeps run. */
+int dmrg2_run(dmrg2_handle* h, const int* chi_schedule, int n_sweeps, dmrg2_sweep_report* out,
+              int max_out, int* n_out);
+
+/* Continue sweeping from the state left by the last dmrg2_run or dmrg2_resume
+ * (environments are kept; no stop rule). No reference counterpart: the reference
+ * run() always rebuilds environments (impl:1427-1436). */
+int dmrg2_resume(dmrg2_handle* h, const int* chi_schedule, int n_sweeps, dmrg2_sweep_report* out,
+                 int max_out, int* n_out);
+
+/* get_energy() (dmrg2_gpu.h:40) */
+int dmrg2_get_energy(const dmrg2_handle* h, double* energy);
+/* seconds spent right-canonicalising and building environments in the last run
+ * (the reference's env_build_sec, impl:1428-1436) */
+int dmrg2_get_env_build_seconds(const dmrg2_handle* h, double* seconds);
+/* chi_L / chi_R (dmrg2_gpu.h:42-43): all L+1 bond dimensions */
+int dmrg2_get_bond_dims(const dmrg2_handle* h, int* bond_dims);
+/* get_mps (dmrg2_gpu.h:41, impl:1464-1472): out[i] must hold
+ * bond_dims[i]*d*bond_dims[i+1] scalars. */
+int dmrg2_get_mps(dmrg2_handle* h, void* const* out, int layout);
+/* <psi|O_i|psi>/<psi|psi> for every site (no reference counterpart on the GPU
+ * path; the oracle computes it from the final MPS). re/im hold L doubles. */
+int dmrg2_expect_local(dmrg2_handle* h, const void* op, double* re, double* im);
+/* device memory held by the handle */
+int dmrg2_get_device_bytes(const dmrg2_handle* h, size_t* bytes);
+
+/* Message of the last failed call on h (h may be NULL for create and op calls). */
+const char* dmrg2_last_error(const dmrg2_handle* h);
+int dmrg2_abi_version(void);
+/* number of CUDA kernels this library has launched in this process */
+long long dmrg2_get_launch_count(void);
+
+/* ---------------------------------------------------------------- ops
+ * One GPU launch sequence per call on host buffers (copied in and out), for
+ * parity tests and for callers that drive their own sweep. Shapes and
+ * conventions follow the numpy primitives they replace. */
+
+/* apply_heff(L, R, W_left, W_right, theta)  (cpu/pdmrg/pdmrg/numerics/effective_ham.py:21-81;
+ * GPU: apply_heff_two_site, dmrg2_gpu_impl.h:607-780)
+ *   L (cL, Dl, cL), R (cR, Dr, cR), WL (Dl, Dm, d, d), WR (Dm, Dr, d, d),
+ *   theta/out (cL, d, d, cR). */
+int dmrg2_op_heff(int dtype, int cL, int cR, int d, int Dl, int Dm, int Dr, const void* L,
+                  const void* R, const void* WL, const void* WR, const void* theta, void* out);
+
+/* update_left_env(L, A, W)  (cpu/pdmrg/pdmrg/environments/update.py:16-80; GPU: impl:787-860)
+ *   L (cL, Dl, cL), A (cL, d, cO), W (Dl, Dr, d, d) -> out (cO, Dr, cO) */
+int dmrg2_op_env_left(int dtype, int cL, int cO, int d, int Dl, int Dr, const void* L,
+                      const void* A, const void* W, void* out);
+
+/* update_right_env(R, B, W)  (update.py:83-127; GPU: impl:867-934)
+ *   R (cI, Dr, cI), B (cO, d, cI), W (Dl, Dr, d, d) -> out (cO, Dl, cO) */
+int dmrg2_op_env_right(int dtype, int cI, int cO, int d, int Dl, int Dr, const void* R,
+                       const void* B, const void* W, void* out);
+
+/* truncated_svd(M, max_bond, cutoff)  (cpu/pdmrg/pdmrg/numerics/accurate_svd.py:82-110;
+ * GPU: svd_split, impl:1167-1343). M is m x n row-major. direction 'R' returns
+ * left = U (m x k, isometric) and right = S*Vh (k x n); 'L' returns left = U*S
+ * and right = Vh (isometric rows). S receives the min(m,n) singular values in
+ * descending order. left/right must hold m*min(m,n) and min(m,n)*n scalars. */
+int dmrg2_op_svd(int dtype, int m, int n, const void* M, int max_bond, double cutoff,
+                 char direction, double* S, void* left, void* right, int* k,
+                 double* trunc_err);
+
+/* optimize_two_site(L, R, W_left, W_right, theta0)  (cpu/pdmrg/pdmrg/numerics/eigensolver.py:13-63;
+ * GPU: lanczos_eigensolver, impl:971-1160). theta is the start vector on entry
+ * and the normalised ground state on exit. */
+int dmrg2_op_lanczos(int dtype, int cL, int cR, int d, int Dl, int Dm, int Dr, const void* L,
+                     const void* R, const void* WL, const void* WR, void* theta, int krylov_max,
+                     double tol, int max_restarts, double* energy, int* iters);
+
+/* C = alpha*op(A)*op(B) + beta*C on the FP64 tensor cores (row-major; test hook
+ * for the contraction kernel). trans: 0 = N, 1 = T, 2 = C (conjugate transpose),
+ * 3 = R (conjugate, no transpose; A only). alpha/beta are (re, im) pairs. */
+int dmrg2_op_gemm(int dtype, int transA, int transB, int M, int N, int K, const double* alpha,
+                  const void* A, long long lda, const void* B, long long ldb, const double* beta,
+                  void* C, long long ldc);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DMRG2_B200_H */

@@ -1,0 +1,172 @@
+"""End-to-end two-site DMRG on the GPU against the oracle and ED.
+
+Same MPO, same seeded initial MPS and the same sweep schedule go to the GPU
+engine (through the C ABI) and to the CPU oracle. Bars (from the spec):
+energies |dE|/|E| <= 1e-10 vs the oracle, ED at L=12 to 1e-12 with an exact
+bond dimension, truncation error and <S^z_i> / <n_i> within 1e-8.
+"""
+import json
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import dmrg2
+from oracle import dmrg2_oracle as O
+from oracle import models as M
+
+pytestmark = pytest.mark.gpu
+REPO = Path(__file__).resolve().parent.parent
+
+
+def gpu_run(mpo, mps, schedule, **kw):
+    L, d = len(mpo), mpo[0].shape[2]
+    cplx = np.iscomplexobj(mpo[0]) or np.iscomplexobj(mps[0])
+    eng = dmrg2.DMRG2GPU(L, d, max(schedule), dtype=np.complex128 if cplx else np.float64, **kw)
+    eng.set_mpo(mpo)
+    eng.set_mps(mps)
+    rep = eng.run(schedule=schedule)
+    return eng, rep
+
+
+def test_heisenberg_L12_ed_exact_bond():
+    """L=12 with chi=64 (exact MPS): energy equals FP64 ED to 1e-12."""
+    L = 12
+    mpo = M.heisenberg_mpo(L)
+    eng, rep = gpu_run(mpo, O.random_mps(L, 2, 8, seed=0), [64] * 10, krylov_max=30,
+                       max_restarts=4)
+    e_ed = M.ground_energy(M.ham_heisenberg(L))
+    assert abs(rep[-1]["energy"] - e_ed) <= 1e-12 * abs(e_ed)
+    assert rep[-1]["trunc_err_max"] < 1e-20
+
+
+def test_heisenberg_L12_config_vs_oracle():
+    """chi0=8 seed 0, chi_max=32, cutoff 1e-14, Krylov 30, 10 sweeps (the L=12 config)."""
+    L = 12
+    mpo, mps = M.heisenberg_mpo(L), O.random_mps(L, 2, 8, seed=0)
+    eng, rep = gpu_run(mpo, mps, [32] * 10, krylov_max=30, cutoff=1e-14, max_restarts=4)
+    ref = O.dmrg2(mpo, mps, [32] * 10, cutoff=1e-14)
+    e, er = rep[-1]["energy"], ref["energy"]
+    assert abs(e - er) <= 1e-10 * abs(er)
+    assert abs(rep[-1]["trunc_err_max"] - ref["trunc_err_max"][-1]) <= 1e-8
+    e_ed = M.ground_energy(M.ham_heisenberg(L))
+    assert abs(e - e_ed) < 1e-11  # chi=32 truncation floor is ~1.5e-12
+    sz_gpu = eng.expect_local(M.SZ)
+    sz_ref = O.expect_local(ref["mps"], M.SZ).real
+    np.testing.assert_allclose(sz_gpu, sz_ref, atol=1e-8)
+    # final MPS: energy of the returned state equals the reported energy
+    A = eng.get_mps()
+    assert eng.bond_dims() == [1] + [a.shape[2] for a in A]
+    assert abs(O.mpo_expectation(A, mpo).real - e) < 1e-9
+
+
+def test_reference_fixture_L12_vs_quimb_golden(golden_dir):
+    """benchmark_data/regular/heisenberg/L12_D20: quimb DMRG2 golden energy at chi=20."""
+    ref = json.loads((golden_dir / "ref_dmrg.json").read_text())["heis_L12_fixture"]
+    mpo = O.load_npz_mpo(golden_dir / "heis_L12_mpo.npz")
+    mps = O.load_npz_mps(golden_dir / "heis_L12_mps.npz")
+    eng, rep = gpu_run(mpo, mps, [20] * 8, max_restarts=4)
+    assert abs(rep[-1]["energy"] - ref["quimb_dmrg2_energy"]) <= 1e-10 * abs(ref["quimb_dmrg2_energy"])
+    assert abs(rep[-1]["energy"] - ref["ref_sweep_chi20"][-1]) <= 1e-10 * 6
+
+
+@pytest.mark.parametrize("key", ["xxz_L10_d07_seed1_chi16", "jos_L6_nmax1_seed2_chi16", "j1j2_L10_seed3_chi24"])
+def test_reference_sweep_loop_energies(golden_dir, key):
+    ref = json.loads((golden_dir / "ref_dmrg.json").read_text())[key]
+    builds = {
+        "xxz_L10_d07_seed1_chi16": lambda: (M.heisenberg_mpo(10, 1.0, 0.7), O.random_mps(10, 2, 4, 1)),
+        "jos_L6_nmax1_seed2_chi16": lambda: (M.josephson_mpo(6), O.random_mps(6, 3, 4, 2, np.complex128)),
+        "j1j2_L10_seed3_chi24": lambda: (M.j1j2_mpo(10, 1.0, 0.3), O.random_mps(10, 2, 4, 3)),
+    }
+    mpo, mps = builds[key]()
+    eng, rep = gpu_run(mpo, mps, [ref["chi"]] * 8, max_restarts=4)
+    e_ref = ref["ref_sweep"][-1]
+    assert abs(rep[-1]["energy"] - e_ref) <= 2e-10 * abs(e_ref)
+
+
+def test_josephson_complex_baseline_form_vs_oracle():
+    """E_C (n - n_g)^2 - E_J/2 (e^{iA} a^dag a + h.c.), d=5, complex128, L=8."""
+    L = 8
+    mpo = M.josephson_mpo(L, 2, 2.0, 1.0, 0.25, 2 * np.pi * 0.1 / L, "shifted")
+    mps = O.random_mps(L, 5, 16, seed=0, dtype=np.complex128)
+    eng, rep = gpu_run(mpo, mps, [48] * 8, max_restarts=4)
+    ref = O.dmrg2(mpo, mps, [48] * 8)
+    assert abs(rep[-1]["energy"] - ref["energy"]) <= 1e-10 * abs(ref["energy"])
+    _, n, _, _ = M.josephson_ops(2)
+    np.testing.assert_allclose(eng.expect_local(n).real, O.expect_local(ref["mps"], n).real, atol=1e-8)
+    assert abs(rep[-1]["trunc_err_max"] - ref["trunc_err_max"][-1]) <= 1e-8
+
+
+def test_chi_schedule_and_reports():
+    L = 20
+    mpo, mps = M.heisenberg_mpo(L), O.random_mps(L, 2, 16, seed=0)
+    sched = [8, 8, 16, 16, 32, 32]
+    eng, rep = gpu_run(mpo, mps, sched, cutoff=1e-12, tol=1e-14, min_sweeps=6)
+    ref = O.dmrg2(mpo, mps, sched, cutoff=1e-12, tol=1e-14, min_sweeps=6)
+    assert [r["chi_max"] for r in rep] == sched
+    for r, e in zip(rep, ref["energies"]):
+        assert r["max_bond"] <= r["chi_max"]
+    # every sweep energy is variational and the last one matches the oracle
+    assert abs(rep[-1]["energy"] - ref["energy"]) <= 1e-10 * abs(ref["energy"])
+    assert all(r["matvecs"] > 0 and r["heff_flops"] > 0 for r in rep)
+
+
+def test_reference_layout_mpo_and_mps_equivalent():
+    """set_mpo in the reference driver's column-major padded layout gives the same run."""
+    L, D, d = 10, 5, 2
+    mpo = M.heisenberg_mpo(L)
+    flat = []
+    for i, W in enumerate(mpo):
+        Wp = np.zeros((D, D, d, d))
+        if i == 0:
+            Wp[0:1] = W
+        elif i == L - 1:
+            Wp[:, D - 1:D] = W
+        else:
+            Wp[:] = W
+        # reference: W[w + s*D + sp*D*d + wp*D*d*d]  == Wp[w, wp, s, sp]
+        flat.append(np.transpose(Wp, (1, 3, 2, 0)).ravel())
+    mps = O.random_mps(L, 2, 8, seed=4)
+    e1 = dmrg2.DMRG2GPU(L, d, 16)
+    e1.set_mpo(mpo); e1.set_mps(mps); r1 = e1.run(schedule=[16] * 4)
+    e2 = dmrg2.DMRG2GPU(L, d, 16)
+    e2.set_mpo_reference(flat, D); e2.set_mps(mps); r2 = e2.run(schedule=[16] * 4)
+    assert abs(r1[-1]["energy"] - r2[-1]["energy"]) < 1e-12
+
+
+def test_initializers_neel_product_random():
+    L = 8
+    for init in ("neel", "product", "random"):
+        eng = dmrg2.DMRG2GPU(L, 2, 32)
+        eng.set_mpo(M.heisenberg_mpo(L))
+        getattr(eng, f"initialize_mps_{init}")()
+        rep = eng.run(schedule=[32] * 10)
+        if init == "product":
+            # |0...0> is an eigenstate of the XXZ chain (S^z_tot sector): DMRG stays there
+            assert abs(rep[-1]["energy"] - 0.25 * (L - 1)) < 1e-10
+        else:
+            assert abs(rep[-1]["energy"] - (-3.374932598688)) < 1e-10
+
+
+@pytest.mark.parametrize("args,expect", [
+    (["8", "32", "10"], -3.374932598688),
+    (["4", "16", "10"], -1.616025403784),
+    (["6", "32", "10", "--josephson"], -1.748843818181493),
+    (["8", "32", "10", "--j1j2"], -3.0),
+    (["8", "32", "10", "--j1j2j3", "--j2", "0.4", "--j3", "0.2"], -3.1205086380),
+    (["4", "32", "10", "--ladder"], -4.2930664566945656),
+])
+def test_cli_known_answers(args, expect, tmp_path):
+    """The CLI keeps the reference driver's argv/stdout contract and its KATs."""
+    cli = REPO / "dmrg-implementations_b200" / "bin" / "dmrg2_gpu"
+    out = tmp_path / "row.json"
+    r = subprocess.run([str(cli)] + args + ["--json", str(out)], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "PASS" in r.stdout
+    line = [l for l in r.stdout.splitlines() if l.startswith("Final energy:")][0]
+    assert abs(float(line.split(":")[1]) - expect) < 1e-8
+    assert "timer_scope: sweep_only" in r.stdout
+    row = json.loads(out.read_text())["results"][0]
+    assert row["arch"] == "b200" and row["success"] and abs(row["energy"] - expect) < 1e-8

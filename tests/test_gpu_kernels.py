@@ -1,0 +1,187 @@
+"""Kernel-level parity on the GPU through the C ABI, against the oracle.
+
+Each GPU primitive is compared with the oracle's restatement of the
+reference's numpy primitive (apply_heff, update_left_env, update_right_env,
+truncated_svd, optimize_two_site) on the same seeded inputs, and with the
+golden outputs of the reference modules (tests/golden/ref_primitives.npz).
+Tolerance: 1e-12 relative to the largest output magnitude (FP64 with a
+different summation order).
+"""
+import numpy as np
+import pytest
+
+import dmrg2
+from oracle import dmrg2_oracle as O
+
+pytestmark = pytest.mark.gpu
+RTOL = 1e-12
+
+
+def rnd(rng, shape, cplx):
+    x = rng.standard_normal(shape)
+    if cplx:
+        x = x + 1j * rng.standard_normal(shape)
+    return x
+
+
+def close(a, b, rtol=RTOL):
+    scale = max(np.abs(b).max(), 1e-300)
+    err = np.abs(a - b).max() / scale
+    assert err <= rtol, f"relative error {err:.3e} > {rtol:.1e}"
+
+
+GEMM_SHAPES = [(1, 1, 1), (3, 5, 7), (64, 64, 16), (65, 33, 17), (130, 70, 129), (200, 257, 64)]
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+@pytest.mark.parametrize("shape", GEMM_SHAPES)
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("N", "T"), ("T", "N"), ("T", "T"), ("C", "N"), ("R", "N"), ("C", "T")])
+def test_gemm_dmma(cplx, shape, ta, tb):
+    if not cplx and ta in ("C", "R"):
+        pytest.skip("conjugation is the identity for real data")
+    rng = np.random.default_rng(hash((cplx, shape, ta, tb)) % 2**32)
+    M, N, K = shape
+    A = rnd(rng, (K, M) if ta in ("T", "C") else (M, K), cplx)
+    B = rnd(rng, (N, K) if tb == "T" else (K, N), cplx)
+    C0 = rnd(rng, (M, N), cplx)
+    opA = {"N": A, "T": A.T, "C": A.conj().T, "R": A.conj()}[ta]
+    opB = B.T if tb == "T" else B
+    alpha, beta = (0.75 - 0.5j, 0.25 + 1j) if cplx else (0.75, -0.5)
+    ref = alpha * opA @ opB + beta * C0
+    out = dmrg2.gemm(A, B, ta, tb, alpha=alpha, beta=beta, C=C0)
+    close(out, ref)
+
+
+@pytest.fixture(scope="module")
+def prim(golden_dir):
+    return np.load(golden_dir / "ref_primitives.npz")
+
+
+@pytest.mark.parametrize("tag", ["r0", "r1", "r2", "c0", "c1"])
+def test_primitives_vs_reference_golden(prim, tag):
+    g = lambda k: prim[f"{tag}_{k}"]
+    close(dmrg2.apply_heff(g("L"), g("R"), g("WL"), g("WR"), g("theta")), g("heff"))
+    close(dmrg2.update_left_env(g("L"), g("A"), g("WL")), g("lenv"))
+    close(dmrg2.update_right_env(g("R"), g("B"), g("WR")), g("renv"))
+
+
+HEFF_CASES = [
+    # cL, cR, d, Dl, Dm, Dr, complex
+    (1, 2, 2, 1, 5, 5, False),
+    (8, 16, 2, 5, 5, 5, False),
+    (31, 33, 2, 5, 5, 5, False),
+    (64, 64, 2, 5, 5, 5, False),
+    (17, 9, 3, 4, 4, 4, True),
+    (25, 25, 5, 4, 4, 4, True),
+    (40, 37, 2, 8, 8, 8, False),
+    (50, 50, 4, 8, 8, 8, False),
+]
+
+
+@pytest.mark.parametrize("case", HEFF_CASES)
+def test_heff_vs_oracle(case):
+    cL, cR, d, Dl, Dm, Dr, cplx = case
+    rng = np.random.default_rng(cL * 1000 + cR)
+    L = rnd(rng, (cL, Dl, cL), cplx)
+    R = rnd(rng, (cR, Dr, cR), cplx)
+    WL = rnd(rng, (Dl, Dm, d, d), cplx)
+    WR = rnd(rng, (Dm, Dr, d, d), cplx)
+    th = rnd(rng, (cL, d, d, cR), cplx)
+    close(dmrg2.apply_heff(L, R, WL, WR, th), O.apply_heff(L, R, WL, WR, th))
+
+
+ENV_CASES = [(1, 2, 2, 1, 5, False), (16, 32, 2, 5, 5, False), (33, 31, 2, 5, 5, False),
+             (20, 40, 5, 4, 4, True), (64, 64, 2, 8, 8, False), (7, 13, 3, 4, 1, True)]
+
+
+@pytest.mark.parametrize("case", ENV_CASES)
+def test_env_updates_vs_oracle(case):
+    c1, c2, d, Dl, Dr, cplx = case
+    rng = np.random.default_rng(c1 * 77 + c2)
+    Lenv = rnd(rng, (c1, Dl, c1), cplx)
+    A = rnd(rng, (c1, d, c2), cplx)
+    W = rnd(rng, (Dl, Dr, d, d), cplx)
+    close(dmrg2.update_left_env(Lenv, A, W), O.update_left_env(Lenv, A, W))
+    Renv = rnd(rng, (c2, Dr, c2), cplx)
+    close(dmrg2.update_right_env(Renv, A, W), O.update_right_env(Renv, A, W))
+
+
+SVD_CASES = [(4, 4, False), (8, 32, False), (32, 8, False), (64, 64, False), (100, 37, False),
+             (128, 128, False), (40, 40, True), (25, 60, True), (75, 75, True)]
+
+
+@pytest.mark.parametrize("m,n,cplx", SVD_CASES)
+@pytest.mark.parametrize("direction", ["R", "L"])
+def test_svd_split_vs_oracle(m, n, cplx, direction):
+    rng = np.random.default_rng(m * 131 + n)
+    M = rnd(rng, (m, n), cplx)
+    # graded spectrum, like a Schmidt decomposition
+    U, s, Vh = np.linalg.svd(M, full_matrices=False)
+    s = np.exp(-0.3 * np.arange(len(s)))
+    M = (U * s) @ Vh
+    chi = max(1, min(m, n) - 3)
+    left, S, right, te = dmrg2.truncated_svd(M, chi, 0.0, direction)
+    Uo, So, Vho, teo = O.truncated_svd(M, chi)
+    np.testing.assert_allclose(S, np.linalg.svd(M, compute_uv=False), rtol=0, atol=1e-13)
+    assert left.shape == (m, chi) and right.shape == (chi, n)
+    assert abs(te - teo) <= 1e-13
+    close(left @ right, (Uo * So) @ Vho, 1e-12)
+    if direction == "R":
+        np.testing.assert_allclose(left.conj().T @ left, np.eye(chi), atol=1e-12)
+    else:
+        np.testing.assert_allclose(right @ right.conj().T, np.eye(chi), atol=1e-12)
+
+
+def test_svd_rank_deficient_and_cutoff():
+    rng = np.random.default_rng(5)
+    A = rng.standard_normal((48, 5)) @ rng.standard_normal((5, 40))
+    A /= np.linalg.norm(A)
+    left, S, right, te = dmrg2.truncated_svd(A, 30, 1e-12, "R")
+    assert left.shape[1] == 5  # cutoff stops at the numerical rank
+    assert te < 1e-20
+    close(left @ right, A, 1e-12)
+    np.testing.assert_allclose(left.T @ left, np.eye(5), atol=1e-12)
+
+
+def test_svd_degenerate_spectrum():
+    # exactly degenerate singular values (SU(2) multiplets in Heisenberg chains)
+    rng = np.random.default_rng(9)
+    Q1, _ = np.linalg.qr(rng.standard_normal((64, 64)))
+    Q2, _ = np.linalg.qr(rng.standard_normal((64, 64)))
+    s = np.repeat([0.8, 0.4, 0.2, 0.1, 0.05, 0.01, 1e-3, 1e-4], 8)
+    M = (Q1 * s) @ Q2.T
+    for direction in ("R", "L"):
+        left, S, right, te = dmrg2.truncated_svd(M, 24, 0.0, direction)
+        np.testing.assert_allclose(S, s, atol=1e-14)
+        close(left @ right, (Q1[:, :24] * s[:24]) @ Q2[:, :24].T, 1e-12)
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_lanczos_vs_dense(cplx):
+    rng = np.random.default_rng(3 + cplx)
+    cL, cR, d, D = 6, 7, 2, 3
+    if cplx:
+        d = 3
+    L = rnd(rng, (cL, D, cL), cplx)
+    R = rnd(rng, (cR, D, cR), cplx)
+    WL = rnd(rng, (D, D, d, d), cplx)
+    WR = rnd(rng, (D, D, d, d), cplx)
+    # hermitise the environments and MPO so H_eff is Hermitian
+    L = L + np.transpose(L, (2, 1, 0)).conj()
+    R = R + np.transpose(R, (2, 1, 0)).conj()
+    WL = WL + np.transpose(WL, (0, 1, 3, 2)).conj()
+    WR = WR + np.transpose(WR, (0, 1, 3, 2)).conj()
+    n = cL * d * d * cR
+    H = np.zeros((n, n), complex)
+    for j in range(n):
+        e = np.zeros(n)
+        e[j] = 1
+        H[:, j] = O.apply_heff(L, R, WL, WR, e.reshape(cL, d, d, cR)).ravel()
+    assert np.abs(H - H.conj().T).max() < 1e-10 * np.abs(H).max()
+    w, V = np.linalg.eigh(H)
+    th0 = rnd(rng, (cL, d, d, cR), cplx)
+    e, th = dmrg2.optimize_two_site(L, R, WL, WR, th0, max_iter=100, tol=1e-13, max_restarts=8)
+    assert abs(e - w[0]) <= 1e-10 * abs(w).max()
+    ov = abs(np.vdot(V[:, 0], th.ravel()))
+    assert abs(ov - 1.0) < 1e-8
+    assert abs(np.linalg.norm(th) - 1.0) < 1e-12
