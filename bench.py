@@ -1,0 +1,363 @@
+"""Benchmark of the B200 two-site DMRG engine (one JSON line on stdout).
+
+Workload: S=1/2 Heisenberg chain, open boundaries, L=100, J=1, Delta=1, MPO bond
+dimension 5, float64; seeded i.i.d. N(0,1) initial MPS with chi=16 (seed 0);
+cutoff 1e-12; the chi ramp 32 -> 64 -> 128 -> 256. Synthetic inputs of the
+configuration's shapes (no dataset is involved).
+
+  step     = one sweep (left-to-right + right-to-left) at chi = 256, continuing from
+             the state left by the W warm-up sweeps (the ramp 32, 64, 128, 256, ...)
+  value    = K / (device time of the K timed sweeps)  [sweeps/s], CUDA events on the
+             engine's stream, max over ranks
+  e2e      = the whole solve (W ramp sweeps + K sweeps) through the C ABI from host
+             MPO/MPS arrays to the host energy and final MPS, host wall clock,
+             H2D/D2H included  [sweeps/s]
+  roofline = the H_eff contractions (FP64 DMMA): algorithmic flops / their device
+             time over the timed sweeps, against a cuBLAS DGEMM measured in the same
+             run (no FP64 peak exists in the driver-measured peak file)
+
+--impl reference times the oracle (the reference's numpy two-site primitives,
+restated) on the host cores for the same schedule, on a bounded sample.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+sys.path.insert(0, str(REPO / "dmrg-implementations_b200"))
+
+L_SITES = 100
+RAMP = [32, 64, 128, 256]
+CHI = 256
+CUTOFF = 1e-12
+KRYLOV = 30
+RESTARTS = 2
+METRIC = "sweeps/s (two-site DMRG, Heisenberg L=100, chi=256, FP64 plain form)"
+
+
+def workload_config(n_gpus, extra=None):
+    cfg = {"workload": "heisenberg_xxz_L100_chi256_sweep", "L": L_SITES, "d": 2, "D_mpo": 5,
+           "chi": CHI, "warmup_ramp": RAMP, "cutoff": CUTOFF, "krylov_max": KRYLOV,
+           "lanczos_restarts": RESTARTS, "init": "N(0,1) chi=16 seed 0 (+rank)",
+           "l2": "inputs larger than L2: envs+MPS+Krylov ~0.8 GB resident (L2 126 MB)",
+           "parallelism": f"replicas x{n_gpus}"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def schedule(warmup, steps):
+    ramp = [RAMP[min(i, len(RAMP) - 1)] for i in range(warmup)]
+    return ramp, [CHI] * steps
+
+
+# ----------------------------------------------------------------------------
+# CPU baseline (oracle), bounded sample
+# ----------------------------------------------------------------------------
+def bond_profile(L, chi):
+    dims = [min(2 ** min(i, L - i), chi) for i in range(L + 1)]
+    return [(dims[i], dims[i + 2]) for i in range(L - 1)]
+
+
+def cpu_sample(chis, mv_per_bond, budget_s=20.0, seed=0):
+    """Per-bond cost of the oracle at each chi of `chis`, scaled to whole sweeps.
+
+    Measures on the host cores the oracle's apply_heff, truncated_svd and
+    update_left_env at the chain's bond shapes for each chi, then sums
+    mv_per_bond * t_matvec + t_svd + t_env over the L-1 bonds of a half sweep
+    (two half sweeps per sweep). Returns (seconds per sweep for each chi, info).
+    """
+    from oracle import dmrg2_oracle as O
+    from oracle import models as M
+
+    rng = np.random.default_rng(seed)
+    W = M.heisenberg_mpo(8)[3]
+    cache = {}
+    t_start = time.perf_counter()
+
+    def timed(f, min_s=0.25, max_reps=8):
+        f()
+        n, t0 = 0, time.perf_counter()
+        while n < max_reps and (n == 0 or time.perf_counter() - t0 < min_s):
+            f()
+            n += 1
+        return (time.perf_counter() - t0) / n
+
+    def cost(cl, cr):
+        key = (cl, cr)
+        if key in cache:
+            return cache[key]
+        Lenv = rng.standard_normal((cl, 5, cl))
+        Renv = rng.standard_normal((cr, 5, cr))
+        th = rng.standard_normal((cl, 2, 2, cr))
+        A = rng.standard_normal((cl, 2, min(2 * cl, cr, CHI)))
+        t_mv = timed(lambda: O.apply_heff(Lenv, Renv, W, W, th))
+        t_svd = timed(lambda: O.truncated_svd(th.reshape(cl * 2, 2 * cr), CHI))
+        t_env = timed(lambda: O.update_left_env(Lenv, A, W))
+        cache[key] = (t_mv, t_svd, t_env)
+        return cache[key]
+
+    per_sweep = {}
+    shapes = {}
+    for chi in sorted(set(chis)):
+        prof = bond_profile(L_SITES, chi)
+        uniq = sorted(set(prof), key=lambda s: s[0] * s[1])
+        tot = 0.0
+        for s in uniq:
+            t_mv, t_svd, t_env = cost(*s)
+            n = prof.count(s)
+            tot += n * (mv_per_bond * t_mv + t_svd + t_env)
+        per_sweep[chi] = 2.0 * tot
+        shapes[chi] = len(uniq)
+    info = {"shapes_timed": len(cache), "sample_s": round(time.perf_counter() - t_start, 2),
+            "matvecs_per_bond": mv_per_bond}
+    return per_sweep, info
+
+
+def cpu_threads():
+    return os.cpu_count() or 1
+
+
+def set_cpu_threads():
+    n = str(cpu_threads())
+    for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ.setdefault(k, n)
+
+
+# ----------------------------------------------------------------------------
+# clocks
+# ----------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = max(mx, float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------
+def measure_dgemm_peak():
+    import torch
+
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn_like(a)
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        a @ b
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) * 1e-3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    import dmrg2
+    from oracle import dmrg2_oracle as O
+    from oracle import models as M
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    ramp, steady = schedule(args.warmup, args.steps)
+
+    mpo = M.heisenberg_mpo(L_SITES)
+    mps = O.random_mps(L_SITES, 2, 16, seed=rank)
+    h2d = sum(w.nbytes for w in mpo) + sum(a.nbytes for a in mps)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- e2e solve through the C ABI (host arrays in, host energy + MPS out)
+    barrier()
+    t0 = time.perf_counter()
+    eng = dmrg2.DMRG2GPU(L_SITES, 2, CHI, device=local, krylov_max=KRYLOV, max_restarts=RESTARTS,
+                         cutoff=CUTOFF, tol=1e-300, min_sweeps=10 ** 6)
+    eng.set_mpo(mpo)
+    eng.set_mps(mps)
+    warm = eng.run(schedule=ramp) if ramp else []
+    launches0 = dmrg2.launch_count()
+    barrier()
+    with ClockSampler(local) as clocks:
+        timed = eng.resume(steady)
+        barrier()
+    launches = dmrg2.launch_count() - launches0
+    final = eng.get_mps()
+    energy = eng.get_energy()
+    t_e2e = time.perf_counter() - t0
+    d2h = sum(a.nbytes for a in final) + 8 * (len(warm) + len(timed))
+
+    dev = sum(r["device_s"] for r in timed)
+    heff_s = sum(r["heff_s"] for r in timed)
+    heff_fl = sum(r["heff_flops"] for r in timed)
+    svd_s = sum(r["svd_s"] for r in timed)
+    mv = sum(r["matvecs"] for r in timed)
+    n_sw = len(timed)
+
+    t = torch.tensor([dev, t_e2e], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev_max, e2e_max = float(t[0]), float(t[1])
+    peak = measure_dgemm_peak()
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+    value = world * n_sw / dev_max
+    achieved = heff_fl / heff_s / 1e12 if heff_s > 0 else 0.0
+    set_cpu_threads()
+    mv_per_bond = mv / max(1, n_sw * 2 * (L_SITES - 1))
+    per_sweep, info = cpu_sample([CHI], mv_per_bond, budget_s=20.0)
+    cpu_value = 1.0 / per_sweep[CHI]
+    total_sweeps = len(warm) + len(timed)
+    line = {
+        "metric": METRIC, "value": value, "unit": "sweeps/s", "n_gpus": world,
+        "steps": n_sw, "warmup": len(warm), "ms_per_step": dev_max / n_sw * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded N(0,1) initial MPS, Heisenberg MPO)",
+        "config": workload_config(world),
+        "energy": energy,
+        "e2e": {"value": world * total_sweeps / e2e_max, "unit": "sweeps/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "what": "whole solve (warm-up ramp + timed sweeps) through dmrg2_* from host arrays"},
+        "roofline": {"kernel": "H_eff contraction (FP64 DMMA GEMMs)", "bound": "tensor",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak else None, "traffic": None,
+                     "peak_source": "cuBLAS DGEMM 8192^3 (torch.matmul float64) measured in this run; "
+                                    "MEASURED_PEAKS.json has no FP64 figure"},
+        "time_share": {"heff": heff_s / dev, "svd": svd_s / dev, "other": max(0.0, 1 - (heff_s + svd_s) / dev)},
+        "matvecs_per_bond": mv_per_bond,
+        "cpu_baseline": {"value": cpu_value, "unit": "sweeps/s", "cores": cpu_threads(), "kind": "port",
+                         "sample": f"oracle apply_heff/truncated_svd/update_left_env timed at the chi={CHI} "
+                                   f"bond shapes ({info['shapes_timed']} shapes, {info['sample_s']} s), "
+                                   f"x {mv_per_bond:.1f} matvecs/bond, summed over the L=100 chain"},
+        "clocks": clocks.summary(),
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    set_cpu_threads()
+    ramp, steady = schedule(args.warmup, args.steps)
+    mv_per_bond = 20.0
+    per_sweep, info = cpu_sample(sorted(set(ramp + steady)), mv_per_bond, budget_s=40.0)
+    total = sum(per_sweep[c] for c in ramp + steady)
+    n = len(ramp) + len(steady)
+    value = n / total
+    line = {
+        "metric": METRIC, "value": value, "unit": "sweeps/s", "n_gpus": world, "steps": len(steady),
+        "warmup": len(ramp), "ms_per_step": total / n * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(world), "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "sweeps/s", "cores": cpu_threads(), "kind": "port",
+                         "sample": f"oracle (the reference's numpy primitives restated) timed per bond at every "
+                                   f"bond shape of the schedule {ramp + steady} ({info['shapes_timed']} shapes, "
+                                   f"{info['sample_s']} s), x {mv_per_bond:.0f} matvecs/bond, summed over the chain"},
+        "e2e": {"value": value, "unit": "sweeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=4)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

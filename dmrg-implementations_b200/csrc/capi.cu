@@ -11,6 +11,7 @@
 #include "engine.h"
 #include "kernels.cuh"
 #include "lanczos_driver.cuh"
+#include "truncate.cuh"
 
 using namespace dmrg2;
 
@@ -34,6 +35,7 @@ int guarded(dmrg2_handle* h, F&& f) {
     return DMRG2_OK;
   } catch (const CudaError& e) {
     (h ? h->err : g_err) = e.what();
+    (void)cudaGetLastError();  // clear a non-sticky error so the next call starts clean
     return DMRG2_ERR_CUDA;
   } catch (const std::invalid_argument& e) {
     (h ? h->err : g_err) = e.what();
@@ -140,6 +142,34 @@ void do_op_env_right(int cI, int cO, int d, int Dl, int Dr, const void* R, const
   env_right(dR.as<T>(), dB.as<T>(), dW.as<T>(), dout.as<T>(), X.as<T>(), Y.as<T>(), cI, cO, d, Dl,
             Dr, 0);
   DMRG2_CUDA(cudaMemcpy(out, dout.p, sb * cO * Dl * cO, cudaMemcpyDeviceToHost));
+}
+
+template <typename T>
+void do_op_svd_eig(int m, int n, const void* M, int max_bond, double cutoff, char dir, double* S,
+                   void* left, void* right, int* k_out, double* te_out) {
+  const size_t sb = sizeof(T);
+  const bool R = (dir == 'R');
+  const int nn = R ? m : n;
+  const int kmin = std::min(m, n);
+  DBuf dM(M, sb * (size_t)m * n), dl(sb * (size_t)m * kmin), dr(sb * (size_t)kmin * n);
+  EigWork<T> W;
+  std::vector<double> lam(nn);
+  try {
+    W.init(nn, nn);
+    SvdOut o = eig_split<T>(W, dM.as<T>(), m, n, R ? 'R' : 'L', std::min(max_bond, kmin), cutoff,
+                            false, dl.as<T>(), dr.as<T>(), 0, nn, lam.data());
+    const int k = o.k;
+    if (S)
+      for (int r = 0; r < kmin; ++r) S[r] = std::sqrt(std::max(lam[r], 0.0));
+    if (left) DMRG2_CUDA(cudaMemcpy(left, dl.p, sb * (size_t)m * k, cudaMemcpyDeviceToHost));
+    if (right) DMRG2_CUDA(cudaMemcpy(right, dr.p, sb * (size_t)k * n, cudaMemcpyDeviceToHost));
+    if (k_out) *k_out = k;
+    if (te_out) *te_out = o.trunc_err;
+  } catch (...) {
+    W.release();
+    throw;
+  }
+  W.release();
 }
 
 template <typename T>
@@ -280,6 +310,8 @@ int dmrg2_create(const dmrg2_config* cfg, dmrg2_handle** out) {
     c.cutoff = cfg->cutoff > 0 ? cfg->cutoff : (cfg->cutoff < 0 ? 0.0 : 1e-14);
     c.min_sweeps = cfg->min_sweeps > 0 ? cfg->min_sweeps : 2;
     c.seed = (unsigned)(cfg->seed ^ (cfg->seed >> 32));
+    if (cfg->svd_method != 0 && cfg->svd_method != 1) throw std::invalid_argument("unknown svd_method");
+    c.svd_method = cfg->svd_method;
     std::unique_ptr<dmrg2_handle> h(new dmrg2_handle);
     h->cfg = c;
     h->dtype = cfg->dtype;
@@ -534,8 +566,14 @@ int dmrg2_op_svd(int dtype, int m, int n, const void* M, int max_bond, double cu
     check_pos({m, n, max_bond});
     if (direction != 'R' && direction != 'L' && direction != 'r' && direction != 'l')
       throw std::invalid_argument("op_svd: direction must be 'R' or 'L'");
-    if (dtype == DMRG2_C128) do_op_svd<zc>(m, n, M, max_bond, cutoff, direction, S, left, right, k, trunc_err);
-    else do_op_svd<double>(m, n, M, max_bond, cutoff, direction, S, left, right, k, trunc_err);
+    const bool jac = (direction == 'r' || direction == 'l');
+    if (dtype == DMRG2_C128) {
+      if (jac) do_op_svd<zc>(m, n, M, max_bond, cutoff, direction, S, left, right, k, trunc_err);
+      else do_op_svd_eig<zc>(m, n, M, max_bond, cutoff, direction, S, left, right, k, trunc_err);
+    } else {
+      if (jac) do_op_svd<double>(m, n, M, max_bond, cutoff, direction, S, left, right, k, trunc_err);
+      else do_op_svd_eig<double>(m, n, M, max_bond, cutoff, direction, S, left, right, k, trunc_err);
+    }
   });
 }
 

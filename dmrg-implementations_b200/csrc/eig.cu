@@ -1,0 +1,799 @@
+// Dense Hermitian eigen-decomposition for the theta truncation.
+//
+// The reference truncates theta with a full SVD (rocsolver gesvdj/gesvd,
+// gpu-rocm/dmrg2-gpu/src/dmrg2_gpu_impl.h:1167-1202). Here the truncation uses
+// the reduced density matrix of the side that becomes isometric (G = theta
+// theta^H for a left move, theta^H theta for a right move): its dominant
+// eigenvectors ARE the kept singular vectors, its eigenvalues the squared
+// singular values, and both factors of the split come out without dividing
+// by a singular value (left move: A_i = U_k, A_{i+1} = U_k^H theta).
+//
+// Pipeline (textbook methods, written for sm_100a):
+//   1. hetrd_cluster: Householder reduction G = Q T Q^H to real symmetric
+//      tridiagonal form (Golub & Van Loan, Alg. 8.3.1) by ONE thread-block
+//      cluster of up to 16 CTAs. Rows are distributed cyclically over the
+//      CTAs; the two reductions per column (the scalar p^H v and the all-gather
+//      of w) go through distributed shared memory with two cluster barriers per
+//      column. Every CTA recomputes the next column from the pre-update row
+//      plus the rank-2 correction, so no third barrier is needed.
+//   2. tridiag_bisect: the K largest eigenvalues of T by Sturm-count
+//      multisection, one warp per eigenvalue.
+//   3. tridiag_invit: eigenvectors of T by inverse iteration with partial
+//      pivoting, one thread per eigenvector, seeded random starts.
+//   4. group_mgs: modified Gram-Schmidt inside groups of (numerically)
+//      degenerate eigenvalues (e.g. SU(2) multiplets), then a Newton-Schulz
+//      polar step on the whole block (GEMMs) restores orthogonality to ~eps.
+//   5. apply_q: eigenvectors of G = Q z, each CTA applying all reflectors to
+//      its own slab of columns (columns are independent).
+#include <cooperative_groups.h>
+
+#include "kernels.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace dmrg2 {
+
+static constexpr int HT_THREADS = 512;
+
+__device__ inline double warp_sum_d(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <typename T>
+__device__ inline T warp_sum_t(T v);
+template <>
+__device__ inline double warp_sum_t<double>(double v) { return warp_sum_d(v); }
+template <>
+__device__ inline zc warp_sum_t<zc>(zc v) { return mkz(warp_sum_d(v.re), warp_sum_d(v.im)); }
+
+// block-wide sum of a T value (all threads receive the result)
+template <typename T>
+__device__ T block_sum_t(T v, T* sh) {
+  v = warp_sum_t<T>(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    T r = (l < nw) ? sh[l] : ST<T>::zero();
+    r = warp_sum_t<T>(r);
+    if (l == 0) sh[32] = r;
+  }
+  __syncthreads();
+  T r = sh[32];
+  __syncthreads();
+  return r;
+}
+
+// ----------------------------------------------------------------------------
+// 1. Householder tridiagonalisation by one thread-block cluster
+//    G: n x n Hermitian, row-major (ld). On exit row k of G holds the reflector
+//    v_k in columns k+1..n-1 (v_k[k+1] = 1). Row r is owned by CTA r % C; with
+//    SROWS the owned rows live in shared memory for the whole reduction.
+//    One cluster barrier per column: every CTA pushes its slice of p = tau G v
+//    (and the owner of row k+1 pushes that row) into every peer's shared
+//    memory with remote stores, then each CTA forms s = p^H v, w, its rank-2
+//    update and the next column locally (identically in every CTA).
+// ----------------------------------------------------------------------------
+template <typename T, bool SROWS>
+__global__ void __launch_bounds__(HT_THREADS)
+    hetrd_cluster_kernel(T* __restrict__ G, int n, ll ld, double* __restrict__ dg,
+                         double* __restrict__ eg, T* __restrict__ tau) {
+  cg::cluster_group cluster = cg::this_cluster();
+  const int C = (int)cluster.num_blocks();
+  const int rank = (int)cluster.block_rank();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* x = reinterpret_cast<T*>(smem_raw);  // current column k
+  T* v = x + n;                           // Householder vector
+  T* w = v + n;                           // w (full, local)
+  T* pf0 = w + n;                         // p gathered from all CTAs, two parity buffers
+  T* pf1 = pf0 + n;
+  T* rn0 = pf1 + n;                       // column k+1 before step k, gathered, two parity buffers
+  T* rn1 = rn0 + n;
+  T* red = rn1 + n;                       // [34] reduction scratch
+  T* rows = red + 34;                     // own rows (SROWS): [ceil(n/C)][n]
+  __shared__ T sh_tau, sh_alpha2;
+  __shared__ double sh_beta;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
+  auto own_row = [&](int r) -> T* {
+    if (SROWS) return rows + (ll)(r / C) * n;
+    return G + (ll)r * ld;
+  };
+  if (SROWS) {
+    for (int q = warp; q * C + rank < n; q += nwarp) {
+      const T* src = G + (ll)(q * C + rank) * ld;
+      T* dst = rows + (ll)q * n;
+      for (int j = lane; j < n; j += 32) dst[j] = src[j];
+    }
+  }
+  for (int r = tid; r < n; r += blockDim.x) x[r] = ST<T>::conj(G[r]);  // column 0 = conj(row 0)
+  __syncthreads();
+  cluster.sync();  // all CTAs loaded before any rank 0 reflector store to global row 0
+
+  for (int k = 0; k < n - 1; ++k) {
+    const int par = k & 1;
+    T* pf = par ? pf1 : pf0;
+    T* cfk = par ? rn1 : rn0;      // column k+1 before step k (gathered this step)
+    const int r0 = k + 1 + ((rank - (k + 1)) % C + C) % C;  // first own row >= k+1
+    // (a) reflector of x[k+1..n-1] (identical in every CTA), computed by warp 0:
+    //     H^H x = beta e_1, v = [1, x[k+2:] * sc], tau = (beta - alpha) / beta
+    if (warp == 0) {
+      double xn2 = 0.0;
+      for (int r = k + 2 + lane; r < n; r += 32) xn2 += ST<T>::abs2(x[r]);
+      xn2 = warp_sum_d(xn2);
+      if (lane == 0) {
+        T alpha = x[k + 1];
+        double ar = ST<T>::re(alpha), ai = ST<T>::im(alpha);
+        if (xn2 == 0.0 && ai == 0.0) {
+          sh_tau = ST<T>::zero();
+          sh_beta = ar;
+          sh_alpha2 = ST<T>::zero();  // scale of v[k+2:] (zero vector)
+        } else {
+          double beta = -copysign(sqrt(ar * ar + ai * ai + xn2), ar);
+          sh_tau = ST<T>::make((beta - ar) / beta, -ai / beta);
+          sh_beta = beta;
+          double dr = ar - beta, den = dr * dr + ai * ai;
+          sh_alpha2 = ST<T>::make(dr / den, -ai / den);  // 1 / (alpha - beta)
+        }
+        if (rank == 0) {
+          dg[k] = ST<T>::re(x[k]);
+          eg[k] = sh_beta;
+          tau[k] = sh_tau;
+        }
+      }
+    }
+    __syncthreads();
+    const T tk = sh_tau;
+    const T sc = sh_alpha2;
+    // (b) p = tau * G v on own rows (v applied on the fly), pushed with G[r][k+1]
+    //     (column k+1 before this step's update) to every CTA
+    for (int r = r0 + warp * C; r < n; r += nwarp * C) {
+      const T* row = own_row(r);
+      T acc = ST<T>::zero();
+      for (int j = k + 2 + lane; j < n; j += 32) acc = acc + ST<T>::mul(row[j], x[j]);
+      acc = warp_sum_t<T>(acc);
+      const T col = row[k + 1];
+      acc = ST<T>::mul(tk, col + ST<T>::mul(sc, acc));
+      if (lane < C) {
+        cluster.map_shared_rank(pf, lane)[r] = acc;
+        cluster.map_shared_rank(cfk, lane)[r] = col;
+      }
+    }
+    cluster.sync();  // the only inter-CTA barrier of the step
+    // (c) v, s = p^H v, w = p - 1/2 tau s v  (all rows, locally; thread-private r's)
+    {
+      T sp = ST<T>::zero();
+      for (int r = k + 1 + tid; r < n; r += blockDim.x) {
+        const T vr = (r == k + 1) ? ST<T>::one() : ST<T>::mul(x[r], sc);
+        v[r] = vr;
+        sp = sp + ST<T>::cmul(pf[r], vr);
+      }
+      sp = warp_sum_t<T>(sp);
+      if (lane == 0) red[warp] = sp;
+      __syncthreads();
+      T s = ST<T>::zero();
+      for (int q = 0; q < nwarp; ++q) s = s + red[q];
+      const T a2 = ST<T>::scale(-0.5, ST<T>::mul(tk, s));
+      for (int r = k + 1 + tid; r < n; r += blockDim.x) w[r] = pf[r] + ST<T>::mul(a2, v[r]);
+      __syncthreads();
+    }
+    // (d) rank-2 update of own rows: G -= v w^H + w v^H
+    for (int r = r0 + warp * C; r < n; r += nwarp * C) {
+      T* row = own_row(r);
+      const T vr = v[r], wr = w[r];
+      for (int j = k + 1 + lane; j < n; j += 32)
+        row[j] = row[j] - ST<T>::mul(vr, ST<T>::conj(w[j])) - ST<T>::mul(wr, ST<T>::conj(v[j]));
+    }
+    // (e) next column = column k+1 before this step - rank-2 correction; (f) reflector row k
+    {
+      const T wk = ST<T>::conj(w[k + 1]), vk = ST<T>::conj(v[k + 1]);
+      for (int r = k + 1 + tid; r < n; r += blockDim.x)
+        x[r] = cfk[r] - ST<T>::mul(v[r], wk) - ST<T>::mul(w[r], vk);
+      if (rank == 0)
+        for (int j = k + 1 + tid; j < n; j += blockDim.x) G[(ll)k * ld + j] = v[j];
+    }
+    __syncthreads();
+  }
+  if (rank == 0 && tid == 0) {
+    dg[n - 1] = ST<T>::re(x[n - 1]);
+    eg[n - 1] = 0.0;
+  }
+  cluster.sync();  // peers may still write into this CTA's shared memory
+}
+
+// ----------------------------------------------------------------------------
+// 2. K largest eigenvalues of (d, e) by Sturm-count multisection, one CTA per
+//    eigenvalue (blockDim+1 points per round)
+// ----------------------------------------------------------------------------
+// 1/a: hardware reciprocal estimate refined by two Newton-Raphson steps
+// y <- y + y (1 - a y) (each step doubles the correct bits). Only the sign of the
+// Sturm pivots matters, so the last-bit rounding of IEEE division is not needed.
+__device__ inline double rcp_nr(double a) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
+  double r = fma(-a, y, 1.0);
+  y = fma(y, r, y);
+  r = fma(-a, y, 1.0);
+  return fma(y, r, y);
+}
+
+// Number of eigenvalues of (d, e) below x: negative pivots of the LDL^T
+// factorisation of T - x I (Sturm), q_i = (d_i - x) - e_{i-1}^2 / q_{i-1}.
+__device__ inline int sturm_lt(const double* d, const double* e2, int n, double x, double pivmin) {
+  double q = d[0] - x;
+  if (fabs(q) < pivmin) q = -pivmin;
+  int c = (q < 0.0);
+  for (int i = 1; i < n; ++i) {
+    q = (d[i] - x) - e2[i - 1] * rcp_nr(q);
+    if (fabs(q) < pivmin) q = -pivmin;
+    c += (q < 0.0);
+  }
+  return c;
+}
+
+__global__ void __launch_bounds__(256)
+    tridiag_bisect_kernel(const double* __restrict__ dg, const double* __restrict__ eg, int n, int K,
+                          double* __restrict__ lam) {
+  extern __shared__ double sm[];
+  double* d = sm;
+  double* e2 = sm + n;
+  __shared__ double a_s, b_s, piv_s, afloor_s;
+  __shared__ int tmin;
+  const int j = blockIdx.x;
+  if (j >= K) return;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    d[i] = dg[i];
+    e2[i] = (i < n - 1) ? eg[i] * eg[i] : 0.0;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double lo = 1e300, hi = -1e300, em = 0.0;
+    for (int i = 0; i < n; ++i) {
+      double r = (i > 0 ? fabs(eg[i - 1]) : 0.0) + (i < n - 1 ? fabs(eg[i]) : 0.0);
+      lo = fmin(lo, d[i] - r);
+      hi = fmax(hi, d[i] + r);
+      if (i < n - 1) em = fmax(em, e2[i]);
+    }
+    double w = fmax(hi - lo, fmax(fabs(hi), 1e-300));
+    a_s = lo - 2e-15 * w;
+    b_s = hi + 2e-15 * w;
+    piv_s = 1e-290 * fmax(1.0, em);
+    afloor_s = 2.2e-16 * fmax(fabs(lo), fabs(hi));  // Sturm counts resolve eps*|T| at best
+  }
+  __syncthreads();
+  const int t = n - 1 - j;  // ascending index of the wanted eigenvalue
+  const int NT = blockDim.x;
+  for (int round = 0; round < 24; ++round) {
+    const double a = a_s, b = b_s;
+    const double step = (b - a) / (double)(NT + 1);
+    const double x = a + step * (threadIdx.x + 1);
+    const int c = sturm_lt(d, e2, n, x, piv_s);
+    if (threadIdx.x == 0) tmin = NT;
+    __syncthreads();
+    if (c >= t + 1) atomicMin(&tmin, (int)threadIdx.x);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int l = tmin;
+      if (l == NT) {
+        a_s = a + step * NT;
+      } else {
+        b_s = a + step * (l + 1);
+        a_s = a + step * l;
+      }
+    }
+    __syncthreads();
+    if (b_s - a_s <= 2.2e-16 * fmax(fabs(a_s), fabs(b_s)) + afloor_s) break;
+  }
+  if (threadIdx.x == 0) lam[j] = 0.5 * (a_s + b_s);
+}
+
+// ----------------------------------------------------------------------------
+// 3. inverse iteration for the k kept eigenvalues: one thread per eigenvector,
+//    LU factors with partial pivoting in scratch [i][K], the recurrences carried
+//    in registers. Columns k..K-1 of Z are zeroed.
+// ----------------------------------------------------------------------------
+__device__ inline double hash_unit(unsigned long long x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  x ^= x >> 31;
+  return (double)(x >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+}
+
+__global__ void tridiag_invit_kernel(const double* __restrict__ dg, const double* __restrict__ eg,
+                                     int n, int K, const double* __restrict__ lam,
+                                     const SvdOut* __restrict__ tr, double* __restrict__ Z) {
+  extern __shared__ double dsh[];
+  const int vpb = blockDim.x;  // one vector per thread
+  double* d = dsh;
+  double* e = dsh + n;
+  double* base = dsh + 2 * n;  // [5][n][vpb]
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    d[i] = dg[i];
+    e[i] = (i < n - 1) ? eg[i] : 0.0;
+  }
+  __syncthreads();
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= K) return;
+  if (j >= tr->k) {
+    for (int i = 0; i < n; ++i) Z[(ll)i * K + j] = 0.0;
+    return;
+  }
+  const int t = threadIdx.x;
+#define SX(a, i) base[((ll)(a) * n + (i)) * vpb + t]
+  // arrays: 0 = 1/u0, 1 = u1, 2 = u2, 3 = multiplier, 4 = swap flag
+  double tn = 0.0;
+  for (int i = 0; i < n; ++i)
+    tn = fmax(tn, fabs(d[i]) + fabs(i > 0 ? e[i - 1] : 0.0) + fabs(e[i]));
+  const double tiny = fmax(tn, 1e-300) * 2.2e-16;
+  const double sft = lam[j];
+  double c0 = d[0] - sft, c1 = e[0];
+  for (int i = 0; i < n - 1; ++i) {
+    const double s = e[i];
+    const double dn = d[i + 1] - sft;
+    const double en = e[i + 1];
+    if (fabs(c0) >= fabs(s)) {
+      if (fabs(c0) < tiny) c0 = (c0 < 0 ? -tiny : tiny);
+      const double r = 1.0 / c0;
+      const double m = s * r;
+      SX(0, i) = r;
+      SX(1, i) = c1;
+      SX(2, i) = 0.0;
+      SX(3, i) = m;
+      SX(4, i) = 0.0;
+      c0 = dn - m * c1;
+      c1 = en;
+    } else {
+      const double r = 1.0 / s;
+      const double m = c0 * r;
+      SX(0, i) = r;
+      SX(1, i) = dn;
+      SX(2, i) = en;
+      SX(3, i) = m;
+      SX(4, i) = 1.0;
+      c0 = c1 - m * dn;
+      c1 = -m * en;
+    }
+  }
+  if (fabs(c0) < tiny) c0 = (c0 < 0 ? -tiny : tiny);
+  SX(0, n - 1) = 1.0 / c0;
+  SX(1, n - 1) = 0.0;
+  SX(2, n - 1) = 0.0;
+  // the iterate lives in global memory (column j of Z, coalesced across threads)
+#define IZ(i) Z[(ll)(i) * K + j]
+  for (int i = 0; i < n; ++i) IZ(i) = hash_unit(((unsigned long long)(j + 1) << 32) ^ (unsigned long long)i);
+  for (int it = 0; it < 2; ++it) {
+    double y = IZ(0);
+    for (int i = 0; i < n - 1; ++i) {
+      double yn = IZ(i + 1), yi = y;
+      if (SX(4, i) != 0.0) { yi = yn; yn = y; }
+      IZ(i) = yi;
+      y = yn - SX(3, i) * yi;
+    }
+    IZ(n - 1) = y;
+    double x1 = 0.0, x2 = 0.0, nrm = 0.0;
+    for (int i = n - 1; i >= 0; --i) {
+      const double xi = (IZ(i) - SX(1, i) * x1 - SX(2, i) * x2) * SX(0, i);
+      IZ(i) = xi;
+      nrm += xi * xi;
+      x2 = x1;
+      x1 = xi;
+    }
+    nrm = sqrt(nrm);
+    if (!(nrm > 0.0) || !isfinite(nrm)) {
+      for (int i = 0; i < n; ++i) IZ(i) = (i == (n - 1 - j) % n) ? 1.0 : 0.0;
+      break;
+    }
+    const double inv = 1.0 / nrm;
+    for (int i = 0; i < n; ++i) IZ(i) *= inv;
+  }
+#undef IZ
+#undef SX
+}
+
+// ----------------------------------------------------------------------------
+// 4. Gram-Schmidt inside groups of nearly equal eigenvalues (one warp per group)
+// ----------------------------------------------------------------------------
+__global__ void group_mgs_kernel(double* __restrict__ Z, int n, int K, const double* __restrict__ lam,
+                                 const SvdOut* __restrict__ tr, double gtol_rel) {
+  const int lane = threadIdx.x & 31;
+  const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int kk = tr->k;
+  if (j >= kk) return;
+  const double gtol = gtol_rel * fmax(fabs(lam[0]), 1e-300);
+  if (j > 0 && fabs(lam[j - 1] - lam[j]) <= gtol) return;  // not a group start
+  int end = j + 1;
+  while (end < kk && fabs(lam[end - 1] - lam[end]) <= gtol) ++end;
+  if (end - j < 2) return;
+  for (int q = j; q < end; ++q) {
+    for (int pass = 0; pass < 2; ++pass) {
+      for (int p = j; p < q; ++p) {
+        double s = 0.0;
+        for (int i = lane; i < n; i += 32) s += Z[(ll)i * K + p] * Z[(ll)i * K + q];
+        s = warp_sum_d(s);
+        for (int i = lane; i < n; i += 32) Z[(ll)i * K + q] -= s * Z[(ll)i * K + p];
+        __syncwarp();
+      }
+    }
+    double s = 0.0;
+    for (int i = lane; i < n; i += 32) s += Z[(ll)i * K + q] * Z[(ll)i * K + q];
+    s = warp_sum_d(s);
+    const double inv = (s > 0.0) ? 1.0 / sqrt(s) : 0.0;
+    for (int i = lane; i < n; i += 32) Z[(ll)i * K + q] *= inv;
+    __syncwarp();
+  }
+}
+
+// ----------------------------------------------------------------------------
+// 5. Zg = Q Z with Q = H_0 H_1 ... H_{n-2}; reflector i in row i of R (cols i+1..).
+//    Reflectors are grouped in blocks of nb in compact WY form
+//    H_lo ... H_hi = I - V T V^H (Schreiber & Van Loan), T upper triangular
+//    (wy_build); apply_q then costs three barriers per block. Each CTA owns
+//    AQ_COLS columns of Z (columns are independent).
+// ----------------------------------------------------------------------------
+static constexpr int AQ_COLS = 8;
+static constexpr int AQ_MAXNB = 16;
+static constexpr int AQ_THREADS = 512;
+
+template <typename T>
+__global__ void wy_build_kernel(const T* __restrict__ R, ll ld, const T* __restrict__ tau, int n,
+                                int nb, T* __restrict__ Tb) {
+  __shared__ T gram[AQ_MAXNB][AQ_MAXNB];
+  const int blk = blockIdx.x;
+  const int lo = blk * nb;
+  const int hi = min(n - 2, lo + nb - 1);
+  const int cnt = hi - lo + 1;
+  for (int e = threadIdx.x; e < AQ_MAXNB * AQ_MAXNB; e += blockDim.x) {
+    const int p = e / AQ_MAXNB, q = e % AQ_MAXNB;
+    T acc = ST<T>::zero();
+    if (p < cnt && q < cnt && p < q) {
+      const int ip = lo + p, iq = lo + q;
+      for (int r = iq + 1; r < n; ++r) acc = acc + ST<T>::cmul(R[(ll)ip * ld + r], R[(ll)iq * ld + r]);
+    }
+    gram[p][q] = acc;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    T* Tm = Tb + (ll)blk * AQ_MAXNB * AQ_MAXNB;
+    for (int e = 0; e < AQ_MAXNB * AQ_MAXNB; ++e) Tm[e] = ST<T>::zero();
+    for (int q = 0; q < cnt; ++q) {
+      const T tq = tau[lo + q];
+      Tm[q * AQ_MAXNB + q] = tq;
+      for (int p = 0; p < q; ++p) {  // T(p, q) = -tau_q sum_{l=p}^{q-1} T(p, l) (v_l^H v_q)
+        T acc = ST<T>::zero();
+        for (int l = p; l < q; ++l) acc = acc + ST<T>::mul(Tm[p * AQ_MAXNB + l], gram[l][q]);
+        Tm[p * AQ_MAXNB + q] = ST<T>::scale(-1.0, ST<T>::mul(tq, acc));
+      }
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(AQ_THREADS)
+    apply_q_kernel(const T* __restrict__ R, ll ld, const T* __restrict__ Tb, int n, int nb,
+                   const double* __restrict__ Z, int K, const SvdOut* __restrict__ tr,
+                   T* __restrict__ Zg) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* zs = reinterpret_cast<T*>(smem_raw);  // [AQ_COLS][n] (rows contiguous: conflict-free)
+  T* vb = zs + (ll)n * AQ_COLS;            // [nb][n]
+  __shared__ T W[AQ_MAXNB][AQ_COLS];
+  __shared__ T W2[AQ_MAXNB][AQ_COLS];
+  const int c0 = blockIdx.x * AQ_COLS;
+  const int kk = min(tr->k, K);
+  if (c0 >= kk) return;
+  const int nc = min(AQ_COLS, kk - c0);
+  for (int e = threadIdx.x; e < n * AQ_COLS; e += blockDim.x) {
+    int i = e / AQ_COLS, c = e % AQ_COLS;
+    zs[(ll)c * n + i] = (c < nc) ? ST<T>::make(Z[(ll)i * K + c0 + c], 0.0) : ST<T>::zero();
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nblk = (n - 1 + nb - 1) / nb;
+  for (int blk = nblk - 1; blk >= 0; --blk) {
+    const int lo = blk * nb;
+    const int hi = min(n - 2, lo + nb - 1);
+    const int cnt = hi - lo + 1;
+    __syncthreads();
+    for (int e = threadIdx.x; e < cnt * n; e += blockDim.x) {
+      const int q = e / n, r = e % n;
+      const int i = lo + q;
+      vb[(ll)q * n + r] = (r > i) ? R[(ll)i * ld + r] : ST<T>::zero();
+    }
+    __syncthreads();
+    // W = V^H Z  (warp q -> row q of W)
+    for (int q = warp; q < cnt; q += AQ_THREADS / 32) {
+      T acc[AQ_COLS];
+#pragma unroll
+      for (int c = 0; c < AQ_COLS; ++c) acc[c] = ST<T>::zero();
+      const T* vq = vb + (ll)q * n;
+      for (int r = lo + q + 1 + lane; r < n; r += 32) {
+        const T vr = ST<T>::conj(vq[r]);
+#pragma unroll
+        for (int c = 0; c < AQ_COLS; ++c) acc[c] = acc[c] + ST<T>::mul(vr, zs[(ll)c * n + r]);
+      }
+#pragma unroll
+      for (int c = 0; c < AQ_COLS; ++c) {
+        T sm2 = warp_sum_t<T>(acc[c]);
+        if (lane == 0) W[q][c] = sm2;
+      }
+    }
+    __syncthreads();
+    // W2 = T W  (T upper triangular)
+    if (threadIdx.x < cnt * AQ_COLS) {
+      const int q = threadIdx.x / AQ_COLS, c = threadIdx.x % AQ_COLS;
+      const T* Tm = Tb + (ll)blk * AQ_MAXNB * AQ_MAXNB;
+      T acc = ST<T>::zero();
+      for (int p = q; p < cnt; ++p) acc = acc + ST<T>::mul(Tm[q * AQ_MAXNB + p], W[p][c]);
+      W2[q][c] = acc;
+    }
+    __syncthreads();
+    // Z -= V W2
+    for (int r = lo + 1 + threadIdx.x; r < n; r += blockDim.x) {
+      T acc[AQ_COLS];
+#pragma unroll
+      for (int c = 0; c < AQ_COLS; ++c) acc[c] = ST<T>::zero();
+      for (int q = 0; q < cnt; ++q) {
+        const T vr = vb[(ll)q * n + r];
+#pragma unroll
+        for (int c = 0; c < AQ_COLS; ++c) acc[c] = acc[c] + ST<T>::mul(vr, W2[q][c]);
+      }
+#pragma unroll
+      for (int c = 0; c < AQ_COLS; ++c) zs[(ll)c * n + r] = zs[(ll)c * n + r] - acc[c];
+    }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < n * AQ_COLS; e += blockDim.x) {
+    int i = e / AQ_COLS, c = e % AQ_COLS;
+    if (c < nc) Zg[(ll)i * K + c0 + c] = zs[(ll)c * n + i];
+  }
+}
+
+// max |S - I| over the leading k x k block; sets out->ns_done once below tol.
+// Partial maxima per CTA, the last CTA to arrive decides.
+__global__ void ns_check_kernel(const double* __restrict__ S, int K, SvdOut* out, double tol,
+                                double* part, unsigned* counter) {
+  __shared__ double mx[256];
+  __shared__ int last;
+  const int k = min(out->k, K);
+  double m = 0.0;
+  if (!out->ns_done)
+    for (ll e = (ll)blockIdx.x * blockDim.x + threadIdx.x; e < (ll)k * k; e += (ll)gridDim.x * blockDim.x) {
+      const int a = (int)(e / k), b = (int)(e % k);
+      m = fmax(m, fabs(S[(ll)a * K + b] - (a == b ? 1.0 : 0.0)));
+    }
+  mx[threadIdx.x] = m;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) mx[threadIdx.x] = fmax(mx[threadIdx.x], mx[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = mx[0];
+    __threadfence();
+    last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    double t = 0.0;
+    for (int b = 0; b < (int)gridDim.x; ++b) t = fmax(t, part[b]);
+    if (!out->ns_done && t < tol) out->ns_done = 1;
+    *counter = 0u;
+  }
+}
+
+// ----------------------------------------------------------------------------
+// truncation decision from the eigenvalues (single thread)
+// ----------------------------------------------------------------------------
+__global__ void eig_truncate_kernel(const double* __restrict__ dg, const double* __restrict__ lam,
+                                    int n, int K, int chi_max, double cutoff, int relative,
+                                    SvdOut* out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double tr = 0.0;
+  for (int i = 0; i < n; ++i) tr += dg[i];
+  const double l0 = fmax(lam[0], 0.0);
+  const double noise = 8.0 * 2.2e-16 * (double)n * l0;
+  double thr = relative ? (cutoff * cutoff) * l0 : cutoff * cutoff;
+  thr = fmax(thr, noise);
+  int k = chi_max < K ? chi_max : K;
+  for (int r = 0; r < k; ++r)
+    if (!(lam[r] > thr)) { k = r; break; }
+  if (k < 1) k = 1;
+  double kept = 0.0;
+  int nz = 0;
+  for (int r = 0; r < K; ++r) {
+    if (r < k) kept += fmax(lam[r], 0.0);
+    if (lam[r] > noise) ++nz;
+  }
+  out->k = k;
+  out->nonzero = nz;
+  out->trunc_err = fmax(tr - kept, 0.0);
+  out->sigma_max = sqrt(l0);
+  out->sigma_max2 = l0;
+  out->fro2 = tr;
+  out->jacobi_sweeps = 0;
+  out->jacobi_err = 0;
+  out->ns_done = 0;
+}
+
+// ----------------------------------------------------------------------------
+template <typename T, bool SROWS>
+static void hetrd_launch(T* G, int n, ll ld, double* d, double* e, T* tau, int C, size_t smem,
+                         cudaStream_t s, cudaError_t* err) {
+  static int attr_done = 0;
+  if (!attr_done) {
+    DMRG2_CUDA(cudaFuncSetAttribute(hetrd_cluster_kernel<T, SROWS>,
+                                    cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    DMRG2_CUDA(cudaFuncSetAttribute(hetrd_cluster_kernel<T, SROWS>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+    attr_done = 1;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(C);
+  cfg.blockDim = dim3(HT_THREADS);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  *err = cudaLaunchKernelEx(&cfg, hetrd_cluster_kernel<T, SROWS>, G, n, ld, d, e, tau);
+}
+
+template <typename T>
+void hetrd_cluster(T* G, int n, ll ld, double* d, double* e, T* tau, cudaStream_t s) {
+  const size_t base = sizeof(T) * ((size_t)7 * n + 34);
+  if (base > 200 * 1024) throw std::runtime_error("hetrd: matrix order too large for one cluster");
+  int C = 16;
+  if (n < 64) C = 1;
+  else if (n < 128) C = 4;
+  else if (n < 256) C = 8;
+  static int c_cap = 16;  // largest cluster size the device accepted
+  if (C > c_cap) C = c_cap;
+  for (;;) {
+    const size_t rows = sizeof(T) * (size_t)((n + C - 1) / C) * n;
+    const bool srows = base + rows <= 220 * 1024;
+    cudaError_t err;
+    if (srows) hetrd_launch<T, true>(G, n, ld, d, e, tau, C, base + rows, s, &err);
+    else hetrd_launch<T, false>(G, n, ld, d, e, tau, C, base, s, &err);
+    if (err == cudaSuccess) break;
+    if (C > 1 && (err == cudaErrorInvalidClusterSize || err == cudaErrorLaunchOutOfResources ||
+                  err == cudaErrorInvalidValue)) {
+      (void)cudaGetLastError();
+      C /= 2;
+      c_cap = C;
+      continue;
+    }
+    DMRG2_CUDA(err);
+  }
+  DMRG2_CHECK_LAUNCH();
+}
+
+void tridiag_eigvals(const double* d, const double* e, int n, int K, double* lam, cudaStream_t s) {
+  tridiag_bisect_kernel<<<K, 256, sizeof(double) * 2 * n, s>>>(d, e, n, K, lam);
+  DMRG2_CHECK_LAUNCH();
+}
+
+void tridiag_eigvecs(const double* d, const double* e, int n, int K, const double* lam,
+                     const SvdOut* tr, double* Z, double* scratch, cudaStream_t s) {
+  (void)scratch;
+  static int attr_done = 0;
+  if (!attr_done) {
+    DMRG2_CUDA(cudaFuncSetAttribute(tridiag_invit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    220 * 1024));
+    attr_done = 1;
+  }
+  const size_t per = sizeof(double) * 5 * (size_t)n;
+  int vpb = (int)std::min<size_t>(8, (220 * 1024 - sizeof(double) * 2 * (size_t)n) / per);
+  if (vpb < 1) throw std::runtime_error("inverse iteration: matrix order too large");
+  const size_t smem = sizeof(double) * 2 * (size_t)n + per * vpb;
+  tridiag_invit_kernel<<<(K + vpb - 1) / vpb, vpb, smem, s>>>(d, e, n, K, lam, tr, Z);
+  DMRG2_CHECK_LAUNCH();
+}
+
+void group_mgs(double* Z, int n, int K, const double* lam, const SvdOut* tr, double gtol_rel,
+               cudaStream_t s) {
+  const int wpb = 4;
+  group_mgs_kernel<<<(K + wpb - 1) / wpb, wpb * 32, 0, s>>>(Z, n, K, lam, tr, gtol_rel);
+  DMRG2_CHECK_LAUNCH();
+}
+
+template <typename T>
+__global__ void copy_real_cols_kernel(const double* Z, ll tot, T* Zg) {
+  for (ll t = (ll)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (ll)gridDim.x * blockDim.x)
+    Zg[t] = ST<T>::make(Z[t], 0.0);
+}
+template <typename T>
+static void copy_real_cols(const double* Z, int n, int K, T* Zg, cudaStream_t s) {
+  copy_real_cols_kernel<T><<<1, 256, 0, s>>>(Z, (ll)n * K, Zg);
+  DMRG2_CHECK_LAUNCH();
+}
+
+template <typename T>
+void apply_q(const T* R, ll ld, const T* tau, int n, const double* Z, int K, const SvdOut* tr, T* Zg,
+             T* Tb, cudaStream_t s) {
+  if (n < 2) {  // Q = I
+    copy_real_cols(Z, n, K, Zg, s);
+    return;
+  }
+  const size_t cap = 220 * 1024 / sizeof(T);
+  int nb = (int)std::min<size_t>(AQ_MAXNB, cap / (size_t)n > AQ_COLS ? cap / (size_t)n - AQ_COLS : 0);
+  if (nb < 1) throw std::runtime_error("apply_q: matrix order too large");
+  const size_t smem = sizeof(T) * (size_t)n * (AQ_COLS + nb);
+  static int attr_done = 0;
+  if (!attr_done) {
+    DMRG2_CUDA(cudaFuncSetAttribute(apply_q_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    220 * 1024));
+    attr_done = 1;
+  }
+  const int nblk = (n - 1 + nb - 1) / nb;
+  wy_build_kernel<T><<<nblk, 256, 0, s>>>(R, ld, tau, n, nb, Tb);
+  DMRG2_CHECK_LAUNCH();
+  apply_q_kernel<T><<<(K + AQ_COLS - 1) / AQ_COLS, AQ_THREADS, smem, s>>>(R, ld, Tb, n, nb, Z, K, tr, Zg);
+  DMRG2_CHECK_LAUNCH();
+}
+
+void ns_check(const double* S, int K, SvdOut* out, double tol, double* part, unsigned* counter,
+              cudaStream_t s) {
+  ns_check_kernel<<<32, 256, 0, s>>>(S, K, out, tol, part, counter);
+  DMRG2_CHECK_LAUNCH();
+}
+
+void eig_truncate(const double* d, const double* lam, int n, int K, int chi_max, double cutoff,
+                  bool relative, SvdOut* out, cudaStream_t s) {
+  eig_truncate_kernel<<<1, 32, 0, s>>>(d, lam, n, K, chi_max, cutoff, relative ? 1 : 0, out);
+  DMRG2_CHECK_LAUNCH();
+}
+
+// out[r][j] = conj(in[r][j]) (j < k), in has leading dimension ldi
+template <typename T>
+__global__ void copy_cols_conj_kernel(const T* __restrict__ in, ll ldi, int rows, int k, T* __restrict__ out) {
+  const ll tot = (ll)rows * k;
+  for (ll t = (ll)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (ll)gridDim.x * blockDim.x) {
+    ll r = t / k;
+    int j = (int)(t % k);
+    out[t] = ST<T>::conj(in[r * ldi + j]);
+  }
+}
+// out[j][r] = conj(in[r][j]) (j < k)
+template <typename T>
+__global__ void transpose_conj_kernel(const T* __restrict__ in, ll ldi, int rows, int k, T* __restrict__ out) {
+  const ll tot = (ll)rows * k;
+  for (ll t = (ll)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (ll)gridDim.x * blockDim.x) {
+    int j = (int)(t / rows);
+    ll r = t % rows;
+    out[t] = ST<T>::conj(in[r * ldi + j]);
+  }
+}
+static int eg_grid(ll tot) {
+  ll g = (tot + 255) / 256;
+  if (g > 148 * 8) g = 148 * 8;
+  return (int)(g < 1 ? 1 : g);
+}
+template <typename T>
+void copy_cols_conj(const T* in, ll ldi, int rows, int k, T* out, cudaStream_t s) {
+  copy_cols_conj_kernel<T><<<eg_grid((ll)rows * k), 256, 0, s>>>(in, ldi, rows, k, out);
+  DMRG2_CHECK_LAUNCH();
+}
+template <typename T>
+void transpose_conj(const T* in, ll ldi, int rows, int k, T* out, cudaStream_t s) {
+  transpose_conj_kernel<T><<<eg_grid((ll)rows * k), 256, 0, s>>>(in, ldi, rows, k, out);
+  DMRG2_CHECK_LAUNCH();
+}
+template void copy_cols_conj<double>(const double*, ll, int, int, double*, cudaStream_t);
+template void copy_cols_conj<zc>(const zc*, ll, int, int, zc*, cudaStream_t);
+template void transpose_conj<double>(const double*, ll, int, int, double*, cudaStream_t);
+template void transpose_conj<zc>(const zc*, ll, int, int, zc*, cudaStream_t);
+
+template void hetrd_cluster<double>(double*, int, ll, double*, double*, double*, cudaStream_t);
+template void hetrd_cluster<zc>(zc*, int, ll, double*, double*, zc*, cudaStream_t);
+template void apply_q<double>(const double*, ll, const double*, int, const double*, int,
+                              const SvdOut*, double*, double*, cudaStream_t);
+template void apply_q<zc>(const zc*, ll, const zc*, int, const double*, int, const SvdOut*, zc*, zc*,
+                          cudaStream_t);
+
+}  // namespace dmrg2

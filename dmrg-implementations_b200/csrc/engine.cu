@@ -21,6 +21,7 @@
 #include "contract.cuh"
 #include "engine.h"
 #include "lanczos_driver.cuh"
+#include "truncate.cuh"
 
 namespace dmrg2 {
 
@@ -65,6 +66,8 @@ class Engine final : public EngineBase {
     tmp_ = dalloc((ll)cfg_.chi_max * cfg_.chi_max);
     lw_.init(cfg_.krylov_max, nmax_);
     bytes_ += lw_.bytes(nmax_);
+    ew_.init((int)qmax_, cfg_.chi_max);
+    bytes_ += ew_.bytes;
     sigma_ = (double*)dalloc_bytes(sizeof(double) * qmax_);
     perm_ = (int*)dalloc_bytes(sizeof(int) * qmax_);
     svdout_ = (SvdOut*)dalloc_bytes(sizeof(SvdOut));
@@ -88,6 +91,7 @@ class Engine final : public EngineBase {
     for (void* p : allocs_) cudaFree(p);
     cudaFreeHost(h_svd_);
     lw_.release();
+    ew_.release();
     cudaEventDestroy(ev_c_);
     cudaEventDestroy(ev_d_);
     cudaEventDestroy(ev_s0_);
@@ -336,17 +340,23 @@ class Engine final : public EngineBase {
     envs_valid_ = false;
     for (int i = L_ - 1; i >= 1; --i) {
       const int cl = dims_[i], cr = dims_[i + 1];
-      const ll nc = (ll)d_ * cr;
-      transpose(mps_[i], svdX_, cl, nc, st_);
-      norm2(svdX_, (ll)cl * nc, dscal_, red_, st_);
-      set_identity(svdQ_, (int)nc, st_);
-      svd_jacobi(svdX_, svdQ_, (int)nc, (ll)cl, jctl_, cfg_.jacobi_max_sweeps, jacobi_tol(cl), dscal_,
-                 st_);
-      svd_sort_truncate(svdX_, (int)nc, (ll)cl, sigma_, perm_, svdout_,
-                        std::min(cfg_.chi_max, cap_[i]), 1e-14, true, jctl_, st_);
-      int k = read_svd().k;
-      svd_gather(svdX_, svdQ_, perm_, (int)nc, (ll)cl, k, 1, tmp_, mps_[i], st_);
-      scale_inplace(tmp_, (ll)cl * k, &svdout_->sigma_max2, st_);
+      const int nc = d_ * cr;
+      const int chi = std::min(cfg_.chi_max, cap_[i]);
+      int k;
+      if (cfg_.svd_method == 1) {
+        transpose(mps_[i], svdX_, cl, nc, st_);
+        norm2(svdX_, (ll)cl * nc, dscal_, red_, st_);
+        set_identity(svdQ_, nc, st_);
+        svd_jacobi(svdX_, svdQ_, nc, (ll)cl, jctl_, cfg_.jacobi_max_sweeps, jacobi_tol(cl), dscal_, st_);
+        svd_sort_truncate(svdX_, nc, (ll)cl, sigma_, perm_, svdout_, chi, 1e-14, true, jctl_, st_);
+        k = read_svd().k;
+        svd_gather(svdX_, svdQ_, perm_, nc, (ll)cl, k, 1, tmp_, mps_[i], st_);
+        scale_inplace(tmp_, (ll)cl * k, &svdout_->sigma_max2, st_);
+      } else {
+        SvdOut o = eig_split(ew_, mps_[i], cl, nc, 'L', chi, 1e-14, true, tmp_, mps_[i], st_);
+        k = o.k;
+        scale_inplace(tmp_, (ll)cl * k, &ew_.out->sigma_max2, st_);
+      }
       {  // A[i-1] <- A[i-1] . (U S / sigma_max)
         Gemm<T> g;
         g.M = dims_[i - 1] * d_; g.N = k; g.K = cl;
@@ -417,30 +427,36 @@ class Engine final : public EngineBase {
   void svd_split(int i, char dir, int chi, SweepStats& ss) {
     const int cL = dims_[i], cR = dims_[i + 2];
     const ll m = (ll)cL * d_, nc = (ll)d_ * cR;
-    int nvec;
-    ll len;
     DMRG2_CUDA(cudaEventRecord(ev_c_, st_));
-    if (dir == 'R') {
-      nvec = (int)m;
-      len = nc;
-      DMRG2_CUDA(cudaMemcpyAsync(svdX_, theta_, sizeof(T) * m * nc, cudaMemcpyDeviceToDevice, st_));
+    SvdOut o;
+    if (cfg_.svd_method == 1) {
+      int nvec;
+      ll len;
+      if (dir == 'R') {
+        nvec = (int)m;
+        len = nc;
+        DMRG2_CUDA(cudaMemcpyAsync(svdX_, theta_, sizeof(T) * m * nc, cudaMemcpyDeviceToDevice, st_));
+      } else {
+        nvec = (int)nc;
+        len = m;
+        transpose(theta_, svdX_, m, nc, st_);
+      }
+      set_identity(svdQ_, nvec, st_);
+      svd_jacobi(svdX_, svdQ_, nvec, len, jctl_, cfg_.jacobi_max_sweeps, jacobi_tol(len), nullptr, st_);
+      svd_sort_truncate(svdX_, nvec, len, sigma_, perm_, svdout_, chi, cfg_.cutoff, false, jctl_, st_);
+      DMRG2_CUDA(cudaEventRecord(ev_d_, st_));
+      o = read_svd();
+      svd_gather(svdX_, svdQ_, perm_, nvec, len, o.k, dir == 'R' ? 0 : 1, mps_[i], mps_[i + 1], st_);
     } else {
-      nvec = (int)nc;
-      len = m;
-      transpose(theta_, svdX_, m, nc, st_);
+      o = eig_split(ew_, theta_, (int)m, (int)nc, dir, chi, cfg_.cutoff, false, mps_[i], mps_[i + 1], st_);
+      DMRG2_CUDA(cudaEventRecord(ev_d_, st_));
+      DMRG2_CUDA(cudaEventSynchronize(ev_d_));
     }
-    set_identity(svdQ_, nvec, st_);
-    svd_jacobi(svdX_, svdQ_, nvec, len, jctl_, cfg_.jacobi_max_sweeps, jacobi_tol(len), nullptr, st_);
-    svd_sort_truncate(svdX_, nvec, len, sigma_, perm_, svdout_, chi, cfg_.cutoff, false, jctl_, st_);
-    DMRG2_CUDA(cudaEventRecord(ev_d_, st_));
-    SvdOut o = read_svd();
     float ms = 0.f;
     DMRG2_CUDA(cudaEventElapsedTime(&ms, ev_c_, ev_d_));
     ss.svd_s += ms * 1e-3;
     ss.jacobi_sweeps_max = std::max(ss.jacobi_sweeps_max, o.jacobi_sweeps);
-    const int k = o.k;
-    svd_gather(svdX_, svdQ_, perm_, nvec, len, k, dir == 'R' ? 0 : 1, mps_[i], mps_[i + 1], st_);
-    dims_[i + 1] = k;
+    dims_[i + 1] = o.k;
     ss.trunc_err_max = std::max(ss.trunc_err_max, o.trunc_err);
     ss.trunc_err_sum += o.trunc_err;
   }
@@ -455,6 +471,7 @@ class Engine final : public EngineBase {
   T *theta_ = nullptr, *X_ = nullptr, *Y_ = nullptr, *svdX_ = nullptr,
     *svdQ_ = nullptr, *tmp_ = nullptr;
   LanczosWork<T> lw_;
+  EigWork<T> ew_;
   double* sigma_ = nullptr;
   int* perm_ = nullptr;
   SvdOut* svdout_ = nullptr;

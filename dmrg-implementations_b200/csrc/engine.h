@@ -25,6 +25,7 @@ struct EngineConfig {
   double cutoff = 1e-14;       // absolute singular-value cutoff (dmrg2_gpu_impl.h:1276)
   int min_sweeps = 2;          // the stop rule applies from the second sweep on
   int jacobi_max_sweeps = 40;
+  int svd_method = 0;          // 0: reduced density matrix eigensolver, 1: one-sided block Jacobi
   unsigned seed = 42;
 };
 

@@ -70,6 +70,7 @@ struct SvdOut {
   double fro2;
   int jacobi_sweeps;
   int jacobi_err;
+  int ns_done;      // eigenvector block already orthonormal (Newton-Schulz steps skipped)
 };
 
 template <typename T>
@@ -85,6 +86,26 @@ void svd_sort_truncate(const T* X, int nvec, ll len, double* sigma, int* perm, S
 template <typename T>
 void svd_gather(const T* X, const T* Q, const int* perm, int nvec, ll len, int k, int mode,
                 T* left, T* right, cudaStream_t s);
+
+// ---------------------------------------------------------------- eigen path (eig.cu)
+template <typename T>
+void hetrd_cluster(T* G, int n, ll ld, double* d, double* e, T* tau, cudaStream_t s);
+void tridiag_eigvals(const double* d, const double* e, int n, int K, double* lam, cudaStream_t s);
+void tridiag_eigvecs(const double* d, const double* e, int n, int K, const double* lam,
+                     const SvdOut* tr, double* Z, double* scratch, cudaStream_t s);
+void group_mgs(double* Z, int n, int K, const double* lam, const SvdOut* tr, double gtol_rel,
+               cudaStream_t s);
+template <typename T>
+void apply_q(const T* R, ll ld, const T* tau, int n, const double* Z, int K, const SvdOut* tr, T* Zg,
+             T* Tb, cudaStream_t s);
+void ns_check(const double* S, int K, SvdOut* out, double tol, double* part, unsigned* counter,
+              cudaStream_t s);
+void eig_truncate(const double* d, const double* lam, int n, int K, int chi_max, double cutoff,
+                  bool relative, SvdOut* out, cudaStream_t s);
+template <typename T>
+void copy_cols_conj(const T* in, ll ldi, int rows, int k, T* out, cudaStream_t s);
+template <typename T>
+void transpose_conj(const T* in, ll ldi, int rows, int k, T* out, cudaStream_t s);
 
 // ---------------------------------------------------------------- misc
 template <typename T>

@@ -1,0 +1,160 @@
+// Host driver of the truncated split of theta through the reduced density
+// matrix (eig.cu). Replaces the SVD + truncation + gauge split of the
+// reference (gpu-rocm/dmrg2-gpu/src/dmrg2_gpu_impl.h:1167-1343).
+#pragma once
+
+#include <algorithm>
+#include <stdexcept>
+#include <vector>
+
+#include "common.cuh"
+#include "gemm.cuh"
+#include "kernels.cuh"
+
+namespace dmrg2 {
+
+template <typename T>
+struct EigWork {
+  T* G = nullptr;      // nmax x nmax Gram matrix, then reflectors
+  double* d = nullptr;
+  double* e = nullptr;
+  T* tau = nullptr;
+  double* lam = nullptr;
+  double* Z = nullptr;   // nmax x Kmax
+  double* Z2 = nullptr;  // nmax x Kmax
+  double* S = nullptr;   // Kmax x Kmax
+  double* scr = nullptr; // 5 * nmax * Kmax
+  T* Zg = nullptr;       // nmax x Kmax
+  T* Tb = nullptr;       // compact-WY triangles, 16 x 16 per block of reflectors
+  double* part = nullptr;
+  unsigned* counter = nullptr;
+  SvdOut* out = nullptr;
+  SvdOut* h_out = nullptr;
+  int nmax = 0, Kmax = 0;
+  size_t bytes = 0;
+  std::vector<void*> owned;
+
+  void* alloc(size_t b) {
+    void* p = nullptr;
+    DMRG2_CUDA(cudaMalloc(&p, std::max<size_t>(b, 16)));
+    owned.push_back(p);
+    bytes += b;
+    return p;
+  }
+  void init(int nmax_, int Kmax_) {
+    nmax = std::max(nmax_, 1);
+    Kmax = std::max(std::min(Kmax_, nmax), 1);
+    const size_t nn = (size_t)nmax, kk = (size_t)Kmax;
+    G = (T*)alloc(sizeof(T) * nn * nn);
+    d = (double*)alloc(sizeof(double) * nn);
+    e = (double*)alloc(sizeof(double) * nn);
+    tau = (T*)alloc(sizeof(T) * nn);
+    lam = (double*)alloc(sizeof(double) * kk);
+    Z = (double*)alloc(sizeof(double) * nn * kk);
+    Z2 = (double*)alloc(sizeof(double) * nn * kk);
+    S = (double*)alloc(sizeof(double) * kk * kk);
+    scr = (double*)alloc(sizeof(double) * 5 * nn * kk);
+    Zg = (T*)alloc(sizeof(T) * nn * kk);
+    Tb = (T*)alloc(sizeof(T) * 256 * (nn + 1));
+    part = (double*)alloc(sizeof(double) * 64);
+    counter = (unsigned*)alloc(sizeof(unsigned) * 4);
+    DMRG2_CUDA(cudaMemset(counter, 0, sizeof(unsigned) * 4));
+    out = (SvdOut*)alloc(sizeof(SvdOut));
+    DMRG2_CUDA(cudaMallocHost(&h_out, sizeof(SvdOut)));
+  }
+  void release() {
+    for (void* p : owned) cudaFree(p);
+    owned.clear();
+    if (h_out) cudaFreeHost(h_out);
+    h_out = nullptr;
+  }
+};
+
+// Truncated split of theta (m x nt, row-major).
+//   dir 'R': left (m x k) isometric columns, right (k x nt) = left^H theta
+//   dir 'L': right (k x nt) isometric rows,   left (m x k)  = theta right^H
+// k = min(chi, rank, #{sigma > cutoff}) (relative: sigma > cutoff * sigma_max),
+// singular values below the density-matrix noise floor count as zero.
+// The host waits once (to learn k). Returns the device-side summary.
+// K_compute (>= chi) eigenpairs are computed; lam_out (optional, host) receives them.
+template <typename T>
+SvdOut eig_split(EigWork<T>& W, const T* theta, int m, int nt, char dir, int chi, double cutoff,
+                 bool relative, T* left, T* right, cudaStream_t s, int K_compute = 0,
+                 double* lam_out = nullptr) {
+  const bool R = (dir == 'R');
+  const int n = R ? m : nt;
+  if (n > W.nmax) throw std::runtime_error("eig_split: workspace too small");
+  const int K = std::min(std::min(std::max(chi, K_compute), n), W.Kmax);
+  chi = std::min(chi, K);
+  {  // Gram matrix: R -> conj(theta theta^H) (Hermitian), L -> theta^H theta
+    Gemm<T> g;
+    g.M = n; g.N = n;
+    if (R) {
+      g.ca = true; g.tb = true; g.K = nt;
+      g.A = theta; g.lda = nt;
+      g.B = theta; g.ldb = nt;
+    } else {
+      g.ta = true; g.ca = true; g.K = m;
+      g.A = theta; g.lda = nt;
+      g.B = theta; g.ldb = nt;
+    }
+    g.C = W.G; g.ldc = n;
+    launch_gemm(g, s);
+  }
+  hetrd_cluster<T>(W.G, n, n, W.d, W.e, W.tau, s);
+  tridiag_eigvals(W.d, W.e, n, K, W.lam, s);
+  eig_truncate(W.d, W.lam, n, K, chi, cutoff, relative, W.out, s);  // k decided before any vector
+  tridiag_eigvecs(W.d, W.e, n, K, W.lam, W.out, W.Z, W.scr, s);
+  group_mgs(W.Z, n, K, W.lam, W.out, 1e-14, s);
+  for (int it = 0; it < 3; ++it) {  // Newton-Schulz polar step: Z <- Z (3I - Z^T Z) / 2
+    Gemm<double> g1;
+    g1.ta = true;
+    g1.M = K; g1.N = K; g1.K = n;
+    g1.A = W.Z; g1.lda = K;
+    g1.B = W.Z; g1.ldb = K;
+    g1.C = W.S; g1.ldc = K;
+    g1.skip = &W.out->ns_done;
+    launch_gemm(g1, s);
+    ns_check(W.S, K, W.out, 4e-16 * (double)n, W.part, W.counter, s);
+    DMRG2_CUDA(cudaMemcpyAsync(W.Z2, W.Z, sizeof(double) * (size_t)n * K, cudaMemcpyDeviceToDevice, s));
+    Gemm<double> g2;
+    g2.M = n; g2.N = K; g2.K = K;
+    g2.A = W.Z; g2.lda = K;
+    g2.B = W.S; g2.ldb = K;
+    g2.C = W.Z2; g2.ldc = K;
+    g2.alpha = -0.5; g2.beta = 1.5;
+    g2.skip = &W.out->ns_done;
+    launch_gemm(g2, s);
+    std::swap(W.Z, W.Z2);
+  }
+  apply_q<T>(W.G, n, W.tau, n, W.Z, K, W.out, W.Zg, W.Tb, s);
+  DMRG2_CUDA(cudaMemcpyAsync(W.h_out, W.out, sizeof(SvdOut), cudaMemcpyDeviceToHost, s));
+  DMRG2_CUDA(cudaStreamSynchronize(s));
+  SvdOut o = *W.h_out;
+  const int k = o.k;
+  if (R) {
+    copy_cols_conj<T>(W.Zg, K, m, k, left, s);  // U = conj(eigvecs of conj(G))
+    Gemm<T> g;                                  // right = U^H theta = Zg^T theta
+    g.ta = true;
+    g.M = k; g.N = nt; g.K = m;
+    g.A = W.Zg; g.lda = K;
+    g.B = theta; g.ldb = nt;
+    g.C = right; g.ldc = nt;
+    launch_gemm(g, s);
+  } else {
+    Gemm<T> g;  // left = theta V (before right is written: right may alias theta)
+    g.M = m; g.N = k; g.K = nt;
+    g.A = theta; g.lda = nt;
+    g.B = W.Zg; g.ldb = K;
+    g.C = left; g.ldc = k;
+    launch_gemm(g, s);
+    transpose_conj<T>(W.Zg, K, nt, k, right, s);  // Vh = V^H
+  }
+  if (lam_out) {
+    DMRG2_CUDA(cudaMemcpyAsync(lam_out, W.lam, sizeof(double) * K, cudaMemcpyDeviceToHost, s));
+    DMRG2_CUDA(cudaStreamSynchronize(s));
+  }
+  return o;
+}
+
+}  // namespace dmrg2

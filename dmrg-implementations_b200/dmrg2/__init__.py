@@ -46,7 +46,7 @@ class Config(ctypes.Structure):
         ("L", ctypes.c_int), ("d", ctypes.c_int), ("chi_max", ctypes.c_int), ("dtype", ctypes.c_int),
         ("tol", ctypes.c_double), ("krylov_max", ctypes.c_int), ("lanczos_tol", ctypes.c_double),
         ("max_restarts", ctypes.c_int), ("cutoff", ctypes.c_double), ("min_sweeps", ctypes.c_int),
-        ("device", ctypes.c_int), ("seed", ctypes.c_uint64),
+        ("device", ctypes.c_int), ("seed", ctypes.c_uint64), ("svd_method", ctypes.c_int),
     ]
 
 
@@ -159,7 +159,8 @@ class DMRG2GPU:
     """Two-site DMRG on one B200 (mirror of DMRG2GPU<Scalar>, dmrg2_gpu.h:24-203)."""
 
     def __init__(self, L, d, chi_max, D_mpo=None, tol=1e-10, dtype=np.float64, *, krylov_max=100,
-                 lanczos_tol=1e-12, max_restarts=0, cutoff=1e-14, min_sweeps=2, device=0, seed=42):
+                 lanczos_tol=1e-12, max_restarts=0, cutoff=1e-14, min_sweeps=2, device=0, seed=42,
+                 svd_method=0):
         lib = load_library()
         self.L, self.d, self.chi_max, self.D_mpo = int(L), int(d), int(chi_max), D_mpo
         self.dtype = np.dtype(dtype)
@@ -167,7 +168,7 @@ class DMRG2GPU:
         cfg = Config(L=self.L, d=self.d, chi_max=self.chi_max, dtype=self.code, tol=tol,
                      krylov_max=krylov_max, lanczos_tol=lanczos_tol, max_restarts=max_restarts,
                      cutoff=(cutoff if cutoff > 0 else -1.0), min_sweeps=min_sweeps, device=device,
-                     seed=seed)
+                     seed=seed, svd_method=svd_method)
         h = ctypes.c_void_p()
         _check(lib.dmrg2_create(ctypes.byref(cfg), ctypes.byref(h)), None, "dmrg2_create")
         self._h = h
@@ -336,13 +337,16 @@ def update_right_env(R_env, B, W):
     return out
 
 
-def truncated_svd(M, max_bond, cutoff=0.0, direction="R"):
+def truncated_svd(M, max_bond, cutoff=0.0, direction="R", method="eig"):
     """Truncated SVD split: returns (left, S, right, trunc_err).
 
     direction 'R': left = U (isometric columns), right = diag(S) @ Vh.
     direction 'L': left = U @ diag(S), right = Vh (isometric rows).
     S holds all min(m, n) singular values in descending order.
+    method 'eig' (default): density-matrix eigensolver; 'jacobi': block Jacobi SVD.
     """
+    if method == "jacobi":
+        direction = direction.lower()
     code = _dtype_code(M)
     M = _prep(M, code)
     m, n = M.shape

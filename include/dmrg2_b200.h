@@ -69,6 +69,8 @@ typedef struct dmrg2_config {
   int min_sweeps;     /* sweeps before the stop rule applies (0 -> 2) */
   int device;         /* CUDA device ordinal */
   uint64_t seed;      /* seed for random initial states and Lanczos restarts */
+  int svd_method;     /* truncation: 0 = eigen-decomposition of the reduced density matrix
+                         (default), 1 = one-sided block Jacobi SVD of theta */
 } dmrg2_config;
 
 /* One row per sweep (left-to-right + right-to-left half sweep). */
@@ -170,7 +172,10 @@ int dmrg2_op_env_right(int dtype, int cI, int cO, int d, int Dl, int Dr, const v
  * GPU: svd_split, impl:1167-1343). M is m x n row-major. direction 'R' returns
  * left = U (m x k, isometric) and right = S*Vh (k x n); 'L' returns left = U*S
  * and right = Vh (isometric rows). S receives the min(m,n) singular values in
- * descending order. left/right must hold m*min(m,n) and min(m,n)*n scalars. */
+ * descending order. left/right must hold m*min(m,n) and min(m,n)*n scalars.
+ * 'R'/'L' use the density-matrix eigensolver (singular values below ~1e-7 of
+ * the largest are resolved only as zero); 'r'/'l' use the one-sided block
+ * Jacobi SVD (full relative accuracy). */
 int dmrg2_op_svd(int dtype, int m, int n, const void* M, int max_bond, double cutoff,
                  char direction, double* S, void* left, void* right, int* k,
                  double* trunc_err);

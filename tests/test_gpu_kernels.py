@@ -107,43 +107,77 @@ def test_env_updates_vs_oracle(case):
 
 
 SVD_CASES = [(4, 4, False), (8, 32, False), (32, 8, False), (64, 64, False), (100, 37, False),
-             (128, 128, False), (40, 40, True), (25, 60, True), (75, 75, True)]
+             (128, 128, False), (512, 512, False), (40, 40, True), (25, 60, True), (75, 75, True),
+             (160, 160, True)]
+
+
+def graded(rng, m, n, cplx, rate=0.3):
+    M = rnd(rng, (m, n), cplx)
+    U, s, Vh = np.linalg.svd(M, full_matrices=False)
+    s = np.exp(-rate * np.arange(len(s)))
+    return (U * s) @ Vh
 
 
 @pytest.mark.parametrize("m,n,cplx", SVD_CASES)
 @pytest.mark.parametrize("direction", ["R", "L"])
-def test_svd_split_vs_oracle(m, n, cplx, direction):
+def test_density_matrix_split_vs_oracle(m, n, cplx, direction):
+    """Default truncation: eigen-decomposition of the reduced density matrix.
+
+    Squared singular values agree to 1e-14 of the largest; the kept factors
+    reproduce the oracle's best rank-k approximation; the isometric side is
+    orthonormal to 1e-12. Singular values below ~1e-7 of the largest sit in
+    the density matrix's rounding floor and are dropped (never kept as noise).
+    """
     rng = np.random.default_rng(m * 131 + n)
-    M = rnd(rng, (m, n), cplx)
-    # graded spectrum, like a Schmidt decomposition
-    U, s, Vh = np.linalg.svd(M, full_matrices=False)
-    s = np.exp(-0.3 * np.arange(len(s)))
-    M = (U * s) @ Vh
+    rate = 0.3 if min(m, n) < 200 else 0.05
+    M = graded(rng, m, n, cplx, rate)
     chi = max(1, min(m, n) - 3)
     left, S, right, te = dmrg2.truncated_svd(M, chi, 0.0, direction)
+    s_np = np.linalg.svd(M, compute_uv=False)
+    np.testing.assert_allclose(S ** 2, s_np ** 2, rtol=0, atol=1e-14 * s_np[0] ** 2)
+    k = left.shape[1]
+    assert right.shape == (k, n) and left.shape == (m, k)
+    assert k <= chi and k >= min(chi, int(np.sum(s_np > 1e-6 * s_np[0])))
+    Uo, So, Vho, teo = O.truncated_svd(M, k)
+    assert abs(te - teo) <= 1e-13
+    # kept directions with sigma ~1e-6 carry the density matrix's eps/sigma^2 rounding
+    close(left @ right, (Uo * So) @ Vho, 1e-9)
+    if direction == "R":
+        np.testing.assert_allclose(left.conj().T @ left, np.eye(k), atol=1e-12)
+    else:
+        np.testing.assert_allclose(right @ right.conj().T, np.eye(k), atol=1e-12)
+
+
+@pytest.mark.parametrize("m,n,cplx", [(4, 4, False), (32, 8, False), (64, 64, False), (100, 37, False),
+                                      (40, 40, True), (25, 60, True)])
+@pytest.mark.parametrize("direction", ["R", "L"])
+def test_jacobi_split_vs_oracle(m, n, cplx, direction):
+    """Optional truncation method: one-sided block Jacobi SVD (full relative accuracy)."""
+    rng = np.random.default_rng(m * 7 + n)
+    M = graded(rng, m, n, cplx)
+    chi = max(1, min(m, n) - 3)
+    left, S, right, te = dmrg2.truncated_svd(M, chi, 0.0, direction, method="jacobi")
     Uo, So, Vho, teo = O.truncated_svd(M, chi)
     np.testing.assert_allclose(S, np.linalg.svd(M, compute_uv=False), rtol=0, atol=1e-13)
     assert left.shape == (m, chi) and right.shape == (chi, n)
     assert abs(te - teo) <= 1e-13
     close(left @ right, (Uo * So) @ Vho, 1e-12)
-    if direction == "R":
-        np.testing.assert_allclose(left.conj().T @ left, np.eye(chi), atol=1e-12)
-    else:
-        np.testing.assert_allclose(right @ right.conj().T, np.eye(chi), atol=1e-12)
 
 
-def test_svd_rank_deficient_and_cutoff():
+@pytest.mark.parametrize("method", ["eig", "jacobi"])
+def test_svd_rank_deficient_and_cutoff(method):
     rng = np.random.default_rng(5)
     A = rng.standard_normal((48, 5)) @ rng.standard_normal((5, 40))
     A /= np.linalg.norm(A)
-    left, S, right, te = dmrg2.truncated_svd(A, 30, 1e-12, "R")
+    left, S, right, te = dmrg2.truncated_svd(A, 30, 1e-12, "R", method=method)
     assert left.shape[1] == 5  # cutoff stops at the numerical rank
     assert te < 1e-20
     close(left @ right, A, 1e-12)
     np.testing.assert_allclose(left.T @ left, np.eye(5), atol=1e-12)
 
 
-def test_svd_degenerate_spectrum():
+@pytest.mark.parametrize("method", ["eig", "jacobi"])
+def test_svd_degenerate_spectrum(method):
     # exactly degenerate singular values (SU(2) multiplets in Heisenberg chains)
     rng = np.random.default_rng(9)
     Q1, _ = np.linalg.qr(rng.standard_normal((64, 64)))
@@ -151,9 +185,11 @@ def test_svd_degenerate_spectrum():
     s = np.repeat([0.8, 0.4, 0.2, 0.1, 0.05, 0.01, 1e-3, 1e-4], 8)
     M = (Q1 * s) @ Q2.T
     for direction in ("R", "L"):
-        left, S, right, te = dmrg2.truncated_svd(M, 24, 0.0, direction)
-        np.testing.assert_allclose(S, s, atol=1e-14)
+        left, S, right, te = dmrg2.truncated_svd(M, 24, 0.0, direction, method=method)
+        np.testing.assert_allclose(S ** 2, s ** 2, atol=1e-15)
         close(left @ right, (Q1[:, :24] * s[:24]) @ Q2[:, :24].T, 1e-12)
+        iso = left.T @ left if direction == "R" else right @ right.T
+        np.testing.assert_allclose(iso, np.eye(24), atol=1e-12)
 
 
 @pytest.mark.parametrize("cplx", [False, True])
