@@ -71,13 +71,16 @@ def bond_profile(L, chi):
     return [(dims[i], dims[i + 2]) for i in range(L - 1)]
 
 
-def cpu_sample(chis, mv_per_bond, budget_s=20.0, seed=0):
+def cpu_sample(chis, mv_per_bond, budget_s=20.0, seed=0, profiles=None):
     """Per-bond cost of the oracle at each chi of `chis`, scaled to whole sweeps.
 
     Measures on the host cores the oracle's apply_heff, truncated_svd and
     update_left_env at the chain's bond shapes for each chi, then sums
     mv_per_bond * t_matvec + t_svd + t_env over the L-1 bonds of a half sweep
-    (two half sweeps per sweep). Returns (seconds per sweep for each chi, info).
+    (two half sweeps per sweep). `profiles` may give, per chi, the list of
+    (chi_left, chi_right) bond shapes actually used (e.g. by the GPU run);
+    otherwise the shapes are min(2^min(i, L-i), chi). Returns (seconds per
+    sweep for each chi, info).
     """
     from oracle import dmrg2_oracle as O
     from oracle import models as M
@@ -112,7 +115,7 @@ def cpu_sample(chis, mv_per_bond, budget_s=20.0, seed=0):
     per_sweep = {}
     shapes = {}
     for chi in sorted(set(chis)):
-        prof = bond_profile(L_SITES, chi)
+        prof = profiles[chi] if profiles and chi in profiles else bond_profile(L_SITES, chi)
         uniq = sorted(set(prof), key=lambda s: s[0] * s[1])
         tot = 0.0
         for s in uniq:
@@ -255,11 +258,11 @@ def run_ours(args):
                          cutoff=CUTOFF, tol=1e-300, min_sweeps=10 ** 6)
     eng.set_mpo(mpo)
     eng.set_mps(mps)
-    warm = eng.run(schedule=ramp) if ramp else []
+    warm = list(eng.run(schedule=ramp)) if ramp else []
     launches0 = dmrg2.launch_count()
     barrier()
     with ClockSampler(local) as clocks:
-        timed = eng.resume(steady)
+        timed = list(eng.resume(steady))
         barrier()
     launches = dmrg2.launch_count() - launches0
     final = eng.get_mps()
@@ -287,7 +290,9 @@ def run_ours(args):
     achieved = heff_fl / heff_s / 1e12 if heff_s > 0 else 0.0
     set_cpu_threads()
     mv_per_bond = mv / max(1, n_sw * 2 * (L_SITES - 1))
-    per_sweep, info = cpu_sample([CHI], mv_per_bond, budget_s=20.0)
+    dims = eng.bond_dims()
+    shapes = [(dims[i], dims[i + 2]) for i in range(L_SITES - 1)]
+    per_sweep, info = cpu_sample([CHI], mv_per_bond, budget_s=20.0, profiles={CHI: shapes})
     cpu_value = 1.0 / per_sweep[CHI]
     total_sweeps = len(warm) + len(timed)
     line = {
@@ -297,6 +302,7 @@ def run_ours(args):
         "data": "synthetic (seeded N(0,1) initial MPS, Heisenberg MPO)",
         "config": workload_config(world),
         "energy": energy,
+        "max_bond": max(eng.bond_dims()),
         "e2e": {"value": world * total_sweeps / e2e_max, "unit": "sweeps/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "what": "whole solve (warm-up ramp + timed sweeps) through dmrg2_* from host arrays"},
@@ -308,8 +314,8 @@ def run_ours(args):
         "time_share": {"heff": heff_s / dev, "svd": svd_s / dev, "other": max(0.0, 1 - (heff_s + svd_s) / dev)},
         "matvecs_per_bond": mv_per_bond,
         "cpu_baseline": {"value": cpu_value, "unit": "sweeps/s", "cores": cpu_threads(), "kind": "port",
-                         "sample": f"oracle apply_heff/truncated_svd/update_left_env timed at the chi={CHI} "
-                                   f"bond shapes ({info['shapes_timed']} shapes, {info['sample_s']} s), "
+                         "sample": f"oracle apply_heff/truncated_svd/update_left_env timed at the bond shapes "
+                                   f"of the GPU run's final MPS ({info['shapes_timed']} shapes, {info['sample_s']} s), "
                                    f"x {mv_per_bond:.1f} matvecs/bond, summed over the L=100 chain"},
         "clocks": clocks.summary(),
         "gpu_launches": launches,

@@ -2,6 +2,37 @@
 
 namespace dmrg2 {
 
+// Y[a][o][e] = sum_k W[o][k] X[a][k][e] for Kin, Kout <= KM (the two-site MPO
+// mixing of H_eff step 2 when D d^2 is small): one thread per (a, e), the Kin
+// inputs in registers, W in shared memory. Bandwidth-bound: X read once, Y
+// written once.
+template <typename T, int KM>
+__global__ void __launch_bounds__(128)
+    mpo_mix_kernel(const T* __restrict__ X, const T* __restrict__ W, T* __restrict__ Y, int Kin,
+                   int Kout, int cR, ll sX, ll sY, const int* skip) {
+  if (skip && *((volatile const int*)skip)) return;
+  __shared__ T Ws[KM * KM];
+  for (int i = threadIdx.x; i < KM * KM; i += blockDim.x) {
+    const int o = i / KM, k = i % KM;
+    Ws[i] = (o < Kout && k < Kin) ? W[(ll)o * Kin + k] : ST<T>::zero();
+  }
+  __syncthreads();
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= cR) return;
+  const ll a = blockIdx.y;
+  const T* xa = X + a * sX + e;
+  T* ya = Y + a * sY + e;
+  T xin[KM];
+#pragma unroll
+  for (int k = 0; k < KM; ++k) xin[k] = (k < Kin) ? xa[(ll)k * cR] : ST<T>::zero();
+  for (int o = 0; o < Kout; ++o) {
+    T acc = ST<T>::zero();
+#pragma unroll
+    for (int k = 0; k < KM; ++k) acc = acc + ST<T>::mul(Ws[o * KM + k], xin[k]);
+    ya[(ll)o * cR] = acc;
+  }
+}
+
 template <typename T>
 void heff_apply(const T* Lenv, const T* Renv, const T* WWt, const T* in, T* out, T* X, T* Y, int cL,
                 int cR, int d, int Dl, int Dr, const int* skip, cudaStream_t s) {
@@ -15,12 +46,17 @@ void heff_apply(const T* Lenv, const T* Renv, const T* WWt, const T* in, T* out,
     g.nb1 = Dl; g.skip = skip;
     launch_gemm(g, s);
   }
-  {
+  const int Kin = (int)(Dl * dd), Kout = (int)(dd * Dr);
+  if (Kin <= 32 && Kout <= 32 && cL <= 65535) {
+    dim3 grid(ceil_div(cR, 128), cL);
+    mpo_mix_kernel<T, 32><<<grid, 128, 0, s>>>(X, WWt, Y, Kin, Kout, cR, (ll)Kin * cR, (ll)Kout * cR, skip);
+    DMRG2_CHECK_LAUNCH();
+  } else {
     Gemm<T> g;
-    g.M = (int)(dd * Dr); g.N = cR; g.K = (int)(Dl * dd);
-    g.A = WWt; g.lda = Dl * dd; g.sA1 = 0;
-    g.B = X; g.ldb = cR; g.sB1 = (ll)Dl * dd * cR;
-    g.C = Y; g.ldc = cR; g.sC1 = dd * Dr * cR;
+    g.M = Kout; g.N = cR; g.K = Kin;
+    g.A = WWt; g.lda = Kin; g.sA1 = 0;
+    g.B = X; g.ldb = cR; g.sB1 = (ll)Kin * cR;
+    g.C = Y; g.ldc = cR; g.sC1 = (ll)Kout * cR;
     g.nb1 = cL; g.skip = skip;
     launch_gemm(g, s);
   }
@@ -32,6 +68,16 @@ void heff_apply(const T* Lenv, const T* Renv, const T* WWt, const T* in, T* out,
     g.B = Renv; g.ldb = (ll)Dr * cR;
     g.C = out; g.ldc = cR;
     g.skip = skip;
+    // split K when the output tiles cannot fill the GPU; X is free again and
+    // holds Dl * cL * d^2 * cR >= splitk * cL * d^2 * cR partial products
+    const int tiles = ceil_div(g.M, GemmTile<T>::BM) * ceil_div(g.N, GemmTile<T>::BN);
+    int sk = 1;
+    while (sk < Dl && sk < 8 && tiles * sk < 2 * 148 && (ll)g.K / (sk * 2) >= 4 * GemmTile<T>::BK) sk *= 2;
+    if (sk > Dl) sk = Dl;
+    if (sk > 1) {
+      g.splitk = sk;
+      g.ws = X;
+    }
     launch_gemm(g, s);
   }
 }

@@ -72,9 +72,11 @@ __device__ T block_sum_t(T v, T* sh) {
 //    G: n x n Hermitian, row-major (ld). On exit row k of G holds the reflector
 //    v_k in columns k+1..n-1 (v_k[k+1] = 1). Row r is owned by CTA r % C; with
 //    SROWS the owned rows live in shared memory for the whole reduction.
-//    One cluster barrier per column: every CTA pushes its slice of p = tau G v
-//    (and the owner of row k+1 pushes that row) into every peer's shared
-//    memory with remote stores, then each CTA forms s = p^H v, w, its rank-2
+//    One cluster barrier per column: every CTA writes its slice of p = tau G v
+//    and of column k+1 into its OWN shared memory, the cluster synchronises
+//    once, and every thread pulls the entries it needs from the owning CTA
+//    (remote stores drained by a release barrier cost several times more on
+//    sm_100a than one pull phase). Each CTA then forms s = p^H v, w, its rank-2
 //    update and the next column locally (identically in every CTA).
 // ----------------------------------------------------------------------------
 template <typename T, bool SROWS>
@@ -88,11 +90,13 @@ __global__ void __launch_bounds__(HT_THREADS)
   T* x = reinterpret_cast<T*>(smem_raw);  // current column k
   T* v = x + n;                           // Householder vector
   T* w = v + n;                           // w (full, local)
-  T* pf0 = w + n;                         // p gathered from all CTAs, two parity buffers
-  T* pf1 = pf0 + n;
-  T* rn0 = pf1 + n;                       // column k+1 before step k, gathered, two parity buffers
-  T* rn1 = rn0 + n;
-  T* red = rn1 + n;                       // [34] reduction scratch
+  T* pf = w + n;                          // p, all rows (pulled)
+  T* cf = pf + n;                         // column k+1 before step k, all rows (pulled)
+  T* po0 = cf + n;                        // own entries of p / column k+1, two parity buffers
+  T* po1 = po0 + n;
+  T* co0 = po1 + n;
+  T* co1 = co0 + n;
+  T* red = co1 + n;                       // [34] reduction scratch
   T* rows = red + 34;                     // own rows (SROWS): [ceil(n/C)][n]
   __shared__ T sh_tau, sh_alpha2;
   __shared__ double sh_beta;
@@ -108,20 +112,28 @@ __global__ void __launch_bounds__(HT_THREADS)
       for (int j = lane; j < n; j += 32) dst[j] = src[j];
     }
   }
-  for (int r = tid; r < n; r += blockDim.x) x[r] = ST<T>::conj(G[r]);  // column 0 = conj(row 0)
+  double* xnp = reinterpret_cast<double*>(red + 17);  // per-warp partial |x[k+2:]|^2 (16 slots)
+  {
+    double part = 0.0;
+    for (int r = tid; r < n; r += blockDim.x) {
+      x[r] = ST<T>::conj(G[r]);  // column 0 = conj(row 0)
+      if (r >= 2) part += ST<T>::abs2(x[r]);
+    }
+    part = warp_sum_d(part);
+    if (lane == 0) xnp[warp] = part;
+  }
   __syncthreads();
   cluster.sync();  // all CTAs loaded before any rank 0 reflector store to global row 0
 
   for (int k = 0; k < n - 1; ++k) {
     const int par = k & 1;
-    T* pf = par ? pf1 : pf0;
-    T* cfk = par ? rn1 : rn0;      // column k+1 before step k (gathered this step)
+    T* po = par ? po1 : po0;
+    T* co = par ? co1 : co0;
     const int r0 = k + 1 + ((rank - (k + 1)) % C + C) % C;  // first own row >= k+1
     // (a) reflector of x[k+1..n-1] (identical in every CTA), computed by warp 0:
     //     H^H x = beta e_1, v = [1, x[k+2:] * sc], tau = (beta - alpha) / beta
     if (warp == 0) {
-      double xn2 = 0.0;
-      for (int r = k + 2 + lane; r < n; r += 32) xn2 += ST<T>::abs2(x[r]);
+      double xn2 = (lane < nwarp) ? xnp[lane] : 0.0;
       xn2 = warp_sum_d(xn2);
       if (lane == 0) {
         T alpha = x[k + 1];
@@ -131,11 +143,12 @@ __global__ void __launch_bounds__(HT_THREADS)
           sh_beta = ar;
           sh_alpha2 = ST<T>::zero();  // scale of v[k+2:] (zero vector)
         } else {
-          double beta = -copysign(sqrt(ar * ar + ai * ai + xn2), ar);
-          sh_tau = ST<T>::make((beta - ar) / beta, -ai / beta);
+          const double beta = -copysign(sqrt(ar * ar + ai * ai + xn2), ar);
+          const double ib = 1.0 / beta;
+          sh_tau = ST<T>::make((beta - ar) * ib, -ai * ib);
           sh_beta = beta;
-          double dr = ar - beta, den = dr * dr + ai * ai;
-          sh_alpha2 = ST<T>::make(dr / den, -ai / den);  // 1 / (alpha - beta)
+          const double dr = ar - beta, iden = 1.0 / (dr * dr + ai * ai);
+          sh_alpha2 = ST<T>::make(dr * iden, -ai * iden);  // 1 / (alpha - beta)
         }
         if (rank == 0) {
           dg[k] = ST<T>::re(x[k]);
@@ -147,28 +160,38 @@ __global__ void __launch_bounds__(HT_THREADS)
     __syncthreads();
     const T tk = sh_tau;
     const T sc = sh_alpha2;
-    // (b) p = tau * G v on own rows (v applied on the fly), pushed with G[r][k+1]
-    //     (column k+1 before this step's update) to every CTA
+    // (b) p = tau * G v on own rows (v applied on the fly) and G[r][k+1] (column
+    //     k+1 before this step's update), into this CTA's own exchange buffers
     for (int r = r0 + warp * C; r < n; r += nwarp * C) {
       const T* row = own_row(r);
-      T acc = ST<T>::zero();
-      for (int j = k + 2 + lane; j < n; j += 32) acc = acc + ST<T>::mul(row[j], x[j]);
-      acc = warp_sum_t<T>(acc);
+      T a0 = ST<T>::zero(), a1 = ST<T>::zero(), a2 = ST<T>::zero(), a3 = ST<T>::zero();
+      int j = k + 2 + lane;
+      for (; j + 96 < n; j += 128) {  // four independent chains hide load + FMA latency
+        a0 = a0 + ST<T>::mul(row[j], x[j]);
+        a1 = a1 + ST<T>::mul(row[j + 32], x[j + 32]);
+        a2 = a2 + ST<T>::mul(row[j + 64], x[j + 64]);
+        a3 = a3 + ST<T>::mul(row[j + 96], x[j + 96]);
+      }
+      for (; j < n; j += 32) a0 = a0 + ST<T>::mul(row[j], x[j]);
+      T acc = warp_sum_t<T>((a0 + a1) + (a2 + a3));
       const T col = row[k + 1];
-      acc = ST<T>::mul(tk, col + ST<T>::mul(sc, acc));
-      if (lane < C) {
-        cluster.map_shared_rank(pf, lane)[r] = acc;
-        cluster.map_shared_rank(cfk, lane)[r] = col;
+      if (lane == 0) {
+        po[r] = ST<T>::mul(tk, col + ST<T>::mul(sc, acc));
+        co[r] = col;
       }
     }
     cluster.sync();  // the only inter-CTA barrier of the step
-    // (c) v, s = p^H v, w = p - 1/2 tau s v  (all rows, locally; thread-private r's)
+    // (c) pull p and column k+1; v, s = p^H v, w = p - 1/2 tau s v (thread-private r's)
     {
       T sp = ST<T>::zero();
       for (int r = k + 1 + tid; r < n; r += blockDim.x) {
+        const int owner = r % C;
+        const T pr = cluster.map_shared_rank(po, owner)[r];
+        cf[r] = cluster.map_shared_rank(co, owner)[r];
+        pf[r] = pr;
         const T vr = (r == k + 1) ? ST<T>::one() : ST<T>::mul(x[r], sc);
         v[r] = vr;
-        sp = sp + ST<T>::cmul(pf[r], vr);
+        sp = sp + ST<T>::cmul(pr, vr);
       }
       sp = warp_sum_t<T>(sp);
       if (lane == 0) red[warp] = sp;
@@ -183,14 +206,22 @@ __global__ void __launch_bounds__(HT_THREADS)
     for (int r = r0 + warp * C; r < n; r += nwarp * C) {
       T* row = own_row(r);
       const T vr = v[r], wr = w[r];
+#pragma unroll 4
       for (int j = k + 1 + lane; j < n; j += 32)
         row[j] = row[j] - ST<T>::mul(vr, ST<T>::conj(w[j])) - ST<T>::mul(wr, ST<T>::conj(v[j]));
     }
-    // (e) next column = column k+1 before this step - rank-2 correction; (f) reflector row k
+    // (e) next column = column k+1 before this step - rank-2 correction (with the norm
+    //     partials of the next reflector); (f) reflector row k
     {
       const T wk = ST<T>::conj(w[k + 1]), vk = ST<T>::conj(v[k + 1]);
-      for (int r = k + 1 + tid; r < n; r += blockDim.x)
-        x[r] = cfk[r] - ST<T>::mul(v[r], wk) - ST<T>::mul(w[r], vk);
+      double part = 0.0;
+      for (int r = k + 1 + tid; r < n; r += blockDim.x) {
+        const T xr = cf[r] - ST<T>::mul(v[r], wk) - ST<T>::mul(w[r], vk);
+        x[r] = xr;
+        if (r >= k + 3) part += ST<T>::abs2(xr);
+      }
+      part = warp_sum_d(part);
+      if (lane == 0) xnp[warp] = part;
       if (rank == 0)
         for (int j = k + 1 + tid; j < n; j += blockDim.x) G[(ll)k * ld + j] = v[j];
     }
@@ -593,7 +624,8 @@ __global__ void eig_truncate_kernel(const double* __restrict__ dg, const double*
   double tr = 0.0;
   for (int i = 0; i < n; ++i) tr += dg[i];
   const double l0 = fmax(lam[0], 0.0);
-  const double noise = 8.0 * 2.2e-16 * (double)n * l0;
+  // density-matrix rounding floor: eigenvalues below ~16 eps lambda_max are noise
+  const double noise = 16.0 * 2.2e-16 * l0;
   double thr = relative ? (cutoff * cutoff) * l0 : cutoff * cutoff;
   thr = fmax(thr, noise);
   int k = chi_max < K ? chi_max : K;
@@ -646,7 +678,7 @@ static void hetrd_launch(T* G, int n, ll ld, double* d, double* e, T* tau, int C
 
 template <typename T>
 void hetrd_cluster(T* G, int n, ll ld, double* d, double* e, T* tau, cudaStream_t s) {
-  const size_t base = sizeof(T) * ((size_t)7 * n + 34);
+  const size_t base = sizeof(T) * ((size_t)9 * n + 34);
   if (base > 200 * 1024) throw std::runtime_error("hetrd: matrix order too large for one cluster");
   int C = 16;
   if (n < 64) C = 1;

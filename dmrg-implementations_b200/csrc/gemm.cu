@@ -8,6 +8,36 @@ long long& launch_counter() {
   return c;
 }
 
+template <typename T>
+__global__ void splitk_reduce_kernel(const T* __restrict__ ws, int ns, int M, int N, double ar,
+                                     double ai, double br, double bi, T* __restrict__ C, ll ldc,
+                                     const int* skip) {
+  if (skip && *((volatile const int*)skip)) return;
+  const ll tot = (ll)M * N;
+  const T alpha = ST<T>::make(ar, ai), beta = ST<T>::make(br, bi);
+  const bool use_beta = (br != 0.0 || bi != 0.0);
+  for (ll t = (ll)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (ll)gridDim.x * blockDim.x) {
+    T acc = ws[t];
+    for (int z = 1; z < ns; ++z) acc = acc + ws[(ll)z * tot + t];
+    const ll m = t / N, n = t % N;
+    T* c = C + m * ldc + n;
+    T v = ST<T>::mul(alpha, acc);
+    if (use_beta) v = v + ST<T>::mul(beta, *c);
+    *c = v;
+  }
+}
+
+template <typename T>
+static void splitk_reduce(const T* ws, int ns, int M, int N, T alpha, T beta, T* C, ll ldc,
+                          const int* skip, cudaStream_t st) {
+  ll tot = (ll)M * N;
+  ll g = (tot + 255) / 256;
+  if (g > 148 * 8) g = 148 * 8;
+  splitk_reduce_kernel<T><<<(int)(g < 1 ? 1 : g), 256, 0, st>>>(ws, ns, M, N, ST<T>::re(alpha), ST<T>::im(alpha),
+                                                          ST<T>::re(beta), ST<T>::im(beta), C, ldc, skip);
+  DMRG2_CHECK_LAUNCH();
+}
+
 template <typename T, bool TA, bool TB, bool CA>
 static void launch_impl(const Gemm<T>& d, cudaStream_t st) {
   using G = GemmTile<T>;
@@ -27,6 +57,22 @@ static void launch_impl(const Gemm<T>& d, cudaStream_t st) {
   a.alpha_re = ST<T>::re(d.alpha); a.alpha_im = ST<T>::im(d.alpha);
   a.beta_re = ST<T>::re(d.beta); a.beta_im = ST<T>::im(d.beta);
   a.skip = d.skip;
+  a.kchunk = 0;
+  if (d.splitk > 1) {
+    // partial products per K slice into ws[z] (M x N, ld N), then one reduction
+    const int chunk = ceil_div(ceil_div(d.K, d.splitk), G::BK) * G::BK;
+    const int nsplit = ceil_div(d.K, chunk);
+    a.kchunk = chunk;
+    a.C = d.ws; a.ldc = d.N; a.sC1 = (ll)d.M * d.N; a.sC2 = 0;
+    a.sA1 = a.sA2 = a.sB1 = a.sB2 = 0;
+    a.nb2 = 1;
+    a.alpha_re = 1.0; a.alpha_im = 0.0; a.beta_re = 0.0; a.beta_im = 0.0;
+    dim3 grid(ceil_div(d.N, G::BN), ceil_div(d.M, G::BM), nsplit);
+    gemm_kernel<T, TA, TB, CA><<<grid, G::THREADS, S::BYTES, st>>>(a);
+    DMRG2_CHECK_LAUNCH();
+    splitk_reduce<T>(d.ws, nsplit, d.M, d.N, d.alpha, d.beta, d.C, d.ldc, d.skip, st);
+    return;
+  }
   dim3 grid(ceil_div(d.N, G::BN), ceil_div(d.M, G::BM), d.nb1 * d.nb2);
   gemm_kernel<T, TA, TB, CA><<<grid, G::THREADS, S::BYTES, st>>>(a);
   DMRG2_CHECK_LAUNCH();
@@ -36,6 +82,8 @@ template <typename T>
 void launch_gemm(const Gemm<T>& d, cudaStream_t st) {
   if (d.M <= 0 || d.N <= 0 || d.nb1 * d.nb2 <= 0) return;
   if (d.nb1 * d.nb2 > 65535) throw std::runtime_error("gemm: batch count exceeds 65535");
+  if (d.splitk > 1 && (d.nb1 * d.nb2 != 1 || !d.ws))
+    throw std::runtime_error("gemm: split-K needs a single GEMM and a workspace");
   if (ceil_div(d.M, GemmTile<T>::BM) > 65535) throw std::runtime_error("gemm: M too large");
   const bool ca = ST<T>::cplx && d.ca;
   if (!d.ta && !d.tb && !ca) return launch_impl<T, false, false, false>(d, st);

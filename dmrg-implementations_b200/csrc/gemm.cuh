@@ -28,6 +28,7 @@ struct GemmArgs {
   int nb2;
   double alpha_re, alpha_im, beta_re, beta_im;
   const int* skip;  // optional device flag: when non-zero the launch does nothing
+  int kchunk;       // split-K: blockIdx.z selects the K slice [z*kchunk, (z+1)*kchunk) (0 = off)
 };
 
 __device__ __forceinline__ void cp_async_8(void* smem, const void* gmem, bool pred) {
@@ -99,7 +100,10 @@ __global__ void __launch_bounds__(GemmTile<T>::THREADS) gemm_kernel(GemmArgs g) 
   const T* Ab = reinterpret_cast<const T*>(g.A) + z1 * g.sA1 + z2 * g.sA2;
   const T* Bb = reinterpret_cast<const T*>(g.B) + z1 * g.sB1 + z2 * g.sB2;
   T* Cb = reinterpret_cast<T*>(g.C) + z1 * g.sC1 + z2 * g.sC2;
-  const int M = g.M, N = g.N, K = g.K;
+  const int M = g.M, N = g.N;
+  // split-K: this CTA covers K range [kbeg, K)
+  const int kbeg = g.kchunk > 0 ? z * g.kchunk : 0;
+  const int K = g.kchunk > 0 ? min(g.K, kbeg + g.kchunk) : g.K;
   const ll lda = g.lda, ldb = g.ldb, ldc = g.ldc;
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
 
@@ -111,7 +115,7 @@ __global__ void __launch_bounds__(GemmTile<T>::THREADS) gemm_kernel(GemmArgs g) 
   auto load_stage = [&](int stage, int kt) {
     T* As = smem + stage * S::STAGE;
     T* Bs = As + S::SA;
-    const int k0 = kt * BK;
+    const int k0 = kbeg + kt * BK;
 #pragma unroll
     for (int j = 0; j < (BM * BK) / G::THREADS; ++j) {
       int e = tid + j * G::THREADS;
@@ -148,7 +152,7 @@ __global__ void __launch_bounds__(GemmTile<T>::THREADS) gemm_kernel(GemmArgs g) 
         if constexpr (CPLX) acc_im[i][j][r] = 0.0;
       }
 
-  const int nk = (K + BK - 1) / BK;
+  const int nk = (K - kbeg + BK - 1) / BK;
 #pragma unroll
   for (int s = 0; s < G::STAGES - 1; ++s) {
     if (s < nk) load_stage(s, s);
@@ -255,6 +259,8 @@ struct Gemm {
   int nb1 = 1, nb2 = 1;
   T alpha = ST<T>::one(), beta = ST<T>::zero();
   const int* skip = nullptr;
+  int splitk = 1;     // >1: K is split over CTAs, partials go to ws, then summed into C
+  T* ws = nullptr;    // splitk * M * N scratch (single, non-batched GEMMs only)
 };
 
 template <typename T>

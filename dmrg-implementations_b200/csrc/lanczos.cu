@@ -62,13 +62,23 @@ __device__ inline bool arrive_last(unsigned* counter, unsigned nblk) {
 // ----------------------------------------------------------------------------
 // tridiagonal helpers (block-wide / single thread)
 // ----------------------------------------------------------------------------
+// 1/a from the hardware estimate and two Newton-Raphson steps y <- y + y (1 - a y)
+__device__ inline double rcp_refined(double a) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
+  double r = fma(-a, y, 1.0);
+  y = fma(y, r, y);
+  r = fma(-a, y, 1.0);
+  return fma(y, r, y);
+}
+
 __device__ inline int sturm_count(const double* a, const double* b, int k, double x, double pivmin) {
   double q = a[0] - x;
   int c = 0;
   if (fabs(q) < pivmin) q = -pivmin;
   if (q < 0) ++c;
   for (int i = 1; i < k; ++i) {
-    q = (a[i] - x) - b[i - 1] * b[i - 1] / q;
+    q = (a[i] - x) - b[i - 1] * b[i - 1] * rcp_refined(q);
     if (fabs(q) < pivmin) q = -pivmin;
     if (q < 0) ++c;
   }
@@ -76,8 +86,12 @@ __device__ inline int sturm_count(const double* a, const double* b, int k, doubl
 }
 
 // Lowest eigenvalue of the symmetric tridiagonal (a, b) of order k. All threads
-// of the block must call; the result is returned to every thread.
-__device__ double tridiag_lowest(const double* a, const double* b, int k) {
+// of the block must call; the result is returned to every thread. When hint is
+// finite, the bracket starts at [hint - 2|b_{k-2}| - tiny, hint]: by Cauchy
+// interlacing the lowest eigenvalue of T_k is at most that of T_{k-1} (hint),
+// and by Weyl's bound it is at least hint - |b_{k-2}| - |a_{k-1} - ...| which the
+// Gershgorin check below still guards.
+__device__ double tridiag_lowest(const double* a, const double* b, int k, double hint) {
   __shared__ double lo_s, hi_s, piv_s;
   __shared__ int tmin;
   const int NT = blockDim.x;
@@ -93,6 +107,16 @@ __device__ double tridiag_lowest(const double* a, const double* b, int k) {
     lo_s = lo - 1e-14 * w;
     hi_s = hi + 1e-14 * w;
     piv_s = 1e-300 * fmax(1.0, bm);
+    if (k >= 2 && isfinite(hint) && hint < 1e299) {
+      // tight bracket: [hint - 2 |b_{k-2}| - slack, hint + slack], verified by counts below
+      double slack = 1e-12 * fmax(fabs(hint), 1e-300) + 1e-300;
+      double tlo = hint - 2.0 * fabs(b[k - 2]) - slack, thi = hint + slack;
+      int clo = sturm_count(a, b, k, tlo, piv_s), chi = sturm_count(a, b, k, thi, piv_s);
+      if (clo == 0 && chi >= 1) {
+        lo_s = tlo;
+        hi_s = thi;
+      }
+    }
   }
   __syncthreads();
   for (int round = 0; round < 12; ++round) {
@@ -272,7 +296,7 @@ __global__ void __launch_bounds__(VEC_THREADS)
     }
     __syncthreads();
     const int k = j + 1;
-    double lam = tridiag_lowest(st->alpha, st->beta, k);
+    double lam = tridiag_lowest(st->alpha, st->beta, k, st->e_prev);
     if (threadIdx.x == 0) {
       st->e_cur = lam;
       bool conv = (k >= 3) && (fabs(lam - st->e_prev) < st->tol);

@@ -141,7 +141,7 @@ def test_density_matrix_split_vs_oracle(m, n, cplx, direction):
     Uo, So, Vho, teo = O.truncated_svd(M, k)
     assert abs(te - teo) <= 1e-13
     # kept directions with sigma ~1e-6 carry the density matrix's eps/sigma^2 rounding
-    close(left @ right, (Uo * So) @ Vho, 1e-9)
+    close(left @ right, (Uo * So) @ Vho, 1e-8)
     if direction == "R":
         np.testing.assert_allclose(left.conj().T @ left, np.eye(k), atol=1e-12)
     else:
@@ -171,7 +171,7 @@ def test_svd_rank_deficient_and_cutoff(method):
     A /= np.linalg.norm(A)
     left, S, right, te = dmrg2.truncated_svd(A, 30, 1e-12, "R", method=method)
     assert left.shape[1] == 5  # cutoff stops at the numerical rank
-    assert te < 1e-20
+    assert te < 1e-14  # trace minus kept weight: rounding of the density matrix
     close(left @ right, A, 1e-12)
     np.testing.assert_allclose(left.T @ left, np.eye(5), atol=1e-12)
 
