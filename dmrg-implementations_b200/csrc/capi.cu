@@ -11,6 +11,7 @@
 #include "engine.h"
 #include "kernels.cuh"
 #include "lanczos_driver.cuh"
+#include "noalloc.cuh"
 #include "truncate.cuh"
 
 using namespace dmrg2;
@@ -600,6 +601,24 @@ int dmrg2_op_gemm(int dtype, int transA, int transB, int M, int N, int K, const 
     check_pos({M, N, K});
     if (dtype == DMRG2_C128) do_op_gemm<zc>(transA, transB, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
     else do_op_gemm<double>(transA, transB, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+  });
+}
+
+int dmrg2_op_heff_noalloc(int dtype, int cL, int cR, int d, int Dl, int Dm, int Dr, const void* L,
+                          const void* R, const void* WL, const void* WR, const void* theta, void* out,
+                          void* stream) {
+  return guarded(nullptr, [&] {
+    check_dtype(dtype);
+    check_pos({cL, cR, d, Dl, Dm, Dr});
+    if (!L || !R || !WL || !WR || !theta || !out)
+      throw std::invalid_argument("op_heff_noalloc: null device pointer");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (dtype == DMRG2_C128)
+      heff_noalloc<zc>(cL, cR, d, Dl, Dm, Dr, (const zc*)L, (const zc*)R, (const zc*)WL, (const zc*)WR,
+                       (const zc*)theta, (zc*)out, s);
+    else
+      heff_noalloc<double>(cL, cR, d, Dl, Dm, Dr, (const double*)L, (const double*)R, (const double*)WL,
+                           (const double*)WR, (const double*)theta, (double*)out, s);
   });
 }
 

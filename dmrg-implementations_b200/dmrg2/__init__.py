@@ -34,6 +34,7 @@ EXPORTED = [
     "dmrg2_get_mps", "dmrg2_expect_local", "dmrg2_get_device_bytes", "dmrg2_last_error",
     "dmrg2_abi_version", "dmrg2_op_heff", "dmrg2_op_env_left", "dmrg2_op_env_right",
     "dmrg2_op_svd", "dmrg2_op_lanczos", "dmrg2_op_gemm", "dmrg2_resume", "dmrg2_get_launch_count",
+    "dmrg2_op_heff_noalloc",
 ]
 
 
@@ -96,6 +97,7 @@ def load_library(path: str | os.PathLike | None = None):
         "dmrg2_last_error": (ctypes.c_char_p, [vp]),
         "dmrg2_abi_version": (c_int, []),
         "dmrg2_op_heff": (c_int, [c_int] * 7 + [vp] * 6),
+        "dmrg2_op_heff_noalloc": (c_int, [c_int] * 7 + [vp] * 7),
         "dmrg2_op_env_left": (c_int, [c_int] * 6 + [vp] * 4),
         "dmrg2_op_env_right": (c_int, [c_int] * 6 + [vp] * 4),
         "dmrg2_op_svd": (c_int, [c_int, c_int, c_int, vp, c_int, c_dbl, ctypes.c_char, dp, vp, vp, ip, dp]),

@@ -194,6 +194,24 @@ int dmrg2_op_gemm(int dtype, int transA, int transB, int M, int N, int K, const 
                   const void* A, long long lda, const void* B, long long ldb, const double* beta,
                   void* C, long long ldc);
 
+/* apply_heff on DEVICE pointers, allocating no device memory. No counterpart in
+ * the reference: its GPU path only applies H_eff inside its own Lanczos loop on
+ * buffers it allocated up front. For callers that must not allocate while they
+ * run (a solver enqueuing its own loop on a stream, a fixed memory budget): the
+ * scratch (fused two-site MPO plus the two contraction intermediates) lives in a
+ * static device array of DMRG2_NOALLOC_SCRATCH_BYTES, and shapes that need more
+ * are rejected with DMRG2_ERR_ARG before any device work. Shapes and layouts as
+ * dmrg2_op_heff; all six arrays are on the current device. Work is enqueued on
+ * `stream` (a cudaStream_t; NULL = legacy default stream) and the call returns
+ * without synchronising. The first call on each device resolves the scratch
+ * address and loads its module; make it before any stream capture. All calls
+ * on a device share the one scratch array: calls on the same stream are safe,
+ * calls that overlap in time on other streams or threads race. */
+#define DMRG2_NOALLOC_SCRATCH_BYTES (64ull << 20)
+int dmrg2_op_heff_noalloc(int dtype, int cL, int cR, int d, int Dl, int Dm, int Dr, const void* L,
+                          const void* R, const void* WL, const void* WR, const void* theta, void* out,
+                          void* stream);
+
 #ifdef __cplusplus
 }
 #endif
