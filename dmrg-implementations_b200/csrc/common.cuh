@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -83,5 +84,21 @@ long long& launch_counter();
   } while (0)
 
 inline int ceil_div(ll a, ll b) { return (int)((a + b - 1) / b); }
+
+// cudaFuncSetAttribute acts on the current device only; `done` records, one bit
+// per device ordinal (mod 64), where the attribute was already set.
+inline void func_attr_once(std::atomic<unsigned long long>& done, const void* func, cudaFuncAttribute attr,
+                           int value) {
+  int dev = 0;
+  DMRG2_CUDA(cudaGetDevice(&dev));
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (done.load(std::memory_order_acquire) & bit) return;
+  DMRG2_CUDA(cudaFuncSetAttribute(func, attr, value));
+  done.fetch_or(bit, std::memory_order_acq_rel);
+}
+
+inline void set_smem_attr_once(std::atomic<unsigned long long>& done, const void* func, int bytes) {
+  func_attr_once(done, func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
 
 }  // namespace dmrg2

@@ -20,9 +20,10 @@
 //      multisection, one warp per eigenvalue.
 //   3. tridiag_invit: eigenvectors of T by inverse iteration with partial
 //      pivoting, one thread per eigenvector, seeded random starts.
-//   4. group_mgs: modified Gram-Schmidt inside groups of (numerically)
-//      degenerate eigenvalues (e.g. SU(2) multiplets), then a Newton-Schulz
-//      polar step on the whole block (GEMMs) restores orthogonality to ~eps.
+//   4. group_mgs: classical Gram-Schmidt with re-orthogonalisation inside
+//      groups of (numerically) degenerate eigenvalues (SU(2) multiplets, the
+//      tail near the noise floor), then a Newton-Schulz polar step on the whole
+//      block (GEMMs) restores orthogonality to ~eps.
 //   5. apply_q: eigenvectors of G = Q z, each CTA applying all reflectors to
 //      its own slab of columns (columns are independent).
 #include <cooperative_groups.h>
@@ -425,36 +426,86 @@ __global__ void tridiag_invit_kernel(const double* __restrict__ dg, const double
 }
 
 // ----------------------------------------------------------------------------
-// 4. Gram-Schmidt inside groups of nearly equal eigenvalues (one warp per group)
+// 4. Gram-Schmidt inside groups of nearly equal eigenvalues. One CTA per group
+//    (the CTA indexed by the group's first member; the others exit at once).
+//    The group's columns are staged transposed in shared memory (zs[q][i]) when
+//    they fit and orthonormalised by classical Gram-Schmidt with one
+//    re-orthogonalisation pass (CGS2, "twice is enough": Giraud, Langou and
+//    Rozloznik 2005). Per vector the dots with all earlier members are formed
+//    at once, one warp per earlier member, then subtracted in one pass.
 // ----------------------------------------------------------------------------
-__global__ void group_mgs_kernel(double* __restrict__ Z, int n, int K, const double* __restrict__ lam,
-                                 const SvdOut* __restrict__ tr, double gtol_rel) {
-  const int lane = threadIdx.x & 31;
-  const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+static constexpr int GS_THREADS = 256;
+static constexpr int GS_SMEM = 200 * 1024;
+
+__global__ void __launch_bounds__(GS_THREADS)
+    group_cgs_kernel(double* __restrict__ Z, int n, int K, const double* __restrict__ lam,
+                     const SvdOut* __restrict__ tr, double gtol_rel) {
+  extern __shared__ __align__(16) double gsm[];
+  __shared__ double red[GS_THREADS / 32 + 1];
+  constexpr int NW = GS_THREADS / 32;
+  const int j = blockIdx.x;
   const int kk = tr->k;
   if (j >= kk) return;
   const double gtol = gtol_rel * fmax(fabs(lam[0]), 1e-300);
   if (j > 0 && fabs(lam[j - 1] - lam[j]) <= gtol) return;  // not a group start
   int end = j + 1;
   while (end < kk && fabs(lam[end - 1] - lam[end]) <= gtol) ++end;
-  if (end - j < 2) return;
-  for (int q = j; q < end; ++q) {
-    for (int pass = 0; pass < 2; ++pass) {
-      for (int p = j; p < q; ++p) {
-        double s = 0.0;
-        for (int i = lane; i < n; i += 32) s += Z[(ll)i * K + p] * Z[(ll)i * K + q];
-        s = warp_sum_d(s);
-        for (int i = lane; i < n; i += 32) Z[(ll)i * K + q] -= s * Z[(ll)i * K + p];
-        __syncwarp();
-      }
+  const int g = end - j;
+  if (g < 2) return;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const size_t cap = GS_SMEM / sizeof(double);
+  const bool staged = (size_t)g * n + g <= cap;  // else the vectors stay in global memory
+  double* zs = gsm;
+  double* cf = gsm + (staged ? (size_t)g * n : 0);  // coefficients, g <= cap always (g <= K <= n)
+  auto at = [&](int q, int i) -> double& {
+    return staged ? zs[(ll)q * n + i] : Z[(ll)i * K + j + q];
+  };
+  if (staged)
+    for (ll e = tid; e < (ll)g * n; e += GS_THREADS) {
+      const int q = (int)(e % g), i = (int)(e / g);
+      zs[(ll)q * n + i] = Z[(ll)i * K + j + q];
     }
-    double s = 0.0;
-    for (int i = lane; i < n; i += 32) s += Z[(ll)i * K + q] * Z[(ll)i * K + q];
-    s = warp_sum_d(s);
-    const double inv = (s > 0.0) ? 1.0 / sqrt(s) : 0.0;
-    for (int i = lane; i < n; i += 32) Z[(ll)i * K + q] *= inv;
-    __syncwarp();
+  __syncthreads();
+  for (int q = 0; q < g; ++q) {
+    for (int pass = 0; pass < 2 && q > 0; ++pass) {
+      for (int p = warp; p < q; p += NW) {
+        double sum = 0.0;
+        for (int i = lane; i < n; i += 32) sum += at(p, i) * at(q, i);
+        sum = warp_sum_d(sum);
+        if (lane == 0) cf[p] = sum;
+      }
+      __syncthreads();
+      for (int i = tid; i < n; i += GS_THREADS) {
+        double v = at(q, i);
+        for (int p = 0; p < q; ++p) v -= cf[p] * at(p, i);
+        at(q, i) = v;
+      }
+      __syncthreads();
+    }
+    double sq = 0.0;
+    for (int i = tid; i < n; i += GS_THREADS) {
+      const double v = at(q, i);
+      sq += v * v;
+    }
+    sq = warp_sum_d(sq);
+    if (lane == 0) red[warp] = sq;
+    __syncthreads();
+    if (warp == 0) {
+      double t = lane < NW ? red[lane] : 0.0;
+      t = warp_sum_d(t);
+      if (lane == 0) red[NW] = t;
+    }
+    __syncthreads();
+    const double tot = red[NW];
+    const double inv = tot > 0.0 ? 1.0 / sqrt(tot) : 0.0;
+    for (int i = tid; i < n; i += GS_THREADS) at(q, i) *= inv;
+    __syncthreads();
   }
+  if (staged)
+    for (ll e = tid; e < (ll)g * n; e += GS_THREADS) {
+      const int q = (int)(e % g), i = (int)(e / g);
+      Z[(ll)i * K + j + q] = zs[(ll)q * n + i];
+    }
 }
 
 // ----------------------------------------------------------------------------
@@ -653,14 +704,10 @@ __global__ void eig_truncate_kernel(const double* __restrict__ dg, const double*
 template <typename T, bool SROWS>
 static void hetrd_launch(T* G, int n, ll ld, double* d, double* e, T* tau, int C, size_t smem,
                          cudaStream_t s, cudaError_t* err) {
-  static int attr_done = 0;
-  if (!attr_done) {
-    DMRG2_CUDA(cudaFuncSetAttribute(hetrd_cluster_kernel<T, SROWS>,
-                                    cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    DMRG2_CUDA(cudaFuncSetAttribute(hetrd_cluster_kernel<T, SROWS>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
-    attr_done = 1;
-  }
+  static std::atomic<unsigned long long> attr_cluster{0}, attr_smem{0};
+  func_attr_once(attr_cluster, (const void*)hetrd_cluster_kernel<T, SROWS>,
+                 cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  set_smem_attr_once(attr_smem, (const void*)hetrd_cluster_kernel<T, SROWS>, 220 * 1024);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(C);
   cfg.blockDim = dim3(HT_THREADS);
@@ -713,12 +760,8 @@ void tridiag_eigvals(const double* d, const double* e, int n, int K, double* lam
 void tridiag_eigvecs(const double* d, const double* e, int n, int K, const double* lam,
                      const SvdOut* tr, double* Z, double* scratch, cudaStream_t s) {
   (void)scratch;
-  static int attr_done = 0;
-  if (!attr_done) {
-    DMRG2_CUDA(cudaFuncSetAttribute(tridiag_invit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    220 * 1024));
-    attr_done = 1;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  set_smem_attr_once(attr, (const void*)tridiag_invit_kernel, 220 * 1024);
   const size_t per = sizeof(double) * 5 * (size_t)n;
   int vpb = (int)std::min<size_t>(8, (220 * 1024 - sizeof(double) * 2 * (size_t)n) / per);
   if (vpb < 1) throw std::runtime_error("inverse iteration: matrix order too large");
@@ -729,8 +772,10 @@ void tridiag_eigvecs(const double* d, const double* e, int n, int K, const doubl
 
 void group_mgs(double* Z, int n, int K, const double* lam, const SvdOut* tr, double gtol_rel,
                cudaStream_t s) {
-  const int wpb = 4;
-  group_mgs_kernel<<<(K + wpb - 1) / wpb, wpb * 32, 0, s>>>(Z, n, K, lam, tr, gtol_rel);
+  if ((size_t)K * sizeof(double) > (size_t)GS_SMEM) throw std::runtime_error("group_mgs: order too large");
+  static std::atomic<unsigned long long> attr{0};
+  set_smem_attr_once(attr, (const void*)group_cgs_kernel, GS_SMEM);
+  group_cgs_kernel<<<K, GS_THREADS, GS_SMEM, s>>>(Z, n, K, lam, tr, gtol_rel);
   DMRG2_CHECK_LAUNCH();
 }
 
@@ -756,12 +801,8 @@ void apply_q(const T* R, ll ld, const T* tau, int n, const double* Z, int K, con
   int nb = (int)std::min<size_t>(AQ_MAXNB, cap / (size_t)n > AQ_COLS ? cap / (size_t)n - AQ_COLS : 0);
   if (nb < 1) throw std::runtime_error("apply_q: matrix order too large");
   const size_t smem = sizeof(T) * (size_t)n * (AQ_COLS + nb);
-  static int attr_done = 0;
-  if (!attr_done) {
-    DMRG2_CUDA(cudaFuncSetAttribute(apply_q_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    220 * 1024));
-    attr_done = 1;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  set_smem_attr_once(attr, (const void*)apply_q_kernel<T>, 220 * 1024);
   const int nblk = (n - 1 + nb - 1) / nb;
   wy_build_kernel<T><<<nblk, 256, 0, s>>>(R, ld, tau, n, nb, Tb);
   DMRG2_CHECK_LAUNCH();

@@ -78,6 +78,8 @@ class Engine final : public EngineBase {
     red_.counter = (unsigned*)dalloc_bytes(sizeof(unsigned) * 4);
     DMRG2_CUDA(cudaMemset(red_.counter, 0, sizeof(unsigned) * 4));
     DMRG2_CUDA(cudaMallocHost(&h_svd_, sizeof(SvdOut)));
+    canon_flags_ = (int*)dalloc_bytes(sizeof(int) * (size_t)(L_ + 1));
+    DMRG2_CUDA(cudaMallocHost(&h_flags_, sizeof(int) * (size_t)(L_ + 1)));
     DMRG2_CUDA(cudaEventCreate(&ev_c_));
     DMRG2_CUDA(cudaEventCreate(&ev_d_));
     DMRG2_CUDA(cudaEventCreate(&ev_s0_));
@@ -90,6 +92,7 @@ class Engine final : public EngineBase {
     free_mpo();
     for (void* p : allocs_) cudaFree(p);
     cudaFreeHost(h_svd_);
+    cudaFreeHost(h_flags_);
     lw_.release();
     ew_.release();
     cudaEventDestroy(ev_c_);
@@ -336,9 +339,33 @@ class Engine final : public EngineBase {
   double jacobi_tol(ll len) const { return 2.2e-16 * std::max<double>(16.0, (double)len); }
 
   // ---------------------------------------------------------------- setup
+  // Highest site whose tensor is not a right isometry (A A^H = 1 to 1e-12), with every
+  // site above it one; 0 when sites 1..L-1 all are. Such sites (an MPS read back after
+  // a right-to-left half-sweep, a checkpoint) need no decomposition: A A^H = 1 makes the
+  // density matrix a projector, whose degenerate spectrum would only be rotated.
+  int first_non_isometry() {
+    for (int i = L_ - 1; i >= 1; --i) {
+      const int cl = dims_[i], nc = d_ * dims_[i + 1];
+      Gemm<T> g;  // conj(A A^H) = conj(A) A^T
+      g.ca = true; g.tb = true;
+      g.M = cl; g.N = cl; g.K = nc;
+      g.A = mps_[i]; g.lda = nc;
+      g.B = mps_[i]; g.ldb = nc;
+      g.C = theta_; g.ldc = cl;
+      launch_gemm(g, st_);
+      identity_check(theta_, cl, 1e-12, canon_flags_ + i, st_);
+    }
+    DMRG2_CUDA(cudaMemcpyAsync(h_flags_, canon_flags_, sizeof(int) * (size_t)(L_ + 1), cudaMemcpyDeviceToHost, st_));
+    DMRG2_CUDA(cudaStreamSynchronize(st_));
+    for (int i = L_ - 1; i >= 1; --i)
+      if (!h_flags_[i]) return i;
+    return 0;
+  }
+
   void right_canonicalize() {
     envs_valid_ = false;
-    for (int i = L_ - 1; i >= 1; --i) {
+    const int first = first_non_isometry();
+    for (int i = first; i >= 1; --i) {
       const int cl = dims_[i], cr = dims_[i + 1];
       const int nc = d_ * cr;
       const int chi = std::min(cfg_.chi_max, cap_[i]);
@@ -479,6 +506,8 @@ class Engine final : public EngineBase {
   double* dscal_ = nullptr;
   RedScratch red_;
   SvdOut* h_svd_ = nullptr;
+  int* canon_flags_ = nullptr;
+  int* h_flags_ = nullptr;
   cudaEvent_t ev_c_ = nullptr, ev_d_ = nullptr, ev_s0_ = nullptr, ev_s1_ = nullptr;
   bool envs_valid_ = false;
   std::vector<void*> allocs_, mpo_allocs_, tmp_allocs_;

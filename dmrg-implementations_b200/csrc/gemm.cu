@@ -42,12 +42,8 @@ template <typename T, bool TA, bool TB, bool CA>
 static void launch_impl(const Gemm<T>& d, cudaStream_t st) {
   using G = GemmTile<T>;
   using S = GemmSmem<T, TA, TB>;
-  static bool attr_set = false;  // per instantiation; set once per process
-  if (!attr_set) {
-    DMRG2_CUDA(cudaFuncSetAttribute(gemm_kernel<T, TA, TB, CA>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::BYTES));
-    attr_set = true;
-  }
+  static std::atomic<unsigned long long> attr{0};  // per instantiation, per device
+  set_smem_attr_once(attr, (const void*)gemm_kernel<T, TA, TB, CA>, (int)S::BYTES);
   GemmArgs a;
   a.M = d.M; a.N = d.N; a.K = d.K;
   a.A = d.A; a.lda = d.lda; a.sA1 = d.sA1; a.sA2 = d.sA2;

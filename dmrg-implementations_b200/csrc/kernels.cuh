@@ -118,5 +118,8 @@ template <typename T>
 void norm2(const T* x, ll n, double* out_dev, RedScratch& r, cudaStream_t s);
 template <typename T>
 void trace_real(const T* M, int n, ll ld, double* out_re, double* out_im, cudaStream_t s);
+// flag = 1 when the n x n matrix P equals the identity to tol (max |P - 1|)
+template <typename T>
+void identity_check(const T* P, int n, double tol, int* flag, cudaStream_t s);
 
 }  // namespace dmrg2

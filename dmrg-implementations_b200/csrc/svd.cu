@@ -407,6 +407,33 @@ void set_identity(T* Q, int n, cudaStream_t s) {
   DMRG2_CHECK_LAUNCH();
 }
 
+// flag[0] = 1 when max |P - 1| <= tol for the n x n matrix P (one block)
+template <typename T>
+__global__ void identity_check_kernel(const T* __restrict__ P, int n, double tol, int* __restrict__ flag) {
+  __shared__ double red[256];
+  double m = 0.0;
+  const ll tot = (ll)n * n;
+  for (ll e = threadIdx.x; e < tot; e += blockDim.x) {
+    const ll i = e / n, j = e % n;
+    const T v = P[e];
+    const double re = ST<T>::re(v) - (i == j ? 1.0 : 0.0), im = ST<T>::im(v);
+    m = fmax(m, fabs(re) + fabs(im));
+  }
+  red[threadIdx.x] = m;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *flag = (red[0] <= tol) ? 1 : 0;
+}
+
+template <typename T>
+void identity_check(const T* P, int n, double tol, int* flag, cudaStream_t s) {
+  identity_check_kernel<T><<<1, 256, 0, s>>>(P, n, tol, flag);
+  DMRG2_CHECK_LAUNCH();
+}
+
 template <typename T>
 __global__ void trace_kernel(const T* M, int n, ll ld, double* out_re, double* out_im) {
   __shared__ double sr[256], si[256];
@@ -442,7 +469,8 @@ void trace_real(const T* M, int n, ll ld, double* out_re, double* out_im, cudaSt
                               cudaStream_t);                                                     \
   template void transpose<T>(const T*, T*, ll, ll, cudaStream_t);                                \
   template void set_identity<T>(T*, int, cudaStream_t);                                          \
-  template void trace_real<T>(const T*, int, ll, double*, double*, cudaStream_t);
+  template void trace_real<T>(const T*, int, ll, double*, double*, cudaStream_t);                \
+  template void identity_check<T>(const T*, int, double, int*, cudaStream_t);
 INST(double)
 INST(zc)
 #undef INST

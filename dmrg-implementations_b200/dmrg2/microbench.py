@@ -1,0 +1,101 @@
+"""Timing of single sweep primitives on one GPU, on seeded random operands.
+
+    python -m dmrg2.microbench heff --chi 256 [--d 2 --D 5 --complex --reps 50]
+    python -m dmrg2.microbench svd  --n 512   [--keep 256 --complex --reps 5]
+
+heff runs dmrg2_op_heff_noalloc on device-resident operands (torch tensors)
+and reports the device time per matvec (CUDA events) and its algorithmic
+TFLOP/s; svd runs the truncated split through dmrg2_op_svd (host buffers,
+so the time includes the copies). Both are the fixed small workloads the
+kernel profiles are taken on.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import time
+
+import numpy as np
+
+import dmrg2
+
+
+def heff_flops(cL, cR, d, D, cplx):
+    dd = d * d
+    f = 2.0 * D * cL * dd * cR * cL + 2.0 * cL * dd * D * cR * D * dd + 2.0 * cL * dd * cR * D * cR
+    return 4.0 * f if cplx else f
+
+
+def _rnd(rng, shape, cplx):
+    x = rng.standard_normal(shape)
+    return x + 1j * rng.standard_normal(shape) if cplx else x
+
+
+def bench_heff(chi, d, D, cplx, reps, seed=0):
+    import torch
+
+    rng = np.random.default_rng(seed)
+    lib = dmrg2.load_library()
+    code = dmrg2.C128 if cplx else dmrg2.F64
+    host = [_rnd(rng, s, cplx) for s in ((chi, D, chi), (chi, D, chi), (D, D, d, d), (D, D, d, d), (chi, d, d, chi))]
+    L, R, WL, WR, th = (torch.from_numpy(a).cuda() for a in host)
+    out = torch.empty_like(th)
+    stream = torch.cuda.current_stream()
+    p = lambda t: ctypes.c_void_p(t.data_ptr())
+
+    def call():
+        rc = lib.dmrg2_op_heff_noalloc(code, chi, chi, d, D, D, D, p(L), p(R), p(WL), p(WR), p(th), p(out),
+                                       ctypes.c_void_p(stream.cuda_stream))
+        if rc != 0:
+            raise RuntimeError(lib.dmrg2_last_error(None).decode())
+
+    for _ in range(3):
+        call()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        call()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) * 1e-3 / reps
+    fl = heff_flops(chi, chi, d, D, cplx)
+    return {"op": "heff", "chi": chi, "d": d, "D": D, "complex": cplx, "us_per_matvec": t * 1e6,
+            "gflop_per_matvec": fl / 1e9, "tflops": fl / t / 1e12}
+
+
+def bench_svd(n, keep, cplx, reps, seed=0):
+    rng = np.random.default_rng(seed)
+    U, _ = np.linalg.qr(_rnd(rng, (n, n), cplx))
+    V, _ = np.linalg.qr(_rnd(rng, (n, n), cplx))
+    s = np.exp(-0.05 * np.arange(n))
+    M = (U * s) @ V.conj().T
+    times = []
+    for _ in range(reps + 1):
+        t = time.perf_counter()
+        dmrg2.truncated_svd(M, keep, 1e-12, "R")
+        times.append(time.perf_counter() - t)
+    return {"op": "svd", "n": n, "keep": keep, "complex": cplx, "ms_per_call_host": 1e3 * float(np.median(times[1:]))}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("op", choices=["heff", "svd"])
+    ap.add_argument("--chi", type=int, default=256)
+    ap.add_argument("--d", type=int, default=2)
+    ap.add_argument("--D", type=int, default=5)
+    ap.add_argument("--n", type=int, default=512)
+    ap.add_argument("--keep", type=int, default=0)
+    ap.add_argument("--complex", action="store_true")
+    ap.add_argument("--reps", type=int, default=0)
+    a = ap.parse_args()
+    if a.op == "heff":
+        r = bench_heff(a.chi, a.d, a.D, a.complex, a.reps or 50)
+    else:
+        r = bench_svd(a.n, a.keep or a.n // 2, a.complex, a.reps or 5)
+    print(json.dumps(r))
+
+
+if __name__ == "__main__":
+    main()

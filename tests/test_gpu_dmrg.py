@@ -170,3 +170,23 @@ def test_cli_known_answers(args, expect, tmp_path):
     assert "timer_scope: sweep_only" in r.stdout
     row = json.loads(out.read_text())["results"][0]
     assert row["arch"] == "b200" and row["success"] and abs(row["energy"] - expect) < 1e-8
+
+
+def test_resume_from_right_canonical_mps_readback():
+    """An MPS read back after a run (right-canonical sites 1..L-1) restarts without
+    re-decomposing those sites and continues at the same energy; a perturbed site
+    forces the decomposition from that site down and still converges back."""
+    L = 16
+    mpo = M.heisenberg_mpo(L)
+    eng, rep = gpu_run(mpo, O.random_mps(L, 2, 8, seed=4), [32] * 8, krylov_max=30, max_restarts=4)
+    A = eng.get_mps()
+    for k in range(1, L):
+        a = A[k].reshape(A[k].shape[0], -1)
+        np.testing.assert_allclose(a @ a.conj().T, np.eye(a.shape[0]), atol=1e-12)
+    eng2, rep2 = gpu_run(mpo, A, [32] * 2, krylov_max=30, max_restarts=4)
+    assert eng2.bond_dims() == eng.bond_dims()
+    assert abs(rep2[-1]["energy"] - rep[-1]["energy"]) <= 1e-10 * abs(rep[-1]["energy"])
+    B = [a.copy() for a in A]
+    B[L // 2] = B[L // 2] * 1.5 + 1e-3 * np.random.default_rng(1).standard_normal(B[L // 2].shape)
+    eng3, rep3 = gpu_run(mpo, B, [32] * 6, krylov_max=30, max_restarts=4)
+    assert abs(rep3[-1]["energy"] - rep[-1]["energy"]) <= 1e-10 * abs(rep[-1]["energy"])

@@ -193,6 +193,27 @@ def test_svd_degenerate_spectrum(method):
 
 
 @pytest.mark.parametrize("cplx", [False, True])
+@pytest.mark.parametrize("cluster", [40, 64])
+def test_svd_large_degenerate_cluster(cplx, cluster):
+    # one group of `cluster` equal singular values at order 512: 40 members are
+    # orthogonalised in shared memory, 64 members (64 x 512 doubles) in global memory
+    rng = np.random.default_rng(21 + cluster + cplx)
+    n = 512
+    Q1, _ = np.linalg.qr(rnd(rng, (n, n), cplx))
+    Q2, _ = np.linalg.qr(rnd(rng, (n, n), cplx))
+    s = np.concatenate([[1.0, 0.7, 0.5, 0.3], np.full(cluster, 0.05),
+                        np.geomspace(1e-2, 1e-6, n - 4 - cluster)])
+    M = (Q1 * s) @ Q2.conj().T
+    keep = cluster + 36
+    for direction in ("R", "L"):
+        left, S, right, te = dmrg2.truncated_svd(M, keep, 0.0, direction)
+        np.testing.assert_allclose(S[:keep] ** 2, s[:keep] ** 2, atol=1e-14)
+        close(left @ right, (Q1[:, :keep] * s[:keep]) @ Q2[:, :keep].conj().T, 1e-9)
+        iso = left.conj().T @ left if direction == "R" else right @ right.conj().T
+        np.testing.assert_allclose(iso, np.eye(keep), atol=1e-12)
+
+
+@pytest.mark.parametrize("cplx", [False, True])
 def test_lanczos_vs_dense(cplx):
     rng = np.random.default_rng(3 + cplx)
     cL, cR, d, D = 6, 7, 2, 3
