@@ -236,6 +236,264 @@ __global__ void __launch_bounds__(HT_THREADS)
 }
 
 // ----------------------------------------------------------------------------
+// 1b. Real symmetric G of order n <= 512: the same reduction with the trailing
+//     matrix held in registers. Row r belongs to CTA r % C (local row q = r / C)
+//     and, inside it, to warp q % 16 (slot q / 16 < RW); lane l holds columns
+//     j = l + 32 t, t < NT. Column k's step is one fused pass per warp: with p
+//     and column k+1 pulled from the owners, each warp forms v, w and the next
+//     column x' = column k+1 - (v w^T + w v^T)[:, k+1] for its lane's columns,
+//     applies the rank-2 update to its rows and, in the same pass, accumulates
+//     the next step's symv sum_j G'[r][j] x'[j] (the reflector of x' only
+//     scales it, and every warp derives that reflector itself from x'). Per
+//     column: one CTA barrier after the pull and one cluster barrier after the
+//     owners publish p', column k+2 and the partial sums of s' = p'^T v'.
+// ----------------------------------------------------------------------------
+__device__ inline void house_real(double alpha, double xn2, double& tk, double& sc, double& beta) {
+  if (xn2 == 0.0) {
+    tk = 0.0;
+    sc = 0.0;
+    beta = alpha;
+  } else {
+    beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+    const double ib = 1.0 / beta;
+    tk = (beta - alpha) * ib;
+    const double dr = alpha - beta;
+    sc = dr * (1.0 / (dr * dr));  // 1 / (alpha - beta)
+  }
+}
+
+template <int NT, int RW, int C>
+__global__ void __launch_bounds__(HT_THREADS, 1)
+    hetrd_reg_kernel(double* __restrict__ G, int n, ll ld, double* __restrict__ dg,
+                     double* __restrict__ eg, double* __restrict__ tau) {
+  static_assert((C & (C - 1)) == 0 && C <= 32, "cluster size: power of two <= 32");
+  cg::cluster_group cluster = cg::this_cluster();
+  constexpr int lgC = (C >= 32) ? 5 : (C >= 16) ? 4 : (C >= 8) ? 3 : (C >= 4) ? 2 : (C >= 2) ? 1 : 0;
+  const int rank = (int)cluster.block_rank();
+  constexpr int NW = HT_THREADS / 32;
+  extern __shared__ __align__(16) double hsm[];
+  // pulled p and column k+1 are kept owner-major, padded: row r at pidx(r)
+  const int Q = (n + C - 1) >> lgC;  // rows per CTA
+  auto pidx = [&](int r) { return (r & (C - 1)) * (Q + 1) + (r >> lgC); };
+  double* pf = hsm;                   // p of this step, all rows (pulled)
+  double* cf = pf + C * (Q + 1);      // column k+1 before this step, all rows (pulled)
+  double* xs0 = cf + C * (Q + 1);     // column k (parity buffers)
+  double* xs1 = xs0 + n;
+  double* po0 = xs1 + n;  // own p entries by local row r / C (parity buffers)
+  double* po1 = po0 + n;
+  double* co0 = po1 + n;  // own column entries (parity buffers)
+  double* co1 = co0 + n;
+  double* sp0 = co1 + n;  // per-warp partial s (parity buffers, NW each)
+  double* sp1 = sp0 + NW;
+  double* sall = sp1 + NW;  // all C * NW partials of s, pulled
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+  int rr[RW];
+  double g[RW][NT];
+#pragma unroll
+  for (int i = 0; i < RW; ++i) {
+    rr[i] = (warp + NW * i) * C + rank;
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+      const int j = lane + 32 * t;
+      g[i][t] = (rr[i] < n && j < n) ? G[(ll)rr[i] * ld + j] : 0.0;
+    }
+  }
+  // ---- prologue: column 0 (row 0 by symmetry), its reflector, the first symv
+  for (int j = tid; j < n; j += HT_THREADS) xs0[j] = G[j];
+  __syncthreads();
+  double tk, sc, beta;
+  {
+    double xn2 = 0.0;
+    for (int j = 2 + lane; j < n; j += 32) xn2 += xs0[j] * xs0[j];
+    xn2 = warp_sum_d(xn2);
+    house_real(xs0[1], xn2, tk, sc, beta);
+    if (rank == 0 && tid == 0) {
+      dg[0] = xs0[0];
+      eg[0] = beta;
+      tau[0] = tk;
+    }
+    double sp = 0.0;
+#pragma unroll
+    for (int i = 0; i < RW; ++i) {
+      const int r = rr[i];
+      double acc = 0.0;
+#pragma unroll
+      for (int t = 0; t < NT; ++t) {
+        const int j = lane + 32 * t;
+        if (j >= 2 && j < n) acc += g[i][t] * xs0[j];
+      }
+      acc = warp_sum_d(acc);
+      const double c1 = __shfl_sync(0xffffffffu, g[i][0], 1);
+      if (r >= 1 && r < n) {
+        const double p = tk * (c1 + sc * acc);
+        if (lane == 0) {
+          po0[r >> lgC] = p;
+          co0[r >> lgC] = c1;
+        }
+        sp += p * ((r == 1) ? 1.0 : xs0[r] * sc);
+      }
+    }
+    if (lane == 0) sp0[warp] = sp;
+  }
+  cluster.sync();  // all rows loaded (rank 0 overwrites row k from step k on), step-0 data published
+
+  for (int k = 0; k < n - 1; ++k) {
+    const int par = k & 1;
+    const double* po = par ? po1 : po0;
+    const double* co = par ? co1 : co0;
+    const double* spr = par ? sp1 : sp0;
+    const double* xs = par ? xs1 : xs0;
+    double* pon = par ? po0 : po1;
+    double* con = par ? co0 : co1;
+    double* spn = par ? sp0 : sp1;
+    double* xsn = par ? xs0 : xs1;
+    // (1) pull p and column k+1 from the row owners and every partial of s (one remote
+    //     load per thread and array, all in flight together)
+    {  // thread -> (owner c, local row q): a warp reads consecutive entries of one owner
+      const int c = tid / Q, q = tid - c * Q;
+      const int r = (q << lgC) + c;
+      if (c < C && r >= k + 1 && r < n) {
+        pf[c * (Q + 1) + q] = cluster.map_shared_rank(po, c)[q];
+        cf[c * (Q + 1) + q] = cluster.map_shared_rank(co, c)[q];
+      }
+    }
+    if (tid < C * NW) sall[tid] = cluster.map_shared_rank(spr, tid / NW)[tid % NW];
+    __syncthreads();
+    double ssum = 0.0;
+    for (int q = lane; q < C * NW; q += 32) ssum += sall[q];
+    ssum = warp_sum_d(ssum);
+    // (2) w = p - tau s / 2 v; fused rank-2 update + next symv + next column
+    const double a2 = -0.5 * tk * ssum;
+    const double wk1 = pf[pidx(k + 1)] + a2;  // v[k+1] = 1
+    double vr[RW], wr[RW], acc[RW], c2[RW];
+    bool act[RW];
+#pragma unroll
+    for (int i = 0; i < RW; ++i) {
+      const int r = rr[i];
+      vr[i] = 0.0;
+      wr[i] = 0.0;
+      act[i] = (r >= k + 1 && r < n);
+      if (act[i]) {
+        vr[i] = (r == k + 1) ? 1.0 : xs[r] * sc;
+        wr[i] = pf[pidx(r)] + a2 * vr[i];
+      }
+      acc[i] = 0.0;
+      c2[i] = 0.0;
+    }
+    double nrm = 0.0, a_next = 0.0, d_next = 0.0;
+    const bool store_v = (rank == 0);
+    // column chunks t < tb lie left of the active block; chunks tb and tb + 1 hold
+    // columns k+1 and k+2 and take the checked path, as does a ragged last chunk
+    const int tb = (k + 1) >> 5;
+    const int pl = (lane & (C - 1)) * (Q + 1) + (lane >> lgC);  // pidx(lane); + t * 32 / C per chunk
+    auto chunk = [&](const int t, const bool edge) {
+      const int j = lane + 32 * t;
+      if (edge && !(j >= k + 1 && j < n)) return;
+      const int pj = pl + t * (32 / C);
+      const double vj = (edge && j == k + 1) ? 1.0 : xs[j] * sc;
+      const double wj = pf[pj] + a2 * vj;
+      const double xn = cf[pj] - vj * wk1 - wj;
+      if (!edge || j >= k + 3) nrm += xn * xn;
+      if (edge && j == k + 2) a_next = xn;
+      if (edge && j == k + 1) d_next = xn;
+      if (t % NW == warp) {  // one warp per column chunk publishes x' and the reflector
+        xsn[j] = xn;
+        if (store_v) G[(ll)k * ld + j] = vj;
+      }
+#pragma unroll
+      for (int i = 0; i < RW; ++i) {
+        if (act[i]) {
+          const double gg = g[i][t] - vr[i] * wj - wr[i] * vj;
+          g[i][t] = gg;
+          if (!edge || j >= k + 3) acc[i] += gg * xn;
+          if (edge && j == k + 2) c2[i] = gg;
+        }
+      }
+    };
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+      if (t < tb || 32 * t >= n) continue;
+      if (t <= tb + 1 || 32 * t + 32 > n) chunk(t, true);
+      else chunk(t, false);
+    }
+    // (3) next reflector (every warp derives the same one), publish p', column k+2, s'
+    nrm = warp_sum_d(nrm);
+    a_next = __shfl_sync(0xffffffffu, a_next, (k + 2) & 31);
+    d_next = __shfl_sync(0xffffffffu, d_next, (k + 1) & 31);
+    double tk2 = 0.0, sc2 = 0.0, beta2 = 0.0;
+    if (k + 2 <= n - 1) house_real(a_next, nrm, tk2, sc2, beta2);
+    if (rank == 0 && tid == 32) {
+      dg[k + 1] = d_next;
+      eg[k + 1] = beta2;
+      if (k + 1 < n - 1) tau[k + 1] = tk2;
+    }
+    double sp = 0.0;
+#pragma unroll
+    for (int i = 0; i < RW; ++i) {
+      const int r = rr[i];
+      const double a = warp_sum_d(acc[i]);
+      const double c = __shfl_sync(0xffffffffu, c2[i], (k + 2) & 31);
+      if (r >= k + 2 && r < n) {
+        const double p = tk2 * (c + sc2 * a);
+        if (lane == 0) {
+          pon[r >> lgC] = p;
+          con[r >> lgC] = c;
+        }
+        const double xnr = cf[pidx(r)] - vr[i] * wk1 - wr[i];
+        sp += p * ((r == k + 2) ? 1.0 : xnr * sc2);
+      }
+    }
+    if (lane == 0) spn[warp] = sp;
+    tk = tk2;
+    sc = sc2;
+    cluster.sync();
+  }
+}
+
+template <int NT, int RW, int C>
+static cudaError_t hetrd_reg_launch(double* G, int n, ll ld, double* d, double* e, double* tau,
+                                    cudaStream_t s) {
+  static std::atomic<unsigned long long> attr_cluster{0};
+  func_attr_once(attr_cluster, (const void*)hetrd_reg_kernel<NT, RW, C>,
+                 cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(C);
+  cfg.blockDim = dim3(HT_THREADS);
+  const int Q = (n + C - 1) / C;
+  cfg.dynamicSmemBytes = sizeof(double) * ((size_t)2 * C * (Q + 1) + 6 * (size_t)n + 2 * (HT_THREADS / 32) +
+                                           16 * (HT_THREADS / 32));
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, hetrd_reg_kernel<NT, RW, C>, G, n, ld, d, e, tau);
+}
+
+// register-resident reduction for real G with 32 <= n <= 512; false when the device
+// refused the cluster (the caller then takes the shared-memory kernel)
+static bool hetrd_reg(double* G, int n, ll ld, double* d, double* e, double* tau, cudaStream_t s) {
+  static std::atomic<int> refused{0};
+  if (n < 32 || n > 512 || refused.load()) return false;
+  cudaError_t err;
+  if (n <= 128) err = hetrd_reg_launch<4, 1, 8>(G, n, ld, d, e, tau, s);
+  else if (n <= 256) err = hetrd_reg_launch<8, 1, 16>(G, n, ld, d, e, tau, s);
+  else err = hetrd_reg_launch<16, 2, 16>(G, n, ld, d, e, tau, s);
+  if (err == cudaSuccess) return true;
+  if (err == cudaErrorInvalidClusterSize || err == cudaErrorLaunchOutOfResources || err == cudaErrorInvalidValue) {
+    (void)cudaGetLastError();
+    refused.store(1);
+    return false;
+  }
+  DMRG2_CUDA(err);
+  return false;
+}
+
+// ----------------------------------------------------------------------------
 // 2. K largest eigenvalues of (d, e) by Sturm-count multisection, one CTA per
 //    eigenvalue (blockDim+1 points per round)
 // ----------------------------------------------------------------------------
@@ -725,6 +983,12 @@ static void hetrd_launch(T* G, int n, ll ld, double* d, double* e, T* tau, int C
 
 template <typename T>
 void hetrd_cluster(T* G, int n, ll ld, double* d, double* e, T* tau, cudaStream_t s) {
+  if constexpr (!ST<T>::cplx) {
+    if (hetrd_reg((double*)G, n, ld, d, e, (double*)tau, s)) {
+      ++launch_counter();
+      return;
+    }
+  }
   const size_t base = sizeof(T) * ((size_t)9 * n + 34);
   if (base > 200 * 1024) throw std::runtime_error("hetrd: matrix order too large for one cluster");
   int C = 16;
