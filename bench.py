@@ -338,6 +338,12 @@ def run_ours(args):
                      "peak_source": "cuBLAS DGEMM 8192^3 (torch.matmul float64) measured in this run; "
                                     "MEASURED_PEAKS.json has no FP64 figure"},
         "time_share": {"heff": heff_s / dev, "svd": svd_s / dev, "other": max(0.0, 1 - (heff_s + svd_s) / dev)},
+        "dominant_kernel": {"name": "density-matrix truncation (Gram GEMM, cluster tridiagonalisation, bisection, "
+                                    "inverse iteration, back-transform)",
+                            "share": svd_s / dev, "bound": "latency",
+                            "ms_per_bond": 1e3 * svd_s / max(1, n_sw * 2 * (L_SITES - 1)),
+                            "note": "n_g - 1 dependent Householder steps per bond (n_g = 512 at chi = 256), "
+                                    "one cluster barrier each; no bandwidth or tensor roofline applies"},
         "matvecs_per_bond": mv_per_bond,
         "cpu_baseline": {"value": cpu_value, "unit": "sweeps/s", "cores": cpu_threads(), "kind": "port",
                          "sample": f"oracle apply_heff/truncated_svd/update_left_env timed at the bond shapes "

@@ -1,6 +1,12 @@
 // extern "C" boundary of the engine (declared in include/dmrg2_b200.h).
+#include <chrono>
+#include <condition_variable>
 #include <cstring>
+#include <deque>
 #include <functional>
+#include <map>
+#include <mutex>
+#include <thread>
 #include <memory>
 #include <random>
 #include <string>
@@ -278,6 +284,25 @@ void do_op_gemm(int ta, int tb, int M, int N, int K, const double* alpha, const 
 void check_dtype(int dt) {
   if (dt != DMRG2_F64 && dt != DMRG2_C128) throw std::invalid_argument("unknown dtype");
 }
+
+// dmrg2_config -> engine configuration (fields at 0 take the reference defaults)
+EngineConfig engine_config(const dmrg2_config* cfg) {
+  EngineConfig c;
+  c.L = cfg->L;
+  c.d = cfg->d;
+  c.chi_max = cfg->chi_max;
+  c.complex = cfg->dtype == DMRG2_C128;
+  c.tol = cfg->tol > 0 ? cfg->tol : 1e-10;
+  c.krylov_max = cfg->krylov_max > 0 ? cfg->krylov_max : 100;
+  c.lanczos_tol = cfg->lanczos_tol > 0 ? cfg->lanczos_tol : 1e-12;
+  c.max_restarts = cfg->max_restarts > 0 ? cfg->max_restarts : 0;
+  c.cutoff = cfg->cutoff > 0 ? cfg->cutoff : (cfg->cutoff < 0 ? 0.0 : 1e-14);
+  c.min_sweeps = cfg->min_sweeps > 0 ? cfg->min_sweeps : 2;
+  c.seed = (unsigned)(cfg->seed ^ (cfg->seed >> 32));
+  if (cfg->svd_method != 0 && cfg->svd_method != 1) throw std::invalid_argument("unknown svd_method");
+  c.svd_method = cfg->svd_method;
+  return c;
+}
 void check_pos(std::initializer_list<int> v) {
   for (int x : v)
     if (x < 1) throw std::invalid_argument("dimensions must be positive");
@@ -299,20 +324,7 @@ int dmrg2_create(const dmrg2_config* cfg, dmrg2_handle** out) {
     check_pos({cfg->L, cfg->d, cfg->chi_max});
     if (cfg->L < 2) throw std::invalid_argument("L must be >= 2");
     DMRG2_CUDA(cudaSetDevice(cfg->device));
-    EngineConfig c;
-    c.L = cfg->L;
-    c.d = cfg->d;
-    c.chi_max = cfg->chi_max;
-    c.complex = cfg->dtype == DMRG2_C128;
-    c.tol = cfg->tol > 0 ? cfg->tol : 1e-10;
-    c.krylov_max = cfg->krylov_max > 0 ? cfg->krylov_max : 100;
-    c.lanczos_tol = cfg->lanczos_tol > 0 ? cfg->lanczos_tol : 1e-12;
-    c.max_restarts = cfg->max_restarts > 0 ? cfg->max_restarts : 0;
-    c.cutoff = cfg->cutoff > 0 ? cfg->cutoff : (cfg->cutoff < 0 ? 0.0 : 1e-14);
-    c.min_sweeps = cfg->min_sweeps > 0 ? cfg->min_sweeps : 2;
-    c.seed = (unsigned)(cfg->seed ^ (cfg->seed >> 32));
-    if (cfg->svd_method != 0 && cfg->svd_method != 1) throw std::invalid_argument("unknown svd_method");
-    c.svd_method = cfg->svd_method;
+    const EngineConfig c = engine_config(cfg);
     std::unique_ptr<dmrg2_handle> h(new dmrg2_handle);
     h->cfg = c;
     h->dtype = cfg->dtype;
@@ -468,7 +480,7 @@ int dmrg2_resume(dmrg2_handle* h, const int* chi_schedule, int n_sweeps, dmrg2_s
   });
 }
 
-long long dmrg2_get_launch_count(void) { return launch_counter(); }
+long long dmrg2_get_launch_count(void) { return launch_counter().load(); }
 
 int dmrg2_get_energy(const dmrg2_handle* h, double* e) {
   if (!h || !e) return DMRG2_ERR_ARG;
@@ -620,6 +632,228 @@ int dmrg2_op_heff_noalloc(int dtype, int cL, int cR, int d, int Dl, int Dm, int 
       heff_noalloc<double>(cL, cR, d, Dl, Dm, Dr, (const double*)L, (const double*)R, (const double*)WL,
                            (const double*)WR, (const double*)theta, (double*)out, s);
   });
+}
+
+}  // extern "C"
+
+// ============================================================================
+// Served / batched form. Requests are copied at submit, admitted in arrival
+// order while a worker slot is idle and their device footprint fits in the
+// budget, and solved by the worker that admitted them, each on its own engine
+// and CUDA stream, so the kernels of different solves overlap on the device.
+// ============================================================================
+namespace {
+
+struct ServedRequest {
+  long long id = 0;
+  dmrg2_config cfg{};
+  std::vector<std::vector<char>> W;
+  std::vector<int> Dl, Dr;
+  std::vector<std::vector<char>> A;
+  std::vector<int> dims;
+  int init_kind = DMRG2_INIT_RANDOM;
+  std::vector<int> schedule;
+  dmrg2_result res{};
+};
+
+void set_message(dmrg2_result& r, const std::string& m) {
+  std::strncpy(r.message, m.c_str(), sizeof(r.message) - 1);
+  r.message[sizeof(r.message) - 1] = 0;
+}
+
+}  // namespace
+
+struct dmrg2_server {
+  int device = 0;
+  int max_active = 8;
+  size_t budget = 0;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<ServedRequest*> queue;
+  std::map<long long, std::unique_ptr<ServedRequest>> reqs;
+  size_t reserved = 0;
+  int active = 0;
+  bool stop = false;
+  long long next_id = 1;
+  std::vector<std::thread> workers;
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+
+  double now() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
+
+  void worker() {
+    (void)cudaSetDevice(device);
+    for (;;) {
+      ServedRequest* r = nullptr;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv_work.wait(lk, [&] {
+          return stop || (!queue.empty() && reserved + queue.front()->res.footprint_bytes <= budget);
+        });
+        if (stop) return;
+        r = queue.front();
+        queue.pop_front();
+        reserved += r->res.footprint_bytes;
+        ++active;
+        r->res.state = DMRG2_REQ_RUNNING;
+        r->res.t_admit = now();
+      }
+      solve(r);
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        reserved -= r->res.footprint_bytes;
+        --active;
+        r->res.t_done = now();
+        r->res.state = r->res.status == DMRG2_OK ? DMRG2_REQ_DONE : DMRG2_REQ_FAILED;
+      }
+      cv_done.notify_all();
+      cv_work.notify_all();
+    }
+  }
+
+  // one solve through the public entry points, on this worker's own handle
+  static void solve(ServedRequest* r) {
+    dmrg2_handle* h = nullptr;
+    int rc = dmrg2_create(&r->cfg, &h);
+    const int L = r->cfg.L;
+    if (rc == DMRG2_OK) {
+      std::vector<const void*> w(L);
+      for (int i = 0; i < L; ++i) w[i] = r->W[i].data();
+      rc = dmrg2_set_mpo(h, w.data(), r->Dl.data(), r->Dr.data(), DMRG2_LAYOUT_ROWMAJOR);
+    }
+    if (rc == DMRG2_OK) {
+      if (!r->A.empty()) {
+        std::vector<const void*> a(L);
+        for (int i = 0; i < L; ++i) a[i] = r->A[i].data();
+        rc = dmrg2_set_mps(h, a.data(), r->dims.data(), DMRG2_LAYOUT_ROWMAJOR);
+      } else {
+        rc = dmrg2_init_mps(h, r->init_kind, r->cfg.seed);
+      }
+    }
+    std::vector<dmrg2_sweep_report> rep(r->schedule.size());
+    int n_out = 0;
+    if (rc == DMRG2_OK)
+      rc = dmrg2_run(h, r->schedule.data(), (int)r->schedule.size(), rep.data(), (int)rep.size(), &n_out);
+    if (rc == DMRG2_OK && n_out > 0) {
+      const dmrg2_sweep_report& last = rep[(size_t)std::min<int>(n_out, (int)rep.size()) - 1];
+      r->res.energy = last.energy;
+      r->res.sweeps = n_out;
+      r->res.trunc_err_max = last.trunc_err_max;
+      r->res.max_bond = last.max_bond;
+      for (int i = 0; i < std::min<int>(n_out, (int)rep.size()); ++i) r->res.device_s += rep[i].device_s;
+    } else if (rc != DMRG2_OK) {
+      set_message(r->res, dmrg2_last_error(h));
+    }
+    r->res.status = rc;
+    if (h) dmrg2_destroy(h);
+  }
+};
+
+extern "C" {
+
+int dmrg2_server_create(const dmrg2_server_config* cfg, dmrg2_server** out) {
+  if (!cfg || !out) { g_err = "null argument"; return DMRG2_ERR_ARG; }
+  *out = nullptr;
+  return guarded(nullptr, [&] {
+    if (cfg->max_active < 0) throw std::invalid_argument("server: max_active must be >= 0");
+    DMRG2_CUDA(cudaSetDevice(cfg->device));
+    std::unique_ptr<dmrg2_server> s(new dmrg2_server);
+    s->device = cfg->device;
+    s->max_active = cfg->max_active > 0 ? cfg->max_active : 8;
+    size_t budget = cfg->hbm_budget_bytes;
+    if (budget == 0) {
+      size_t fr = 0, tot = 0;
+      DMRG2_CUDA(cudaMemGetInfo(&fr, &tot));
+      budget = fr / 10 * 9;
+    }
+    s->budget = budget;
+    dmrg2_server* raw = s.get();
+    for (int i = 0; i < s->max_active; ++i) s->workers.emplace_back([raw] { raw->worker(); });
+    *out = s.release();
+  });
+}
+
+int dmrg2_server_submit(dmrg2_server* s, const dmrg2_request* q, long long* id) {
+  if (!s || !q || !id) { g_err = "null argument"; return DMRG2_ERR_ARG; }
+  return guarded(nullptr, [&] {
+    const dmrg2_config& c = q->cfg;
+    check_dtype(c.dtype);
+    check_pos({c.L, c.d, c.chi_max, q->n_sweeps});
+    if (c.L < 2) throw std::invalid_argument("L must be >= 2");
+    if (!q->W || !q->Dl || !q->Dr || !q->schedule) throw std::invalid_argument("submit: null MPO or schedule");
+    std::unique_ptr<ServedRequest> r(new ServedRequest);
+    r->cfg = c;
+    r->cfg.device = s->device;
+    const int L = c.L, d = c.d;
+    const size_t sb = scalar_bytes(c.dtype);
+    r->Dl.assign(q->Dl, q->Dl + L);
+    r->Dr.assign(q->Dr, q->Dr + L);
+    r->W.resize(L);
+    for (int i = 0; i < L; ++i) {
+      if (r->Dl[i] < 1 || r->Dr[i] < 1) throw std::invalid_argument("submit: MPO bonds must be positive");
+      const size_t b = (size_t)r->Dl[i] * r->Dr[i] * d * d * sb;
+      r->W[i].assign((const char*)q->W[i], (const char*)q->W[i] + b);
+    }
+    if (q->A) {
+      if (!q->bond_dims) throw std::invalid_argument("submit: MPS without bond dimensions");
+      r->dims.assign(q->bond_dims, q->bond_dims + L + 1);
+      r->A.resize(L);
+      for (int i = 0; i < L; ++i) {
+        const size_t b = (size_t)r->dims[i] * d * r->dims[i + 1] * sb;
+        r->A[i].assign((const char*)q->A[i], (const char*)q->A[i] + b);
+      }
+    }
+    r->init_kind = q->init_kind;
+    r->schedule.assign(q->schedule, q->schedule + q->n_sweeps);
+    for (int x : r->schedule)
+      if (x < 1 || x > c.chi_max) throw std::invalid_argument("submit: schedule entry outside [1, chi_max]");
+    r->res.footprint_bytes = engine_footprint(engine_config(&c), r->Dl, r->Dr);
+    if (r->res.footprint_bytes > s->budget)
+      throw std::invalid_argument("submit: request needs " + std::to_string(r->res.footprint_bytes) +
+                                  " device bytes, above the server budget of " + std::to_string(s->budget));
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      if (s->stop) throw std::logic_error("submit: server is shutting down");
+      r->id = s->next_id++;
+      r->res.state = DMRG2_REQ_QUEUED;
+      r->res.t_submit = s->now();
+      *id = r->id;
+      s->queue.push_back(r.get());
+      s->reqs[r->id] = std::move(r);
+    }
+    s->cv_work.notify_one();
+  });
+}
+
+int dmrg2_server_poll(dmrg2_server* s, long long id, int wait_ms, dmrg2_result* out) {
+  if (!s || !out) { g_err = "null argument"; return DMRG2_ERR_ARG; }
+  return guarded(nullptr, [&] {
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) throw std::invalid_argument("poll: unknown request id");
+    ServedRequest* r = it->second.get();
+    auto finished = [&] { return r->res.state == DMRG2_REQ_DONE || r->res.state == DMRG2_REQ_FAILED; };
+    if (wait_ms < 0) s->cv_done.wait(lk, finished);
+    else if (wait_ms > 0) s->cv_done.wait_for(lk, std::chrono::milliseconds(wait_ms), finished);
+    *out = r->res;
+  });
+}
+
+void dmrg2_server_destroy(dmrg2_server* s) {
+  if (!s) return;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+    for (ServedRequest* r : s->queue) {
+      r->res.state = DMRG2_REQ_FAILED;
+      r->res.status = DMRG2_ERR_STATE;
+      set_message(r->res, "server destroyed before admission");
+    }
+    s->queue.clear();
+  }
+  s->cv_work.notify_all();
+  for (auto& t : s->workers) t.join();  // running solves finish first
+  s->cv_done.notify_all();
+  delete s;
 }
 
 }  // extern "C"

@@ -76,7 +76,7 @@ struct CudaError : public std::runtime_error {
 
 // Every kernel launch of the library goes through DMRG2_CHECK_LAUNCH, which
 // also counts it (reported through dmrg2_get_launch_count).
-long long& launch_counter();
+std::atomic<long long>& launch_counter();  // kernels launched by this library (all threads)
 #define DMRG2_CHECK_LAUNCH()            \
   do {                                  \
     DMRG2_CUDA(cudaGetLastError());     \

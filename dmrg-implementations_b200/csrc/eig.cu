@@ -684,8 +684,9 @@ __global__ void tridiag_invit_kernel(const double* __restrict__ dg, const double
 }
 
 // ----------------------------------------------------------------------------
-// 4. Gram-Schmidt inside groups of nearly equal eigenvalues. One CTA per group
-//    (the CTA indexed by the group's first member; the others exit at once).
+// 4. Gram-Schmidt inside groups of nearly equal eigenvalues. Each CTA takes
+//    candidate group starts j = blockIdx.x + m * gridDim.x and skips those
+//    that do not start a group of two or more.
 //    The group's columns are staged transposed in shared memory (zs[q][i]) when
 //    they fit and orthonormalised by classical Gram-Schmidt with one
 //    re-orthogonalisation pass (CGS2, "twice is enough": Giraud, Langou and
@@ -701,69 +702,70 @@ __global__ void __launch_bounds__(GS_THREADS)
   extern __shared__ __align__(16) double gsm[];
   __shared__ double red[GS_THREADS / 32 + 1];
   constexpr int NW = GS_THREADS / 32;
-  const int j = blockIdx.x;
   const int kk = tr->k;
-  if (j >= kk) return;
   const double gtol = gtol_rel * fmax(fabs(lam[0]), 1e-300);
-  if (j > 0 && fabs(lam[j - 1] - lam[j]) <= gtol) return;  // not a group start
-  int end = j + 1;
-  while (end < kk && fabs(lam[end - 1] - lam[end]) <= gtol) ++end;
-  const int g = end - j;
-  if (g < 2) return;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const size_t cap = GS_SMEM / sizeof(double);
-  const bool staged = (size_t)g * n + g <= cap;  // else the vectors stay in global memory
-  double* zs = gsm;
-  double* cf = gsm + (staged ? (size_t)g * n : 0);  // coefficients, g <= cap always (g <= K <= n)
-  auto at = [&](int q, int i) -> double& {
-    return staged ? zs[(ll)q * n + i] : Z[(ll)i * K + j + q];
-  };
-  if (staged)
-    for (ll e = tid; e < (ll)g * n; e += GS_THREADS) {
-      const int q = (int)(e % g), i = (int)(e / g);
-      zs[(ll)q * n + i] = Z[(ll)i * K + j + q];
-    }
-  __syncthreads();
-  for (int q = 0; q < g; ++q) {
-    for (int pass = 0; pass < 2 && q > 0; ++pass) {
-      for (int p = warp; p < q; p += NW) {
-        double sum = 0.0;
-        for (int i = lane; i < n; i += 32) sum += at(p, i) * at(q, i);
-        sum = warp_sum_d(sum);
-        if (lane == 0) cf[p] = sum;
+  for (int j = blockIdx.x; j < kk; j += gridDim.x) {  // candidate group starts, grid-strided
+    if (j > 0 && fabs(lam[j - 1] - lam[j]) <= gtol) continue;  // not a group start
+    int end = j + 1;
+    while (end < kk && fabs(lam[end - 1] - lam[end]) <= gtol) ++end;
+    const int g = end - j;
+    if (g < 2) continue;
+    const bool staged = (size_t)g * n + g <= cap;  // else the vectors stay in global memory
+    double* zs = gsm;
+    double* cf = gsm + (staged ? (size_t)g * n : 0);  // coefficients, g <= cap always (g <= K <= n)
+    auto at = [&](int q, int i) -> double& {
+      return staged ? zs[(ll)q * n + i] : Z[(ll)i * K + j + q];
+    };
+    if (staged)
+      for (ll e = tid; e < (ll)g * n; e += GS_THREADS) {
+        const int q = (int)(e % g), i = (int)(e / g);
+        zs[(ll)q * n + i] = Z[(ll)i * K + j + q];
       }
-      __syncthreads();
+    __syncthreads();
+    for (int q = 0; q < g; ++q) {
+      for (int pass = 0; pass < 2 && q > 0; ++pass) {
+        for (int p = warp; p < q; p += NW) {
+          double sum = 0.0;
+          for (int i = lane; i < n; i += 32) sum += at(p, i) * at(q, i);
+          sum = warp_sum_d(sum);
+          if (lane == 0) cf[p] = sum;
+        }
+        __syncthreads();
+        for (int i = tid; i < n; i += GS_THREADS) {
+          double v = at(q, i);
+          for (int p = 0; p < q; ++p) v -= cf[p] * at(p, i);
+          at(q, i) = v;
+        }
+        __syncthreads();
+      }
+      double sq = 0.0;
       for (int i = tid; i < n; i += GS_THREADS) {
-        double v = at(q, i);
-        for (int p = 0; p < q; ++p) v -= cf[p] * at(p, i);
-        at(q, i) = v;
+        const double v = at(q, i);
+        sq += v * v;
+      }
+      sq = warp_sum_d(sq);
+      if (lane == 0) red[warp] = sq;
+      __syncthreads();
+      if (warp == 0) {
+        double t = lane < NW ? red[lane] : 0.0;
+        t = warp_sum_d(t);
+        if (lane == 0) red[NW] = t;
       }
       __syncthreads();
+      const double tot = red[NW];
+      const double inv = tot > 0.0 ? 1.0 / sqrt(tot) : 0.0;
+      for (int i = tid; i < n; i += GS_THREADS) at(q, i) *= inv;
+      __syncthreads();
     }
-    double sq = 0.0;
-    for (int i = tid; i < n; i += GS_THREADS) {
-      const double v = at(q, i);
-      sq += v * v;
-    }
-    sq = warp_sum_d(sq);
-    if (lane == 0) red[warp] = sq;
-    __syncthreads();
-    if (warp == 0) {
-      double t = lane < NW ? red[lane] : 0.0;
-      t = warp_sum_d(t);
-      if (lane == 0) red[NW] = t;
-    }
-    __syncthreads();
-    const double tot = red[NW];
-    const double inv = tot > 0.0 ? 1.0 / sqrt(tot) : 0.0;
-    for (int i = tid; i < n; i += GS_THREADS) at(q, i) *= inv;
-    __syncthreads();
+    if (staged)
+      for (ll e = tid; e < (ll)g * n; e += GS_THREADS) {
+        const int q = (int)(e % g), i = (int)(e / g);
+        Z[(ll)i * K + j + q] = zs[(ll)q * n + i];
+      }
+    __syncthreads();  // the shared staging area is reused by this CTA's next group
   }
-  if (staged)
-    for (ll e = tid; e < (ll)g * n; e += GS_THREADS) {
-      const int q = (int)(e % g), i = (int)(e / g);
-      Z[(ll)i * K + j + q] = zs[(ll)q * n + i];
-    }
 }
 
 // ----------------------------------------------------------------------------
@@ -995,8 +997,8 @@ void hetrd_cluster(T* G, int n, ll ld, double* d, double* e, T* tau, cudaStream_
   if (n < 64) C = 1;
   else if (n < 128) C = 4;
   else if (n < 256) C = 8;
-  static int c_cap = 16;  // largest cluster size the device accepted
-  if (C > c_cap) C = c_cap;
+  static std::atomic<int> c_cap{16};  // largest cluster size the device accepted
+  if (C > c_cap.load()) C = c_cap.load();
   for (;;) {
     const size_t rows = sizeof(T) * (size_t)((n + C - 1) / C) * n;
     const bool srows = base + rows <= 220 * 1024;
@@ -1008,7 +1010,7 @@ void hetrd_cluster(T* G, int n, ll ld, double* d, double* e, T* tau, cudaStream_
                   err == cudaErrorInvalidValue)) {
       (void)cudaGetLastError();
       C /= 2;
-      c_cap = C;
+      c_cap.store(C);
       continue;
     }
     DMRG2_CUDA(err);
@@ -1039,7 +1041,7 @@ void group_mgs(double* Z, int n, int K, const double* lam, const SvdOut* tr, dou
   if ((size_t)K * sizeof(double) > (size_t)GS_SMEM) throw std::runtime_error("group_mgs: order too large");
   static std::atomic<unsigned long long> attr{0};
   set_smem_attr_once(attr, (const void*)group_cgs_kernel, GS_SMEM);
-  group_cgs_kernel<<<K, GS_THREADS, GS_SMEM, s>>>(Z, n, K, lam, tr, gtol_rel);
+  group_cgs_kernel<<<std::max(1, std::min(K, 148)), GS_THREADS, GS_SMEM, s>>>(Z, n, K, lam, tr, gtol_rel);
   DMRG2_CHECK_LAUNCH();
 }
 

@@ -517,6 +517,60 @@ class Engine final : public EngineBase {
   double energy_ = 0.0, env_build_s_ = 0.0;
 };
 
+size_t engine_footprint(const EngineConfig& c, const std::vector<int>& Dl, const std::vector<int>& Dr) {
+  const int L = c.L, d = c.d;
+  if (L < 2 || (int)Dl.size() != L || (int)Dr.size() != L) throw std::invalid_argument("footprint: bad shapes");
+  const size_t sb = c.complex ? 16 : 8;
+  const ll chi = c.chi_max;
+  std::vector<ll> cap(L + 1);
+  for (int i = 0; i <= L; ++i) cap[i] = ipow_cap(d, std::min(i, L - i), chi);
+  auto el = [&](ll n) { return sb * (size_t)std::max<ll>(n, 1); };
+  size_t b = 0;
+  // constructor
+  for (int i = 0; i < L; ++i) b += el(cap[i] * d * cap[i + 1]);
+  ll nmax = 1, qmax = 1;
+  for (int i = 0; i + 1 < L; ++i) {
+    nmax = std::max(nmax, cap[i] * d * d * cap[i + 2]);
+    qmax = std::max(qmax, std::max(cap[i] * d, (ll)d * cap[i + 2]));
+  }
+  for (int i = 0; i < L; ++i) qmax = std::max(qmax, (ll)d * cap[i + 1]);
+  b += 2 * el(nmax) + el(qmax * qmax) + el(chi * chi);
+  const int kcap = std::min(std::max(c.krylov_max, 2), KRYLOV_CAP);
+  const ll nblk = vec_blocks(nmax);
+  b += sb * ((size_t)kcap + 1) * (size_t)nmax + sizeof(LanczosDev) + sizeof(double) * (size_t)nblk * 2 * (KRYLOV_CAP + 2);
+  {
+    const size_t nn = (size_t)qmax, kk = (size_t)std::max<ll>(std::min<ll>(chi, qmax), 1);
+    b += sb * nn * nn + 2 * sizeof(double) * nn + sb * nn + sizeof(double) * kk + 2 * sizeof(double) * nn * kk +
+         sizeof(double) * kk * kk + sizeof(double) * 5 * nn * kk + sb * nn * kk + sb * 256 * (nn + 1) +
+         sizeof(double) * 64 + sizeof(unsigned) * 4 + sizeof(SvdOut);
+  }
+  b += sizeof(double) * (size_t)qmax + sizeof(int) * (size_t)qmax + sizeof(SvdOut) + sizeof(JacobiCtl) +
+       sizeof(double) * 16 + sizeof(double) * (size_t)nblk * 2 * (KRYLOV_CAP + 2) + sizeof(unsigned) * 4 +
+       sizeof(int) * (size_t)(L + 1);
+  // set_mpo
+  for (int i = 0; i < L; ++i) b += 2 * el((ll)d * Dr[i] * Dl[i] * d);
+  for (int i = 0; i + 1 < L; ++i) b += el((ll)d * d * Dr[i + 1] * Dl[i] * d * d);
+  std::vector<ll> Db(L + 1, 1);
+  for (int i = 0; i < L; ++i) Db[i] = Dl[i];
+  Db[L] = Dr[L - 1];
+  for (int i = 0; i <= L; ++i) b += 2 * el(cap[i] * cap[i] * Db[i]);
+  ll xs = 1;
+  const ll dd = (ll)d * d;
+  for (int i = 0; i + 1 < L; ++i) {
+    xs = std::max(xs, cap[i] * Db[i] * dd * cap[i + 2]);
+    xs = std::max(xs, cap[i] * dd * Db[i + 2] * cap[i + 2]);
+  }
+  for (int i = 0; i < L; ++i) {
+    const ll a = cap[i], bb = cap[i + 1];
+    xs = std::max(xs, a * Dl[i] * d * bb);
+    xs = std::max(xs, a * d * Dr[i] * bb);
+    xs = std::max(xs, bb * Dr[i] * d * a);
+    xs = std::max(xs, (ll)d * bb * Dl[i] * a);
+  }
+  b += 2 * el(xs);
+  return b;
+}
+
 std::unique_ptr<EngineBase> make_engine(const EngineConfig& cfg) {
   if (cfg.complex) return std::unique_ptr<EngineBase>(new Engine<zc>(cfg));
   return std::unique_ptr<EngineBase>(new Engine<double>(cfg));

@@ -67,4 +67,8 @@ class EngineBase {
 
 std::unique_ptr<EngineBase> make_engine(const EngineConfig& cfg);
 
+// device bytes an engine with this configuration holds once its MPO is set
+// (equals device_bytes() after set_mpo; used for admission by the server)
+size_t engine_footprint(const EngineConfig& cfg, const std::vector<int>& Dl, const std::vector<int>& Dr);
+
 }  // namespace dmrg2

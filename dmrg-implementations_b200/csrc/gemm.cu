@@ -3,8 +3,8 @@
 
 namespace dmrg2 {
 
-long long& launch_counter() {
-  static long long c = 0;
+std::atomic<long long>& launch_counter() {
+  static std::atomic<long long> c{0};
   return c;
 }
 

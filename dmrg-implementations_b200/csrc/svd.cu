@@ -246,8 +246,8 @@ void svd_jacobi(T* X, T* Q, int nvec, ll len, JacobiCtl* ctl, int max_sweeps, do
   if (nb < 2) nb = 2;
   if (nb & 1) ++nb;
   DMRG2_CUDA(cudaMemsetAsync(ctl, 0, sizeof(JacobiCtl), s));
-  static int max_coresident = 0;
-  if (max_coresident == 0) {
+  int max_coresident = 0;
+  {
     int dev = 0, nsm = 0, per = 0;
     DMRG2_CUDA(cudaGetDevice(&dev));
     DMRG2_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));

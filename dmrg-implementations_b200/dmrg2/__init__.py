@@ -34,8 +34,10 @@ EXPORTED = [
     "dmrg2_get_mps", "dmrg2_expect_local", "dmrg2_get_device_bytes", "dmrg2_last_error",
     "dmrg2_abi_version", "dmrg2_op_heff", "dmrg2_op_env_left", "dmrg2_op_env_right",
     "dmrg2_op_svd", "dmrg2_op_lanczos", "dmrg2_op_gemm", "dmrg2_resume", "dmrg2_get_launch_count",
-    "dmrg2_op_heff_noalloc",
+    "dmrg2_op_heff_noalloc", "dmrg2_server_create", "dmrg2_server_submit", "dmrg2_server_poll",
+    "dmrg2_server_destroy",
 ]
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
 
 
 class Dmrg2Error(RuntimeError):
@@ -63,6 +65,33 @@ class SweepReport(ctypes.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("max_active", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_size_t)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [
+        ("cfg", Config), ("W", ctypes.POINTER(ctypes.c_void_p)), ("Dl", ctypes.POINTER(ctypes.c_int)),
+        ("Dr", ctypes.POINTER(ctypes.c_int)), ("A", ctypes.POINTER(ctypes.c_void_p)),
+        ("bond_dims", ctypes.POINTER(ctypes.c_int)), ("init_kind", ctypes.c_int),
+        ("schedule", ctypes.POINTER(ctypes.c_int)), ("n_sweeps", ctypes.c_int),
+    ]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [
+        ("state", ctypes.c_int), ("status", ctypes.c_int), ("energy", ctypes.c_double),
+        ("sweeps", ctypes.c_int), ("trunc_err_max", ctypes.c_double), ("max_bond", ctypes.c_int),
+        ("device_s", ctypes.c_double), ("t_submit", ctypes.c_double), ("t_admit", ctypes.c_double),
+        ("t_done", ctypes.c_double), ("footprint_bytes", ctypes.c_size_t), ("message", ctypes.c_char * 256),
+    ]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "message"}
+        d["message"] = self.message.decode(errors="replace")
+        return d
 
 
 _lib = None
@@ -104,6 +133,10 @@ def load_library(path: str | os.PathLike | None = None):
         "dmrg2_op_lanczos": (c_int, [c_int] * 7 + [vp] * 5 + [c_int, c_dbl, c_int, dp, ip]),
         "dmrg2_op_gemm": (c_int, [c_int] * 6 + [dp, vp, ctypes.c_longlong, vp, ctypes.c_longlong, dp, vp,
                                                ctypes.c_longlong]),
+        "dmrg2_server_create": (c_int, [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]),
+        "dmrg2_server_submit": (c_int, [vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_longlong)]),
+        "dmrg2_server_poll": (c_int, [vp, ctypes.c_longlong, c_int, ctypes.POINTER(Result)]),
+        "dmrg2_server_destroy": (None, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -402,3 +435,81 @@ def gemm(A, B, transA="N", transB="N", alpha=1.0, beta=0.0, C=None):
                                         A.shape[1], _ptr(B), B.shape[1], be, _ptr(C), C.shape[1]),
            None, "op_gemm")
     return C
+
+
+# ----------------------------------------------------------------------------
+# served / batched form
+# ----------------------------------------------------------------------------
+class Server:
+    """Many independent ground-state solves on one device (dmrg2_server_*).
+
+    Requests are admitted in arrival order while one of ``max_active`` slots is
+    idle and their device footprint fits ``hbm_budget_bytes``; admitted solves run
+    concurrently, each on its own CUDA stream.
+    """
+
+    def __init__(self, device=0, max_active=8, hbm_budget_bytes=0):
+        self._lib = load_library()
+        self._s = ctypes.c_void_p()
+        cfg = ServerConfig(int(device), int(max_active), int(hbm_budget_bytes))
+        _check(self._lib.dmrg2_server_create(ctypes.byref(cfg), ctypes.byref(self._s)), None, "server_create")
+
+    def submit(self, mpo, schedule, mps=None, init=INIT_RANDOM, seed=0, dtype=None, tol=1e-10,
+               krylov_max=30, lanczos_tol=1e-12, max_restarts=2, cutoff=1e-14, min_sweeps=2, chi_max=None):
+        """Queue one solve; returns its id. mpo: L tensors (Dl, Dr, d, d)."""
+        Ws = _mpo4(mpo)
+        L, d = len(Ws), Ws[0].shape[2]
+        cplx = dtype == np.complex128 or any(np.iscomplexobj(w) for w in Ws) or (
+            mps is not None and any(np.iscomplexobj(a) for a in mps))
+        code = C128 if cplx else F64
+        Ws = [_prep(w, code) for w in Ws]
+        sched = (ctypes.c_int * len(schedule))(*[int(c) for c in schedule])
+        cfg = Config()
+        cfg.L, cfg.d, cfg.chi_max, cfg.dtype = L, d, int(chi_max or max(schedule)), code
+        cfg.tol, cfg.krylov_max, cfg.lanczos_tol = tol, krylov_max, lanczos_tol
+        cfg.max_restarts, cfg.min_sweeps, cfg.seed = max_restarts, min_sweeps, int(seed)
+        cfg.cutoff = cutoff if cutoff > 0 else -1.0
+        wp = (ctypes.c_void_p * L)(*[w.ctypes.data for w in Ws])
+        Dl = (ctypes.c_int * L)(*[w.shape[0] for w in Ws])
+        Dr = (ctypes.c_int * L)(*[w.shape[1] for w in Ws])
+        req = Request()
+        req.cfg, req.W, req.Dl, req.Dr = cfg, wp, Dl, Dr
+        keep = [Ws]
+        if mps is not None:
+            As = [_prep(a, code) for a in mps]
+            keep.append(As)
+            req.A = (ctypes.c_void_p * L)(*[a.ctypes.data for a in As])
+            req.bond_dims = (ctypes.c_int * (L + 1))(*([1] + [a.shape[2] for a in As]))
+        req.init_kind, req.schedule, req.n_sweeps = int(init), sched, len(schedule)
+        rid = ctypes.c_longlong()
+        _check(self._lib.dmrg2_server_submit(self._s, ctypes.byref(req), ctypes.byref(rid)), None, "server_submit")
+        del keep
+        return rid.value
+
+    def poll(self, rid, wait=0.0):
+        """Result dict of request rid; waits up to `wait` seconds (None: until finished)."""
+        r = Result()
+        ms = -1 if wait is None else int(wait * 1000)
+        _check(self._lib.dmrg2_server_poll(self._s, ctypes.c_longlong(rid), ms, ctypes.byref(r)), None,
+               "server_poll")
+        return r.as_dict()
+
+    def result(self, rid):
+        return self.poll(rid, wait=None)
+
+    def close(self):
+        if getattr(self, "_s", None):
+            self._lib.dmrg2_server_destroy(self._s)
+            self._s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

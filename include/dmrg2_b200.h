@@ -212,6 +212,67 @@ int dmrg2_op_heff_noalloc(int dtype, int cL, int cR, int d, int Dl, int Dm, int 
                           const void* R, const void* WL, const void* WR, const void* theta, void* out,
                           void* stream);
 
+/* ---------------------------------------------------------------- served / batched form
+ * A server owns one device and runs many independent ground-state solves at once.
+ * No counterpart in the reference, where one DMRG2GPU object runs one solve at a time.
+ *
+ * Requests are copied at submit. They are admitted in arrival order while one of
+ * max_active worker slots is idle and their device footprint fits the budget. The
+ * footprint covers the MPS, environments, Krylov space, eigen workspace and
+ * contraction scratch, and equals dmrg2_get_device_bytes of the same solve after
+ * set_mpo. Each admitted request is solved on its own engine and CUDA stream, so
+ * solves that arrive while others run overlap with them on the device (continuous
+ * admission; no batch boundary). A request that fits no budget is rejected at
+ * submit. */
+typedef struct dmrg2_server dmrg2_server;
+
+typedef struct dmrg2_server_config {
+  int device;               /* CUDA device ordinal */
+  int max_active;           /* solves running at once (0 -> 8) */
+  size_t hbm_budget_bytes;  /* admission budget (0 -> 90% of the free device memory at create) */
+} dmrg2_server_config;
+
+typedef struct dmrg2_request {
+  dmrg2_config cfg;         /* as for dmrg2_create (device is the server's) */
+  const void* const* W;     /* L row-major MPO tensors (Dl, Dr, d, d) */
+  const int* Dl;            /* L left MPO bonds */
+  const int* Dr;            /* L right MPO bonds */
+  const void* const* A;     /* initial MPS (L row-major tensors), or NULL */
+  const int* bond_dims;     /* L+1 bond dimensions of A */
+  int init_kind;            /* dmrg2_init_kind when A is NULL (seeded by cfg.seed) */
+  const int* schedule;      /* bond cap per sweep, each in [1, cfg.chi_max] */
+  int n_sweeps;             /* length of schedule; the cfg.tol stop rule applies */
+} dmrg2_request;
+
+enum dmrg2_request_state {
+  DMRG2_REQ_QUEUED = 0,
+  DMRG2_REQ_RUNNING = 1,
+  DMRG2_REQ_DONE = 2,
+  DMRG2_REQ_FAILED = 3
+};
+
+typedef struct dmrg2_result {
+  int state;                /* dmrg2_request_state */
+  int status;               /* dmrg2_status of the solve (set when it finished) */
+  double energy;            /* energy of the last sweep */
+  int sweeps;               /* sweeps run */
+  double trunc_err_max;     /* largest discarded weight of the last sweep */
+  int max_bond;
+  double device_s;          /* device time of the sweeps (CUDA events on the solve's stream) */
+  double t_submit, t_admit, t_done;  /* seconds since dmrg2_server_create */
+  size_t footprint_bytes;   /* device bytes reserved at admission */
+  char message[256];        /* error message of a failed solve */
+} dmrg2_result;
+
+int dmrg2_server_create(const dmrg2_server_config* cfg, dmrg2_server** out);
+/* Copies the request and queues it; *id identifies it for dmrg2_server_poll. */
+int dmrg2_server_submit(dmrg2_server* s, const dmrg2_request* req, long long* id);
+/* State and result of request id. Waits up to wait_ms for it to finish
+ * (0: no wait, < 0: until it finishes). */
+int dmrg2_server_poll(dmrg2_server* s, long long id, int wait_ms, dmrg2_result* out);
+/* Fails queued requests, waits for running solves, frees the server. */
+void dmrg2_server_destroy(dmrg2_server* s);
+
 #ifdef __cplusplus
 }
 #endif
