@@ -232,8 +232,7 @@ def run_ours(args):
     import torch.distributed as dist
 
     import dmrg2
-    from oracle import dmrg2_oracle as O
-    from oracle import models as M
+    from dmrg2 import models as P
 
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
@@ -242,8 +241,8 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     ramp, steady = schedule(args.warmup, args.steps)
 
-    mpo = M.heisenberg_mpo(L_SITES)
-    mps = O.random_mps(L_SITES, 2, 16, seed=rank)
+    mpo = P.xxz(L_SITES)
+    mps = P.random_mps(L_SITES, 2, 16, seed=rank)
     h2d = sum(w.nbytes for w in mpo) + sum(a.nbytes for a in mps)
 
     def barrier():
@@ -382,16 +381,127 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+# ----------------------------------------------------------------------------
+# batched and served forms (dmrg2_server_*): solves/s and time-to-converged-energy
+# ----------------------------------------------------------------------------
+def ramp_to(chi, extra):
+    ramp = [c for c in (16, 32, 64, 128, 256) if c < chi] + [chi]
+    return ramp + [chi] * extra, len(ramp) + 1
+
+
+def batched_requests(n=64, seed=7):
+    """64 XXZ chains: L in {24,32,48,64}, Delta ~ U[0.5,1.5], J=1, chi_max in {64,128}."""
+    from dmrg2 import models as P
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        L = int(rng.choice([24, 32, 48, 64]))
+        delta = float(rng.uniform(0.5, 1.5))
+        chi = int(rng.choice([64, 128]))
+        sched, min_sw = ramp_to(chi, 8)
+        out.append(dict(mpo=P.xxz(L, delta=delta), mps=P.random_mps(L, 2, 16, seed=int(rng.integers(1 << 30))),
+                        schedule=sched, min_sweeps=min_sw, arrival=0.0,
+                        desc={"L": L, "delta": round(delta, 4), "chi": chi}))
+    return out
+
+
+def served_requests(n=512, rate=20.0, seed=11):
+    """J1-J2 chains (D=8): J1=1, J2 ~ U[0,0.5], L ~ U{16..96}, chi_max in {32,64,128,256};
+    Poisson arrivals at `rate` requests/s."""
+    from dmrg2 import models as P
+    rng = np.random.default_rng(seed)
+    out, t = [], 0.0
+    for _ in range(n):
+        t += float(rng.exponential(1.0 / rate))
+        L = int(rng.integers(16, 97))
+        j2 = float(rng.uniform(0.0, 0.5))
+        chi = int(rng.choice([32, 64, 128, 256]))
+        sched, min_sw = ramp_to(chi, 8)
+        out.append(dict(mpo=P.j1j2(L, 1.0, j2), mps=P.random_mps(L, 2, 16, seed=int(rng.integers(1 << 30))),
+                        schedule=sched, min_sweeps=min_sw, arrival=t,
+                        desc={"L": L, "J2": round(j2, 4), "chi": chi}))
+    return out
+
+
+def serve(reqs, max_active, device, timed_arrivals):
+    """Submit reqs to a server (at their arrival times when timed_arrivals), wait for all."""
+    import dmrg2
+    srv = dmrg2.Server(device=device, max_active=max_active)
+    t0 = time.perf_counter()
+    ids = []
+    for r in reqs:
+        if timed_arrivals:
+            dt = r["arrival"] - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+        ids.append(srv.submit(r["mpo"], r["schedule"], mps=r["mps"], tol=1e-10, min_sweeps=r["min_sweeps"],
+                              krylov_max=KRYLOV, max_restarts=RESTARTS, cutoff=1e-12))
+    res = [srv.result(i) for i in ids]
+    wall = time.perf_counter() - t0
+    srv.close()
+    return res, wall
+
+
+def run_server_workload(args):
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if args.workload == "batched":
+        reqs = batched_requests(args.requests or 64)
+        timed = False
+        metric = "solves/s (64 XXZ chains, L in {24..64}, chi_max in {64,128}, FP64, continuous admission)"
+    else:
+        reqs = served_requests(args.requests or 512)
+        timed = True
+        metric = "solves/s (J1-J2 D=8 request stream, Poisson 20 req/s, L in 16..96, chi_max in {32..256}, FP64)"
+    n_plain = min(len(reqs), args.plain_sample)
+    # the plain form: the same requests one at a time, back to back (no arrival gaps)
+    plain, plain_wall = serve(reqs[:n_plain], 1, local, False)
+    with ClockSampler(local) as clocks:
+        res, wall = serve(reqs, args.max_active, local, timed)
+    import dmrg2
+    failed = [r["message"] for r in res if r["state"] != dmrg2.REQ_DONE]
+    lat = np.array([r["t_done"] - r["t_submit"] for r in res])
+    span = max(r["t_done"] for r in res) - min(r["t_submit"] for r in res)
+    dE = max(abs(a["energy"] - b["energy"]) / abs(b["energy"]) for a, b in zip(res[:n_plain], plain))
+    plain_rate = n_plain / sum(r["t_done"] - r["t_admit"] for r in plain)
+    value = len(res) / span
+    line = {
+        "metric": metric, "value": value, "unit": "solves/s", "n_gpus": 1, "steps": len(res), "warmup": 0,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded MPOs and N(0,1) initial MPS)", "impl": "ours",
+        "config": {"workload": args.workload, "requests": len(res), "max_active": args.max_active,
+                   "schedule": "ramp 16,32,.. to chi_max then chi_max x8, stop |dE| < 1e-10",
+                   "krylov_max": KRYLOV, "cutoff": 1e-12},
+        "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                      "max": float(lat.max())},
+        "plain": {"solves_per_s": plain_rate, "requests": n_plain,
+                  "what": "the same requests solved one at a time on one stream (sum of solve times)"},
+        "speedup_vs_plain": value / plain_rate,
+        "max_rel_dE_mix_vs_alone": dE, "failed": len(failed),
+        "mean_sweeps": float(np.mean([r["sweeps"] for r in res])),
+        "clocks": clocks.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["sweep", "batched", "served"], default="sweep")
+    ap.add_argument("--requests", type=int, default=0)
+    ap.add_argument("--max-active", type=int, default=12)
+    ap.add_argument("--plain-sample", type=int, default=24)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.workload != "sweep" and args.impl == "ours":
+        run_server_workload(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)
