@@ -190,3 +190,16 @@ def test_resume_from_right_canonical_mps_readback():
     B[L // 2] = B[L // 2] * 1.5 + 1e-3 * np.random.default_rng(1).standard_normal(B[L // 2].shape)
     eng3, rep3 = gpu_run(mpo, B, [32] * 6, krylov_max=30, max_restarts=4)
     assert abs(rep3[-1]["energy"] - rep[-1]["energy"]) <= 1e-10 * abs(rep[-1]["energy"])
+
+
+def test_reference_bin_data_josephson_vs_oracle(golden_dir):
+    """The reference's own .bin benchmark data (complex Josephson L=12, n_max=2, its
+    seeded chi=10 random state) through dmrg2.io into the GPU engine, against the
+    oracle on the same inputs and schedule."""
+    from dmrg2 import io
+    W = io.load_mpo_bin(golden_dir / "josephson_L12_n2_mpo.bin")
+    A = io.load_mps_bin(golden_dir / "josephson_L12_n2_chi10_mps.bin")
+    sched = [24] * 4
+    eng, rep = gpu_run(W, A, sched, krylov_max=30, max_restarts=4, cutoff=1e-14)
+    ref = O.dmrg2(W, A, sched, cutoff=1e-14)
+    assert abs(rep[-1]["energy"] - ref["energy"]) <= 1e-10 * abs(ref["energy"])
