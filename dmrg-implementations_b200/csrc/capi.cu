@@ -19,6 +19,7 @@
 #include "lanczos_driver.cuh"
 #include "noalloc.cuh"
 #include "truncate.cuh"
+#include "umma.cuh"
 
 using namespace dmrg2;
 
@@ -279,6 +280,28 @@ void do_op_gemm(int ta, int tb, int M, int N, int K, const double* alpha, const 
   g.beta = ST<T>::make(beta[0], beta[1]);
   launch_gemm(g, 0);
   DMRG2_CUDA(cudaMemcpy(C, dC.p, sb * (size_t)M * ldc, cudaMemcpyDeviceToHost));
+}
+
+template <typename T>
+void do_op_gemm_bf16x3(int ta, int tb, int M, int N, int K, const double* alpha, const void* A, ll lda,
+                       const void* B, ll ldb, const double* beta, void* C, ll ldc) {
+  const size_t sb = sizeof(T);
+  const ll arows = (ta == 1 || ta == 2) ? K : M;
+  const ll brows = (tb == 1 || tb == 2) ? N : K;
+  DBuf dA(A, sb * (size_t)arows * lda), dB(B, sb * (size_t)brows * ldb), dC(C, sb * (size_t)M * ldc);
+  SplitScratch ws;
+  try {
+    gemm_bf16x3<T>(ta, tb, M, N, K, ST<T>::make(alpha[0], alpha[1]), dA.as<T>(), lda, 0, dB.as<T>(), ldb, 0,
+                   ST<T>::make(beta[0], beta[1]), dC.as<T>(), ldc, 0, 1, ws, 0);
+    int err = 0;
+    DMRG2_CUDA(cudaMemcpy(&err, ws.err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) throw std::runtime_error("op_gemm_bf16x3: tensor-core completion wait timed out");
+    DMRG2_CUDA(cudaMemcpy(C, dC.p, sb * (size_t)M * ldc, cudaMemcpyDeviceToHost));
+  } catch (...) {
+    ws.release();
+    throw;
+  }
+  ws.release();
 }
 
 void check_dtype(int dt) {
@@ -613,6 +636,21 @@ int dmrg2_op_gemm(int dtype, int transA, int transB, int M, int N, int K, const 
     check_pos({M, N, K});
     if (dtype == DMRG2_C128) do_op_gemm<zc>(transA, transB, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
     else do_op_gemm<double>(transA, transB, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+  });
+}
+
+int dmrg2_op_gemm_bf16x3(int dtype, int transA, int transB, int M, int N, int K, const double* alpha,
+                         const void* A, long long lda, const void* B, long long ldb, const double* beta,
+                         void* C, long long ldc) {
+  return guarded(nullptr, [&] {
+    check_dtype(dtype);
+    check_pos({M, N, K});
+    if (!alpha || !beta || !A || !B || !C) throw std::invalid_argument("op_gemm_bf16x3: null argument");
+    if (transA < 0 || transA > 3 || transB < 0 || transB > 2) throw std::invalid_argument("op_gemm_bf16x3: bad trans");
+    if (dtype == DMRG2_C128)
+      do_op_gemm_bf16x3<zc>(transA, transB, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+    else
+      do_op_gemm_bf16x3<double>(transA, transB, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
   });
 }
 

@@ -35,7 +35,7 @@ EXPORTED = [
     "dmrg2_abi_version", "dmrg2_op_heff", "dmrg2_op_env_left", "dmrg2_op_env_right",
     "dmrg2_op_svd", "dmrg2_op_lanczos", "dmrg2_op_gemm", "dmrg2_resume", "dmrg2_get_launch_count",
     "dmrg2_op_heff_noalloc", "dmrg2_server_create", "dmrg2_server_submit", "dmrg2_server_poll",
-    "dmrg2_server_destroy",
+    "dmrg2_server_destroy", "dmrg2_op_gemm_bf16x3",
 ]
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
 
@@ -133,6 +133,8 @@ def load_library(path: str | os.PathLike | None = None):
         "dmrg2_op_lanczos": (c_int, [c_int] * 7 + [vp] * 5 + [c_int, c_dbl, c_int, dp, ip]),
         "dmrg2_op_gemm": (c_int, [c_int] * 6 + [dp, vp, ctypes.c_longlong, vp, ctypes.c_longlong, dp, vp,
                                                ctypes.c_longlong]),
+        "dmrg2_op_gemm_bf16x3": (c_int, [c_int] * 6 + [dp, vp, ctypes.c_longlong, vp, ctypes.c_longlong, dp,
+                                                      vp, ctypes.c_longlong]),
         "dmrg2_server_create": (c_int, [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]),
         "dmrg2_server_submit": (c_int, [vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_longlong)]),
         "dmrg2_server_poll": (c_int, [vp, ctypes.c_longlong, c_int, ctypes.POINTER(Result)]),
@@ -434,6 +436,23 @@ def gemm(A, B, transA="N", transB="N", alpha=1.0, beta=0.0, C=None):
     _check(load_library().dmrg2_op_gemm(code, _TRANS[transA], _TRANS[transB], M, N, K, al, _ptr(A),
                                         A.shape[1], _ptr(B), B.shape[1], be, _ptr(C), C.shape[1]),
            None, "op_gemm")
+    return C
+
+
+def gemm_bf16x3(A, B, transA="N", transB="N", alpha=1.0, beta=0.0, C=None):
+    """The same product in the precision form: three-term BF16 split of each operand,
+    FP32 accumulation on the tcgen05 tensor cores, FP64 result (real alpha, beta)."""
+    code = _dtype_code(A, B) if C is None else _dtype_code(A, B, C)
+    A, B = _prep(A, code), _prep(B, code)
+    M = A.shape[1] if transA in ("T", "C") else A.shape[0]
+    K = A.shape[0] if transA in ("T", "C") else A.shape[1]
+    N = B.shape[0] if transB in ("T", "C") else B.shape[1]
+    C = np.zeros((M, N), A.dtype) if C is None else _prep(C, code).copy()
+    al = (ctypes.c_double * 2)(float(np.real(alpha)), float(np.imag(alpha)))
+    be = (ctypes.c_double * 2)(float(np.real(beta)), float(np.imag(beta)))
+    _check(load_library().dmrg2_op_gemm_bf16x3(code, _TRANS[transA], _TRANS[transB], M, N, K, al, _ptr(A),
+                                               A.shape[1], _ptr(B), B.shape[1], be, _ptr(C), C.shape[1]),
+           None, "op_gemm_bf16x3")
     return C
 
 

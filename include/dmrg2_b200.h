@@ -194,6 +194,16 @@ int dmrg2_op_gemm(int dtype, int transA, int transB, int M, int N, int K, const 
                   const void* A, long long lda, const void* B, long long ldb, const double* beta,
                   void* C, long long ldc);
 
+/* The same product computed by the precision form: each operand split into three
+ * BF16 pieces (x = x1 + x2 + x3), the six leading piece products accumulated in FP32
+ * on the tcgen05 tensor cores, the result written in FP64 (complex via the real
+ * embedding [[Ar, -Ai], [Ai, Ar]]). Relative error ~1e-7 of sum |a_ik b_kj|. No
+ * counterpart in the reference (its GEMMs are FP64 only). transB 2 = conjugate
+ * transpose; alpha and beta must be real. */
+int dmrg2_op_gemm_bf16x3(int dtype, int transA, int transB, int M, int N, int K, const double* alpha,
+                         const void* A, long long lda, const void* B, long long ldb, const double* beta,
+                         void* C, long long ldc);
+
 /* apply_heff on DEVICE pointers, allocating no device memory. No counterpart in
  * the reference: its GPU path only applies H_eff inside its own Lanczos loop on
  * buffers it allocated up front. For callers that must not allocate while they

@@ -52,6 +52,35 @@ def test_gemm_dmma(cplx, shape, ta, tb):
     close(out, ref)
 
 
+SPLIT_SHAPES = [(1, 1, 1), (37, 45, 29), (128, 128, 64), (200, 130, 300), (256, 1024, 256), (96, 40, 1280)]
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+@pytest.mark.parametrize("shape", SPLIT_SHAPES)
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("N", "T"), ("T", "N"), ("C", "T")])
+def test_gemm_bf16x3_tcgen05(cplx, shape, ta, tb):
+    """Precision-form GEMM (three-term BF16 split, FP32 accumulation in tensor memory):
+    error below 2.5e-7 sqrt(K) of sum_k |a_ik| |b_kj| per entry against the FP64
+    product (split truncation ~2^-24 per term, FP32 accumulation growing as sqrt(K))."""
+    if not cplx and ta == "C":
+        pytest.skip("conjugation is the identity for real data")
+    rng = np.random.default_rng(hash((cplx, shape, ta, tb, 7)) % 2**32)
+    M, N, K = shape
+    A = rnd(rng, (K, M) if ta in ("T", "C") else (M, K), cplx)
+    B = rnd(rng, (N, K) if tb == "T" else (K, N), cplx)
+    C0 = rnd(rng, (M, N), cplx)
+    opA = {"N": A, "T": A.T, "C": A.conj().T}[ta]
+    opB = B.T if tb == "T" else B
+    alpha, beta = 0.75, -0.5
+    ref = alpha * opA @ opB + beta * C0
+    out = dmrg2.gemm_bf16x3(A, B, ta, tb, alpha=alpha, beta=beta, C=C0)
+    bound = 2.5e-7 * np.sqrt(K) * abs(alpha) * (np.abs(opA) @ np.abs(opB)) + 1e-15
+    assert np.all(np.abs(out - ref) <= bound), float(np.max(np.abs(out - ref) / bound))
+    # and it is not the FP64 product: the split really ran at reduced precision
+    if K >= 64:
+        assert np.max(np.abs(out - ref)) > 0
+
+
 @pytest.fixture(scope="module")
 def prim(golden_dir):
     return np.load(golden_dir / "ref_primitives.npz")
