@@ -324,6 +324,8 @@ EngineConfig engine_config(const dmrg2_config* cfg) {
   c.seed = (unsigned)(cfg->seed ^ (cfg->seed >> 32));
   if (cfg->svd_method != 0 && cfg->svd_method != 1) throw std::invalid_argument("unknown svd_method");
   c.svd_method = cfg->svd_method;
+  if (cfg->precision != 0 && cfg->precision != 1) throw std::invalid_argument("unknown precision form");
+  c.precision = cfg->precision;
   return c;
 }
 void check_pos(std::initializer_list<int> v) {
@@ -476,6 +478,7 @@ static void fill_reports(const std::vector<SweepStats>& st, dmrg2_sweep_report* 
     r.svd_s = st[s].svd_s;
     r.jacobi_sweeps_max = st[s].jacobi_sweeps_max;
     r.device_s = st[s].device_s;
+    r.lowprec_matvecs = st[s].lowprec_matvecs;
   }
 }
 

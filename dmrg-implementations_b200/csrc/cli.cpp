@@ -39,7 +39,7 @@ struct Args {
   double delta = 1.0;
   std::vector<int> schedule;
   double cutoff = 0.0, tol = 1e-10, lanczos_tol = 0.0;
-  int krylov = 0, restarts = 0;
+  int krylov = 0, restarts = 0, precision = 0;
   unsigned long long seed = 42;
   std::string init;
   std::string json;
@@ -86,13 +86,13 @@ void write_json(const Args& a, const Mpo& m, double energy, double wall, double 
                "      \"energy\": %s, \"energies\": [%s], \"repeats\": 1, \"successful_reps\": 1,\n"
                "      \"cmd\": \"%s\", \"timer_scope\": \"sweep_only\", \"env_build_sec\": %s,\n"
                "      \"sweep_energies\": [%s], \"trunc_err\": [%s], \"sweeps_run\": %d,\n"
-               "      \"sweeps_per_s\": %s, \"heff_tflops\": %s, \"precision_form\": \"fp64\"%s\n"
+               "      \"sweeps_per_s\": %s, \"heff_tflops\": %s, \"precision_form\": \"%s\"%s\n"
                "    }\n  ]\n}\n",
                stamp, m.name.c_str(), a.L, a.chi, a.sweeps, fmt(wall).c_str(), fmt(wall).c_str(),
                fmt(wall).c_str(), fmt(wall).c_str(), fmt(energy).c_str(), fmt(energy).c_str(),
                a.cmdline.c_str(), fmt(env_s).c_str(), es.str().c_str(), ts.str().c_str(),
                (int)rep.size(), fmt(wall > 0 ? rep.size() / wall : 0.0).c_str(),
-               fmt(hs > 0 ? flops / hs * 1e-12 : 0.0).c_str(),
+               fmt(hs > 0 ? flops / hs * 1e-12 : 0.0).c_str(), a.precision ? "split_bf16" : "fp64",
                m.name == "josephson" ? (", \"nmax\": " + std::to_string(a.n_max)).c_str() : "");
   std::fclose(f);
 }
@@ -113,6 +113,7 @@ int solve(const Args& a, const Mpo& m, bool default_neel, double exact, double e
   cfg.max_restarts = a.restarts;
   cfg.cutoff = a.cutoff;
   cfg.seed = a.seed;
+  cfg.precision = a.precision;
   dmrg2_handle* h = nullptr;
   if (dmrg2_create(&cfg, &h) != DMRG2_OK) return fail(nullptr, "create");
   std::vector<const void*> W(m.L);
@@ -210,6 +211,12 @@ int main(int argc, char** argv) {
     if (s == "--seed") { a.seed = std::strtoull(next("--seed"), nullptr, 10); continue; }
     if (s == "--init") { a.init = next("--init"); continue; }
     if (s == "--json") { a.json = next("--json"); continue; }
+    if (s == "--precision") {
+      const std::string v = next("--precision");
+      if (v != "plain" && v != "split") { std::fprintf(stderr, "--precision takes plain or split\n"); std::exit(1); }
+      a.precision = v == "split" ? 1 : 0;
+      continue;
+    }
     if (s == "--schedule") {
       std::stringstream ss(next("--schedule"));
       std::string tok;

@@ -33,19 +33,11 @@ __global__ void __launch_bounds__(128)
   }
 }
 
+// step 2 of the matvec: Y[a] = WWt X[a] for every a (MPO mixing, FP64)
 template <typename T>
-void heff_apply(const T* Lenv, const T* Renv, const T* WWt, const T* in, T* out, T* X, T* Y, int cL,
-                int cR, int d, int Dl, int Dr, const int* skip, cudaStream_t s) {
+static void heff_mix(const T* X, const T* WWt, T* Y, int cL, int cR, int d, int Dl, int Dr, const int* skip,
+                     cudaStream_t s) {
   const ll dd = (ll)d * d;
-  {
-    Gemm<T> g;
-    g.M = cL; g.N = (int)(dd * cR); g.K = cL;
-    g.A = Lenv; g.lda = (ll)Dl * cL; g.sA1 = cL;
-    g.B = in; g.ldb = dd * cR; g.sB1 = 0;
-    g.C = X; g.ldc = (ll)Dl * dd * cR; g.sC1 = dd * cR;
-    g.nb1 = Dl; g.skip = skip;
-    launch_gemm(g, s);
-  }
   const int Kin = (int)(Dl * dd), Kout = (int)(dd * Dr);
   if (Kin <= 32 && Kout <= 32 && cL <= 65535) {
     dim3 grid(ceil_div(cR, 128), cL);
@@ -60,6 +52,36 @@ void heff_apply(const T* Lenv, const T* Renv, const T* WWt, const T* in, T* out,
     g.nb1 = cL; g.skip = skip;
     launch_gemm(g, s);
   }
+}
+
+template <typename T>
+void heff_apply_split(const T* Lenv, const T* Renv, const T* WWt, const T* in, T* out, T* X, T* Y, int cL,
+                      int cR, int d, int Dl, int Dr, SplitScratch& ws, const int* skip, cudaStream_t s) {
+  const ll dd = (ll)d * d;
+  const T one = ST<T>::one(), zero = ST<T>::zero();
+  // step 1: X[a][w][.] = L[a][w][:] theta, Dl batches sharing theta
+  gemm_bf16x3<T>(0, 0, cL, (int)(dd * cR), cL, one, Lenv, (ll)Dl * cL, cL, in, dd * cR, 0, zero, X,
+                 (ll)Dl * dd * cR, dd * cR, Dl, ws, s, skip);
+  heff_mix(X, WWt, Y, cL, cR, d, Dl, Dr, skip, s);
+  // step 3: out[(a,p,q)][f] = sum_(n,e) Y[(a,p,q)][(n,e)] R[f][(n,e)]
+  gemm_bf16x3<T>(0, 1, (int)(cL * dd), cR, Dr * cR, one, Y, (ll)Dr * cR, 0, Renv, (ll)Dr * cR, 0, zero, out, cR,
+                 0, 1, ws, s, skip);
+}
+
+template <typename T>
+void heff_apply(const T* Lenv, const T* Renv, const T* WWt, const T* in, T* out, T* X, T* Y, int cL,
+                int cR, int d, int Dl, int Dr, const int* skip, cudaStream_t s) {
+  const ll dd = (ll)d * d;
+  {
+    Gemm<T> g;
+    g.M = cL; g.N = (int)(dd * cR); g.K = cL;
+    g.A = Lenv; g.lda = (ll)Dl * cL; g.sA1 = cL;
+    g.B = in; g.ldb = dd * cR; g.sB1 = 0;
+    g.C = X; g.ldc = (ll)Dl * dd * cR; g.sC1 = dd * cR;
+    g.nb1 = Dl; g.skip = skip;
+    launch_gemm(g, s);
+  }
+  heff_mix(X, WWt, Y, cL, cR, d, Dl, Dr, skip, s);
   {
     Gemm<T> g;
     g.tb = true;
@@ -219,6 +241,8 @@ void build_wmix_right(const T* W, int Dl, int Dr, int d, std::vector<T>& out) {
 #define INST(T)                                                                                 \
   template void heff_apply<T>(const T*, const T*, const T*, const T*, T*, T*, T*, int, int, int, \
                               int, int, const int*, cudaStream_t);                               \
+  template void heff_apply_split<T>(const T*, const T*, const T*, const T*, T*, T*, T*, int, int,   \
+                                    int, int, int, SplitScratch&, const int*, cudaStream_t);     \
   template void env_left<T>(const T*, const T*, const T*, T*, T*, T*, int, int, int, int, int,  \
                             cudaStream_t);                                                       \
   template void env_right<T>(const T*, const T*, const T*, T*, T*, T*, int, int, int, int, int, \

@@ -13,6 +13,7 @@
 
 #include "common.cuh"
 #include "gemm.cuh"
+#include "umma.cuh"
 
 namespace dmrg2 {
 
@@ -23,6 +24,12 @@ namespace dmrg2 {
 template <typename T>
 void heff_apply(const T* Lenv, const T* Renv, const T* WWt, const T* in, T* out, T* X, T* Y, int cL,
                 int cR, int d, int Dl, int Dr, const int* skip, cudaStream_t s);
+
+// The same matvec in the precision form: steps 1 and 3 as split-BF16 GEMMs on the
+// tcgen05 tensor cores (FP32 accumulation), step 2 in FP64.
+template <typename T>
+void heff_apply_split(const T* Lenv, const T* Renv, const T* WWt, const T* in, T* out, T* X, T* Y, int cL,
+                      int cR, int d, int Dl, int Dr, SplitScratch& ws, const int* skip, cudaStream_t s);
 
 // algorithmic real flops of one heff_apply
 double heff_flops(int cL, int cR, int d, int Dl, int Dr, bool cplx);

@@ -93,6 +93,7 @@ class Engine final : public EngineBase {
     for (void* p : allocs_) cudaFree(p);
     cudaFreeHost(h_svd_);
     cudaFreeHost(h_flags_);
+    split_.release();
     lw_.release();
     ew_.release();
     cudaEventDestroy(ev_c_);
@@ -441,8 +442,25 @@ class Engine final : public EngineBase {
     auto mv = [&](const T* in, T* out, const int* skip) {
       heff_apply(lenv_[i], renv_[i + 2], wwt_[i], in, out, X_, Y_, cL, cR, d_, Dl, Dr, skip, st_);
     };
-    LanczosResult r = lanczos_solve<T>(lw_, theta_, n, cfg_.krylov_max, cfg_.lanczos_tol,
-                                       cfg_.max_restarts, cfg_.seed + 7919u * (unsigned)i, mv, st_);
+    LanczosResult r;
+    if (cfg_.precision == 1) {
+      // precision form: converge on the split-BF16 operator (FP32-level accuracy), then
+      // refine the Ritz vector with FP64 matvecs; the energy is the FP64 one
+      auto mv_lp = [&](const T* in, T* out, const int* skip) {
+        heff_apply_split(lenv_[i], renv_[i + 2], wwt_[i], in, out, X_, Y_, cL, cR, d_, Dl, Dr, split_, skip, st_);
+      };
+      LanczosResult lp = lanczos_solve<T>(lw_, theta_, n, cfg_.krylov_max, std::max(cfg_.lanczos_tol, 1e-9),
+                                          cfg_.max_restarts, cfg_.seed + 7919u * (unsigned)i, mv_lp, st_);
+      r = lanczos_solve<T>(lw_, theta_, n, std::min(cfg_.krylov_max, 16), cfg_.lanczos_tol, 1,
+                           cfg_.seed + 7919u * (unsigned)i + 1u, mv, st_);
+      ss.lowprec_matvecs += lp.matvecs;
+      r.matvecs += lp.matvecs;
+      r.iters += lp.iters;
+      r.matvec_s += lp.matvec_s;
+    } else {
+      r = lanczos_solve<T>(lw_, theta_, n, cfg_.krylov_max, cfg_.lanczos_tol, cfg_.max_restarts,
+                           cfg_.seed + 7919u * (unsigned)i, mv, st_);
+    }
     ss.heff_s += r.matvec_s;
     ss.matvecs += r.matvecs;
     ss.heff_flops += fl * r.matvecs;
@@ -506,6 +524,7 @@ class Engine final : public EngineBase {
   double* dscal_ = nullptr;
   RedScratch red_;
   SvdOut* h_svd_ = nullptr;
+  SplitScratch split_;  // BF16 pieces of the precision-form matvec
   int* canon_flags_ = nullptr;
   int* h_flags_ = nullptr;
   cudaEvent_t ev_c_ = nullptr, ev_d_ = nullptr, ev_s0_ = nullptr, ev_s1_ = nullptr;

@@ -26,6 +26,7 @@ struct EngineConfig {
   int min_sweeps = 2;          // the stop rule applies from the second sweep on
   int jacobi_max_sweeps = 40;
   int svd_method = 0;          // 0: reduced density matrix eigensolver, 1: one-sided block Jacobi
+  int precision = 0;           // 0: FP64 matvecs; 1: split-BF16 matvecs on tcgen05, then FP64 refinement
   unsigned seed = 42;
 };
 
@@ -45,6 +46,7 @@ struct SweepStats {
   double svd_s = 0.0;
   int jacobi_sweeps_max = 0;
   double device_s = 0.0;     // device time of the whole sweep (CUDA events on the engine stream)
+  long long lowprec_matvecs = 0;  // precision form: matvecs on the split-BF16 operator
 };
 
 class EngineBase {

@@ -109,7 +109,8 @@ __device__ inline T load_op(const T* X, ll ld, int trans, int r, int c) {
 // A' (Mp x Kp, K-major): real: op(A); complex: [[Ar, -Ai], [Ai, Ar]]
 template <typename T>
 __global__ void split_a_kernel(const T* __restrict__ A, ll lda, ll sA, int ta, int M, int K, int Mp, int Kp,
-                               int nb, __nv_bfloat16* __restrict__ out) {
+                               int nb, __nv_bfloat16* __restrict__ out, const int* skip) {
+  if (skip && *((volatile const int*)skip)) return;
   const ll per = (ll)Mp * Kp, tot = per * nb;
   const ll piece = tot;  // elements per piece array (all batches)
   for (ll t = (ll)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (ll)gridDim.x * blockDim.x) {
@@ -131,7 +132,8 @@ __global__ void split_a_kernel(const T* __restrict__ A, ll lda, ll sA, int ta, i
 // B' (Np x Kp, K-major, row n holds column n of op(B)): real: op(B)^T; complex: [Br; Bi]^T
 template <typename T>
 __global__ void split_b_kernel(const T* __restrict__ B, ll ldb, ll sB, int tb, int K, int N, int Np, int Kp,
-                               int nb, __nv_bfloat16* __restrict__ out) {
+                               int nb, __nv_bfloat16* __restrict__ out, const int* skip) {
+  if (skip && *((volatile const int*)skip)) return;
   const ll per = (ll)Np * Kp, tot = per * nb;
   const ll piece = tot;
   for (ll t = (ll)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (ll)gridDim.x * blockDim.x) {
@@ -153,17 +155,18 @@ __global__ void split_b_kernel(const T* __restrict__ B, ll ldb, ll sB, int tb, i
 template <typename T>
 __global__ void __launch_bounds__(UM_THREADS, 1)
     umma_bf16x3_kernel(const __nv_bfloat16* __restrict__ Ap, const __nv_bfloat16* __restrict__ Bp, int Mp,
-                       int Np, int Kp, int nb, int M, int N, double alpha, double beta, T* __restrict__ C,
-                       ll ldc, ll sC, int* __restrict__ err) {
+                       int Np, int Kp, int nbA, int nbB, int M, int N, double alpha, double beta,
+                       T* __restrict__ C, ll ldc, ll sC, int* __restrict__ err, const int* skip) {
+  if (skip && *((volatile const int*)skip)) return;  // uniform: before any TMEM allocation
   extern __shared__ __align__(1024) unsigned char usm[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t tmem_slot;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int b = blockIdx.z;
   const int m0 = blockIdx.y * UM_BM, n0 = blockIdx.x * UM_BN;
-  const ll pieceA = (ll)nb * Mp * Kp, pieceB = (ll)nb * Np * Kp;
-  const __nv_bfloat16* A0 = Ap + (ll)b * Mp * Kp + (ll)m0 * Kp;
-  const __nv_bfloat16* B0 = Bp + (ll)b * Np * Kp + (ll)n0 * Kp;
+  const ll pieceA = (ll)nbA * Mp * Kp, pieceB = (ll)nbB * Np * Kp;
+  const __nv_bfloat16* A0 = Ap + (ll)(nbA > 1 ? b : 0) * Mp * Kp + (ll)m0 * Kp;
+  const __nv_bfloat16* B0 = Bp + (ll)(nbB > 1 ? b : 0) * Np * Kp + (ll)n0 * Kp;
   const uint32_t sbase = smem_u32(usm);
   const uint32_t sbar = smem_u32(&bar);
 
@@ -265,7 +268,8 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
 
 template <typename T>
 void gemm_bf16x3(int ta, int tb, int M, int N, int K, T alpha, const T* A, ll lda, ll sA, const T* B,
-                 ll ldb, ll sB, T beta, T* C, ll ldc, ll sC, int nbatch, SplitScratch& ws, cudaStream_t s) {
+                 ll ldb, ll sB, T beta, T* C, ll ldc, ll sC, int nbatch, SplitScratch& ws, cudaStream_t s,
+                 const int* skip) {
   if (M < 1 || N < 1 || K < 1 || nbatch < 1) return;
   if (ST<T>::im(alpha) != 0.0 || ST<T>::im(beta) != 0.0)
     throw std::invalid_argument("gemm_bf16x3: alpha and beta must be real");
@@ -273,26 +277,28 @@ void gemm_bf16x3(int ta, int tb, int M, int N, int K, T alpha, const T* A, ll ld
   const ll Mp = round_up(cplx ? 2LL * M : M, UM_BM), Np = round_up(N, UM_BN);
   const ll Kp = round_up(cplx ? 2LL * K : K, UM_BK);
   if (Mp / UM_BM > 65535 || nbatch > 65535) throw std::invalid_argument("gemm_bf16x3: grid too large");
-  const size_t need = sizeof(__nv_bfloat16) * 3 * (size_t)nbatch * (size_t)(Mp + Np) * (size_t)Kp;
+  const int nbA = sA == 0 ? 1 : nbatch, nbB = sB == 0 ? 1 : nbatch;  // shared operands split once
+  const size_t need = sizeof(__nv_bfloat16) * 3 * ((size_t)nbA * Mp + (size_t)nbB * Np) * (size_t)Kp;
   ws.reserve(need);
   __nv_bfloat16* Ap = (__nv_bfloat16*)ws.p;
-  __nv_bfloat16* Bp = Ap + 3 * (size_t)nbatch * Mp * Kp;
+  __nv_bfloat16* Bp = Ap + 3 * (size_t)nbA * Mp * Kp;
   const int grid = 148 * 8;
-  split_a_kernel<T><<<grid, 256, 0, s>>>(A, lda, sA, ta, M, K, (int)Mp, (int)Kp, nbatch, Ap);
+  split_a_kernel<T><<<grid, 256, 0, s>>>(A, lda, sA, ta, M, K, (int)Mp, (int)Kp, nbA, Ap, skip);
   DMRG2_CHECK_LAUNCH();
-  split_b_kernel<T><<<grid, 256, 0, s>>>(B, ldb, sB, tb, K, N, (int)Np, (int)Kp, nbatch, Bp);
+  split_b_kernel<T><<<grid, 256, 0, s>>>(B, ldb, sB, tb, K, N, (int)Np, (int)Kp, nbB, Bp, skip);
   DMRG2_CHECK_LAUNCH();
   static std::atomic<unsigned long long> attr{0};
   set_smem_attr_once(attr, (const void*)umma_bf16x3_kernel<T>, UM_SMEM);
   dim3 g((unsigned)(Np / UM_BN), (unsigned)(Mp / UM_BM), (unsigned)nbatch);
-  umma_bf16x3_kernel<T><<<g, UM_THREADS, UM_SMEM, s>>>(Ap, Bp, (int)Mp, (int)Np, (int)Kp, nbatch, M, N,
-                                                      ST<T>::re(alpha), ST<T>::re(beta), C, ldc, sC, ws.err);
+  umma_bf16x3_kernel<T><<<g, UM_THREADS, UM_SMEM, s>>>(Ap, Bp, (int)Mp, (int)Np, (int)Kp, nbA, nbB, M, N,
+                                                      ST<T>::re(alpha), ST<T>::re(beta), C, ldc, sC, ws.err,
+                                                      skip);
   DMRG2_CHECK_LAUNCH();
 }
 
 template void gemm_bf16x3<double>(int, int, int, int, int, double, const double*, ll, ll, const double*, ll,
-                                  ll, double, double*, ll, ll, int, SplitScratch&, cudaStream_t);
+                                  ll, double, double*, ll, ll, int, SplitScratch&, cudaStream_t, const int*);
 template void gemm_bf16x3<zc>(int, int, int, int, int, zc, const zc*, ll, ll, const zc*, ll, ll, zc, zc*, ll,
-                              ll, int, SplitScratch&, cudaStream_t);
+                              ll, int, SplitScratch&, cudaStream_t, const int*);
 
 }  // namespace dmrg2

@@ -23,9 +23,12 @@ struct SplitScratch {
 };
 
 // op(A): trans 0 = N, 1 = T, 2 = C (conjugate transpose), 3 = conjugate. Row-major
-// storage, leading dimensions in elements, nbatch strided batches (sA, sB, sC).
+// storage, leading dimensions in elements, nbatch strided batches (sA, sB, sC); an
+// operand with batch stride 0 is split once and shared by all batches. Every kernel
+// returns at once when *skip is nonzero (device flag, may be null).
 template <typename T>
 void gemm_bf16x3(int ta, int tb, int M, int N, int K, T alpha, const T* A, ll lda, ll sA, const T* B,
-                 ll ldb, ll sB, T beta, T* C, ll ldc, ll sC, int nbatch, SplitScratch& ws, cudaStream_t s);
+                 ll ldb, ll sB, T beta, T* C, ll ldc, ll sC, int nbatch, SplitScratch& ws, cudaStream_t s,
+                 const int* skip = nullptr);
 
 }  // namespace dmrg2

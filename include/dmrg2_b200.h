@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define DMRG2_ABI_VERSION 1
+#define DMRG2_ABI_VERSION 2
 
 enum dmrg2_status {
   DMRG2_OK = 0,
@@ -71,6 +71,9 @@ typedef struct dmrg2_config {
   uint64_t seed;      /* seed for random initial states and Lanczos restarts */
   int svd_method;     /* truncation: 0 = eigen-decomposition of the reduced density matrix
                          (default), 1 = one-sided block Jacobi SVD of theta */
+  int precision;      /* H_eff arithmetic: 0 = FP64 (default); 1 = precision form: Lanczos on
+                         split-BF16 matvecs (tcgen05 tensor cores, FP32 accumulation), then
+                         refined with FP64 matvecs from the Ritz vector; energies are FP64 */
 } dmrg2_config;
 
 /* One row per sweep (left-to-right + right-to-left half sweep). */
@@ -90,6 +93,7 @@ typedef struct dmrg2_sweep_report {
   double svd_s;            /* device time of the SVD truncations */
   int jacobi_sweeps_max;
   double device_s;         /* device time of the whole sweep (CUDA events on the solver stream) */
+  long long lowprec_matvecs; /* precision form: matvecs on the split-BF16 operator */
 } dmrg2_sweep_report;
 
 /* ---------------------------------------------------------------- solver */

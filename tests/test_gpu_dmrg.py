@@ -203,3 +203,30 @@ def test_reference_bin_data_josephson_vs_oracle(golden_dir):
     eng, rep = gpu_run(W, A, sched, krylov_max=30, max_restarts=4, cutoff=1e-14)
     ref = O.dmrg2(W, A, sched, cutoff=1e-14)
     assert abs(rep[-1]["energy"] - ref["energy"]) <= 1e-10 * abs(ref["energy"])
+
+
+@pytest.mark.parametrize("model", ["heisenberg", "josephson"])
+def test_precision_form_matches_fp64(model):
+    """Precision form (Lanczos on split-BF16 tcgen05 matvecs, FP64 refinement) against
+    the plain FP64 form on the same inputs: energy to 1e-10 relative. Local
+    observables carry the vector error the energy-based Lanczos stop allows after
+    the FP32-level operator broke the S^z symmetry slightly (measured ~1e-7); the
+    bound stated for them is 5e-7. The split-BF16 operator is really used."""
+    if model == "heisenberg":
+        L, mpo, op = 16, M.heisenberg_mpo(16), M.SZ
+        mps = O.random_mps(L, 2, 8, seed=21)
+        sched = [16, 32, 32, 32, 32, 32]
+    else:
+        L = 10
+        mpo = M.josephson_mpo(L, n_max=2, E_J=2.0, E_C=1.0, n_g=0.25, phi=2 * np.pi * 0.1 / L, onsite="shifted")
+        op = np.diag(np.arange(5) - 2.0)
+        mps = O.random_mps(L, 5, 8, seed=22, dtype=np.complex128)
+        sched = [16, 32, 32, 32, 32]
+    kw = dict(krylov_max=30, max_restarts=4, cutoff=1e-14, tol=1e-300, min_sweeps=100)
+    e64, r64 = gpu_run(mpo, mps, sched, **kw)
+    esp, rsp = gpu_run(mpo, mps, sched, precision=1, **kw)
+    assert sum(r["lowprec_matvecs"] for r in rsp) > 0
+    assert sum(r["lowprec_matvecs"] for r in r64) == 0
+    E, Es = r64[-1]["energy"], rsp[-1]["energy"]
+    assert abs(E - Es) <= 1e-10 * abs(E)
+    np.testing.assert_allclose(esp.expect_local(op), e64.expect_local(op), atol=5e-7)
