@@ -486,20 +486,72 @@ def run_server_workload(args):
         print(json.dumps(line))
 
 
+# ----------------------------------------------------------------------------
+# precision form: Josephson array, plain FP64 vs split-BF16 matvecs
+# ----------------------------------------------------------------------------
+def run_precision_workload(args):
+    """Josephson junction array L=24, d=5 (n in -2..2), E_C=1, E_J=2, n_g=0.25,
+    A=2 pi 0.1/L, D=4, complex128; seeded complex Gaussian chi=16 start, chi_max=128,
+    10 sweeps; the plain form and the precision form on the same inputs."""
+    import torch
+    import dmrg2
+    from dmrg2 import models as P
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    L, nmax, chi = 24, 2, 128
+    mpo = P.josephson(L, n_max=nmax, E_J=2.0, E_C=1.0, n_g=0.25, phi=2 * np.pi * 0.1 / L, onsite="shifted")
+    mps = P.random_mps(L, 2 * nmax + 1, 16, seed=0, dtype=np.complex128)
+    nop = np.diag(np.arange(2 * nmax + 1) - float(nmax)).astype(np.complex128)
+    sched = [chi] * (args.steps if args.steps != 3 else 10)
+    out = {}
+    for name, prec in (("plain", 0), ("split", 1)):
+        eng = dmrg2.DMRG2GPU(L, 2 * nmax + 1, chi, dtype=np.complex128, krylov_max=KRYLOV, max_restarts=RESTARTS,
+                             cutoff=1e-12, tol=1e-300, min_sweeps=10 ** 6, precision=prec, device=local)
+        eng.set_mpo(mpo)
+        eng.set_mps(mps)
+        rep = eng.run(schedule=sched)
+        out[name] = {"energy": rep[-1]["energy"], "device_s": sum(r["device_s"] for r in rep),
+                     "heff_s": sum(r["heff_s"] for r in rep), "svd_s": sum(r["svd_s"] for r in rep),
+                     "matvecs": sum(r["matvecs"] for r in rep),
+                     "lowprec_matvecs": sum(r["lowprec_matvecs"] for r in rep),
+                     "n": eng.expect_local(nop), "max_bond": max(eng.bond_dims())}
+        eng.close()
+    p, q = out["plain"], out["split"]
+    line = {
+        "metric": "sweeps/s (Josephson L=24 d=5 chi=128 complex128, precision form vs FP64 plain form)",
+        "value": len(sched) / q["device_s"], "unit": "sweeps/s", "n_gpus": 1, "steps": len(sched), "warmup": 0,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128 (split-bf16 matvecs)",
+        "data": "synthetic (seeded complex Gaussian MPS, Josephson MPO)", "impl": "ours",
+        "config": {"workload": "josephson_L24_d5_chi128_precision", "E_C": 1.0, "E_J": 2.0, "n_g": 0.25,
+                   "A": "2 pi 0.1 / L", "sweeps": len(sched), "cutoff": 1e-12, "krylov_max": KRYLOV},
+        "plain": {"sweeps_per_s": len(sched) / p["device_s"], "energy": p["energy"], "matvecs": p["matvecs"],
+                  "heff_s": p["heff_s"], "svd_s": p["svd_s"]},
+        "split": {"sweeps_per_s": len(sched) / q["device_s"], "energy": q["energy"], "matvecs": q["matvecs"],
+                  "lowprec_matvecs": q["lowprec_matvecs"], "heff_s": q["heff_s"], "svd_s": q["svd_s"]},
+        "rel_dE_split_vs_fp64": abs(q["energy"] - p["energy"]) / abs(p["energy"]),
+        "max_abs_dn_split_vs_fp64": float(np.max(np.abs(np.asarray(q["n"]) - np.asarray(p["n"])))),
+        "max_bond": q["max_bond"],
+    }
+    if rank == 0:
+        print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["sweep", "batched", "served"], default="sweep")
+    ap.add_argument("--workload", choices=["sweep", "batched", "served", "precision"], default="sweep")
     ap.add_argument("--requests", type=int, default=0)
     ap.add_argument("--max-active", type=int, default=12)
     ap.add_argument("--plain-sample", type=int, default=24)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.workload != "sweep" and args.impl == "ours":
+    if args.workload == "precision" and args.impl == "ours":
+        run_precision_workload(args)
+    elif args.workload != "sweep" and args.impl == "ours":
         run_server_workload(args)
     elif args.impl == "reference":
         run_reference(args)

@@ -2,11 +2,14 @@
 
     python -m dmrg2.microbench heff --chi 256 [--d 2 --D 5 --complex --reps 50]
     python -m dmrg2.microbench svd  --n 512   [--keep 256 --complex --reps 5]
+    python -m dmrg2.microbench gemm --m 1024 --n 4096 --k 1024 [--complex --reps 5]
 
 heff runs dmrg2_op_heff_noalloc on device-resident operands (torch tensors)
 and reports the device time per matvec (CUDA events) and its algorithmic
 TFLOP/s; svd runs the truncated split through dmrg2_op_svd (host buffers,
-so the time includes the copies). Both are the fixed small workloads the
+so the time includes the copies); gemm runs the FP64 DMMA GEMM and the
+split-BF16 tcgen05 GEMM of the precision form on the same operands (host
+buffers) and reports their difference. They are the fixed small workloads the
 kernel profiles are taken on.
 """
 from __future__ import annotations
@@ -79,21 +82,42 @@ def bench_svd(n, keep, cplx, reps, seed=0):
     return {"op": "svd", "n": n, "keep": keep, "complex": cplx, "ms_per_call_host": 1e3 * float(np.median(times[1:]))}
 
 
+def bench_gemm(m, n, k, cplx, reps, seed=0):
+    rng = np.random.default_rng(seed)
+    A, B = _rnd(rng, (m, k), cplx), _rnd(rng, (k, n), cplx)
+    out = {}
+    for name, f in (("fp64_dmma", dmrg2.gemm), ("split_bf16_tcgen05", dmrg2.gemm_bf16x3)):
+        f(A, B)
+        t = time.perf_counter()
+        for _ in range(reps):
+            C = f(A, B)
+        out[name] = {"ms_per_call_host": 1e3 * (time.perf_counter() - t) / reps}
+        out[name]["C"] = C
+    err = np.abs(out["split_bf16_tcgen05"].pop("C") - out["fp64_dmma"].pop("C")).max()
+    return {"op": "gemm", "m": m, "n": n, "k": k, "complex": cplx, **out,
+            "max_abs_diff": float(err), "flops": (8.0 if cplx else 2.0) * m * n * k}
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("op", choices=["heff", "svd"])
+    ap.add_argument("op", choices=["heff", "svd", "gemm"])
+    ap.add_argument("--m", type=int, default=1024)
+    ap.add_argument("--k", type=int, default=1024)
     ap.add_argument("--chi", type=int, default=256)
     ap.add_argument("--d", type=int, default=2)
     ap.add_argument("--D", type=int, default=5)
-    ap.add_argument("--n", type=int, default=512)
+    ap.add_argument("--n", type=int, default=0)
     ap.add_argument("--keep", type=int, default=0)
     ap.add_argument("--complex", action="store_true")
     ap.add_argument("--reps", type=int, default=0)
     a = ap.parse_args()
     if a.op == "heff":
         r = bench_heff(a.chi, a.d, a.D, a.complex, a.reps or 50)
+    elif a.op == "svd":
+        n = a.n or 512
+        r = bench_svd(n, a.keep or n // 2, a.complex, a.reps or 5)
     else:
-        r = bench_svd(a.n, a.keep or a.n // 2, a.complex, a.reps or 5)
+        r = bench_gemm(a.m, a.n or 4096, a.k, a.complex, a.reps or 5)
     print(json.dumps(r))
 
 
