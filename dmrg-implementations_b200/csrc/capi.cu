@@ -326,6 +326,8 @@ EngineConfig engine_config(const dmrg2_config* cfg) {
   c.svd_method = cfg->svd_method;
   if (cfg->precision != 0 && cfg->precision != 1) throw std::invalid_argument("unknown precision form");
   c.precision = cfg->precision;
+  if (cfg->single_site != 0 && cfg->single_site != 1) throw std::invalid_argument("single_site must be 0 or 1");
+  c.single_site = cfg->single_site;
   return c;
 }
 void check_pos(std::initializer_list<int> v) {

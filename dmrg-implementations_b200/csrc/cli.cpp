@@ -39,7 +39,7 @@ struct Args {
   double delta = 1.0;
   std::vector<int> schedule;
   double cutoff = 0.0, tol = 1e-10, lanczos_tol = 0.0;
-  int krylov = 0, restarts = 0, precision = 0;
+  int krylov = 0, restarts = 0, precision = 0, single_site = 0;
   unsigned long long seed = 42;
   std::string init;
   std::string json;
@@ -114,6 +114,7 @@ int solve(const Args& a, const Mpo& m, bool default_neel, double exact, double e
   cfg.cutoff = a.cutoff;
   cfg.seed = a.seed;
   cfg.precision = a.precision;
+  cfg.single_site = a.single_site;
   dmrg2_handle* h = nullptr;
   if (dmrg2_create(&cfg, &h) != DMRG2_OK) return fail(nullptr, "create");
   std::vector<const void*> W(m.L);
@@ -211,6 +212,7 @@ int main(int argc, char** argv) {
     if (s == "--seed") { a.seed = std::strtoull(next("--seed"), nullptr, 10); continue; }
     if (s == "--init") { a.init = next("--init"); continue; }
     if (s == "--json") { a.json = next("--json"); continue; }
+    if (s == "--single-site") { a.single_site = 1; continue; }
     if (s == "--precision") {
       const std::string v = next("--precision");
       if (v != "plain" && v != "split") { std::fprintf(stderr, "--precision takes plain or split\n"); std::exit(1); }

@@ -33,20 +33,19 @@ __global__ void __launch_bounds__(128)
   }
 }
 
-// step 2 of the matvec: Y[a] = WWt X[a] for every a (MPO mixing, FP64)
+// step 2 of the matvec: Y[a] = W X[a] for every a (MPO mixing, FP64); X[a] is Kin x cR,
+// Y[a] is Kout x cR
 template <typename T>
-static void heff_mix(const T* X, const T* WWt, T* Y, int cL, int cR, int d, int Dl, int Dr, const int* skip,
+static void mix_rows(const T* X, const T* W, T* Y, int cL, int cR, int Kin, int Kout, const int* skip,
                      cudaStream_t s) {
-  const ll dd = (ll)d * d;
-  const int Kin = (int)(Dl * dd), Kout = (int)(dd * Dr);
   if (Kin <= 32 && Kout <= 32 && cL <= 65535) {
     dim3 grid(ceil_div(cR, 128), cL);
-    mpo_mix_kernel<T, 32><<<grid, 128, 0, s>>>(X, WWt, Y, Kin, Kout, cR, (ll)Kin * cR, (ll)Kout * cR, skip);
+    mpo_mix_kernel<T, 32><<<grid, 128, 0, s>>>(X, W, Y, Kin, Kout, cR, (ll)Kin * cR, (ll)Kout * cR, skip);
     DMRG2_CHECK_LAUNCH();
   } else {
     Gemm<T> g;
     g.M = Kout; g.N = cR; g.K = Kin;
-    g.A = WWt; g.lda = Kin; g.sA1 = 0;
+    g.A = W; g.lda = Kin; g.sA1 = 0;
     g.B = X; g.ldb = cR; g.sB1 = (ll)Kin * cR;
     g.C = Y; g.ldc = cR; g.sC1 = (ll)Kout * cR;
     g.nb1 = cL; g.skip = skip;
@@ -62,7 +61,7 @@ void heff_apply_split(const T* Lenv, const T* Renv, const T* WWt, const T* in, T
   // step 1: X[a][w][.] = L[a][w][:] theta, Dl batches sharing theta
   gemm_bf16x3<T>(0, 0, cL, (int)(dd * cR), cL, one, Lenv, (ll)Dl * cL, cL, in, dd * cR, 0, zero, X,
                  (ll)Dl * dd * cR, dd * cR, Dl, ws, s, skip);
-  heff_mix(X, WWt, Y, cL, cR, d, Dl, Dr, skip, s);
+  mix_rows(X, WWt, Y, cL, cR, (int)(Dl * dd), (int)(dd * Dr), skip, s);
   // step 3: out[(a,p,q)][f] = sum_(n,e) Y[(a,p,q)][(n,e)] R[f][(n,e)]
   gemm_bf16x3<T>(0, 1, (int)(cL * dd), cR, Dr * cR, one, Y, (ll)Dr * cR, 0, Renv, (ll)Dr * cR, 0, zero, out, cR,
                  0, 1, ws, s, skip);
@@ -81,7 +80,7 @@ void heff_apply(const T* Lenv, const T* Renv, const T* WWt, const T* in, T* out,
     g.nb1 = Dl; g.skip = skip;
     launch_gemm(g, s);
   }
-  heff_mix(X, WWt, Y, cL, cR, d, Dl, Dr, skip, s);
+  mix_rows(X, WWt, Y, cL, cR, (int)(Dl * dd), (int)(dd * Dr), skip, s);
   {
     Gemm<T> g;
     g.tb = true;
@@ -102,6 +101,45 @@ void heff_apply(const T* Lenv, const T* Renv, const T* WWt, const T* in, T* out,
     }
     launch_gemm(g, s);
   }
+}
+
+template <typename T>
+void heff1_apply(const T* Lenv, const T* Renv, const T* WmixL, const T* in, T* out, T* X, T* Y, int cL, int cR,
+                 int d, int Dl, int Dr, const int* skip, cudaStream_t s) {
+  {
+    Gemm<T> g;  // X[a][w][(s,e)] = sum_c L[a][w][c] A[c][(s,e)]
+    g.M = cL; g.N = d * cR; g.K = cL;
+    g.A = Lenv; g.lda = (ll)Dl * cL; g.sA1 = cL;
+    g.B = in; g.ldb = (ll)d * cR; g.sB1 = 0;
+    g.C = X; g.ldc = (ll)Dl * d * cR; g.sC1 = (ll)d * cR;
+    g.nb1 = Dl; g.skip = skip;
+    launch_gemm(g, s);
+  }
+  mix_rows(X, WmixL, Y, cL, cR, Dl * d, d * Dr, skip, s);  // Y[a][(t,w')][e]
+  {
+    Gemm<T> g;  // out[(a,t)][f] = sum_(w',e) Y[(a,t)][(w',e)] R[f][(w',e)]
+    g.tb = true;
+    g.M = cL * d; g.N = cR; g.K = Dr * cR;
+    g.A = Y; g.lda = (ll)Dr * cR;
+    g.B = Renv; g.ldb = (ll)Dr * cR;
+    g.C = out; g.ldc = cR;
+    g.skip = skip;
+    const int tiles = ceil_div(g.M, GemmTile<T>::BM) * ceil_div(g.N, GemmTile<T>::BN);
+    int sk = 1;
+    while (sk < Dl && sk < 8 && tiles * sk < 2 * 148 && (ll)g.K / (sk * 2) >= 4 * GemmTile<T>::BK) sk *= 2;
+    if (sk > Dl) sk = Dl;
+    if (sk > 1) {
+      g.splitk = sk;
+      g.ws = X;  // X holds Dl * cL * d * cR >= splitk * cL * d * cR partial products
+    }
+    launch_gemm(g, s);
+  }
+}
+
+double heff1_flops(int cL, int cR, int d, int Dl, int Dr, bool cplx) {
+  const double f = 2.0 * Dl * cL * ((double)d * cR) * cL + 2.0 * cL * ((double)d * Dr) * cR * ((double)Dl * d) +
+                   2.0 * ((double)cL * d) * cR * ((double)Dr * cR);
+  return cplx ? 4.0 * f : f;
 }
 
 double heff_flops(int cL, int cR, int d, int Dl, int Dr, bool cplx) {
@@ -241,6 +279,8 @@ void build_wmix_right(const T* W, int Dl, int Dr, int d, std::vector<T>& out) {
 #define INST(T)                                                                                 \
   template void heff_apply<T>(const T*, const T*, const T*, const T*, T*, T*, T*, int, int, int, \
                               int, int, const int*, cudaStream_t);                               \
+  template void heff1_apply<T>(const T*, const T*, const T*, const T*, T*, T*, T*, int, int, int,  \
+                               int, int, const int*, cudaStream_t);                              \
   template void heff_apply_split<T>(const T*, const T*, const T*, const T*, T*, T*, T*, int, int,   \
                                     int, int, int, SplitScratch&, const int*, cudaStream_t);     \
   template void env_left<T>(const T*, const T*, const T*, T*, T*, T*, int, int, int, int, int,  \

@@ -31,6 +31,14 @@ template <typename T>
 void heff_apply_split(const T* Lenv, const T* Renv, const T* WWt, const T* in, T* out, T* X, T* Y, int cL,
                       int cR, int d, int Dl, int Dr, SplitScratch& ws, const int* skip, cudaStream_t s);
 
+// Single-site H_eff (reference: apply_heff, gpu-rocm/dmrg-gpu/src/dmrg_gpu_impl.h):
+//   out[a][t][f] = sum L[a][w][c] A[c][s][e] W[w][w'][s][t] R[f][w'][e], with
+//   WmixL[(t,w')][(w,s)] = W[w][w'][s][t] (the left-environment mixing matrix)
+template <typename T>
+void heff1_apply(const T* Lenv, const T* Renv, const T* WmixL, const T* in, T* out, T* X, T* Y, int cL, int cR,
+                 int d, int Dl, int Dr, const int* skip, cudaStream_t s);
+double heff1_flops(int cL, int cR, int d, int Dl, int Dr, bool cplx);
+
 // algorithmic real flops of one heff_apply
 double heff_flops(int cL, int cR, int d, int Dl, int Dr, bool cplx);
 double env_flops(int chi_in, int chi_out, int d, int Dl, int Dr, bool cplx);

@@ -44,6 +44,8 @@ class Engine final : public EngineBase {
     if (cfg_.d < 1) throw std::runtime_error("d must be >= 1");
     if (cfg_.chi_max < 1) throw std::runtime_error("chi_max must be >= 1");
     if (cfg_.krylov_max < 2) cfg_.krylov_max = 2;
+    if (cfg_.single_site && (cfg_.svd_method != 0 || cfg_.precision != 0))
+      throw std::invalid_argument("single-site sweeps use the density-matrix truncation and FP64 matvecs");
     L_ = cfg_.L;
     d_ = cfg_.d;
     DMRG2_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
@@ -237,8 +239,12 @@ class Engine final : public EngineBase {
       auto ts = std::chrono::steady_clock::now();
       DMRG2_CUDA(cudaEventRecord(ev_s0_, st_));
       double e = 0.0;
-      for (int i = 0; i + 1 < L_; ++i) e = optimize_bond(i, 'R', schedule[sw], ss);
-      for (int i = L_ - 2; i >= 0; --i) e = optimize_bond(i, 'L', schedule[sw], ss);
+      if (cfg_.single_site) {
+        e = sweep1(schedule[sw], ss);
+      } else {
+        for (int i = 0; i + 1 < L_; ++i) e = optimize_bond(i, 'R', schedule[sw], ss);
+        for (int i = L_ - 2; i >= 0; --i) e = optimize_bond(i, 'L', schedule[sw], ss);
+      }
       DMRG2_CUDA(cudaEventRecord(ev_s1_, st_));
       DMRG2_CUDA(cudaStreamSynchronize(st_));
       float ms = 0.f;
@@ -407,7 +413,8 @@ class Engine final : public EngineBase {
     T one = ST<T>::one();
     DMRG2_CUDA(cudaMemcpyAsync(lenv_[0], &one, sizeof(T), cudaMemcpyHostToDevice, st_));
     DMRG2_CUDA(cudaMemcpyAsync(renv_[L_], &one, sizeof(T), cudaMemcpyHostToDevice, st_));
-    for (int i = L_ - 1; i >= 2; --i)
+    const int lowest = cfg_.single_site ? 1 : 2;  // single-site sweeps start with R[1]
+    for (int i = L_ - 1; i >= lowest; --i)
       env_right(renv_[i + 1], mps_[i], wmr_[i], renv_[i], X_, Y_, dims_[i + 1], dims_[i], d_, Dl_[i],
                 Dr_[i], st_);
   }
@@ -467,6 +474,89 @@ class Engine final : public EngineBase {
     ss.lanczos_iters += r.iters;
     if (!r.converged) ss.lanczos_unconverged += 1;
     return r.energy;
+  }
+
+  // ---------------------------------------------------------------- single-site sweep
+  // (reference: DMRGGPU::sweep_left_to_right / sweep_right_to_left, optimize_site and
+  // svd_and_update_mps, gpu-rocm/dmrg-gpu/src/dmrg_gpu_impl.h:1119-1450): every site is
+  // optimised with the one-site H_eff; left to right, A[i] = U and S Vh moves into A[i+1];
+  // right to left, A[i] = Vh and U S moves into A[i-1]; the end sites are optimised
+  // without a split. Bond dimensions can only stay or shrink.
+  double sweep1(int chi, SweepStats& ss) {
+    double e = 0.0;
+    for (int i = 0; i + 1 < L_; ++i) {
+      e = lanczos1(i, ss);
+      split1(i, 'R', chi, ss);
+      env_left(lenv_[i], mps_[i], wml_[i], lenv_[i + 1], X_, Y_, dims_[i], dims_[i + 1], d_, Dl_[i], Dr_[i], st_);
+    }
+    e = lanczos1(L_ - 1, ss);
+    DMRG2_CUDA(cudaMemcpyAsync(mps_[L_ - 1], theta_, sizeof(T) * (size_t)dims_[L_ - 1] * d_ * dims_[L_],
+                               cudaMemcpyDeviceToDevice, st_));
+    for (int i = L_ - 1; i >= 1; --i) {
+      e = lanczos1(i, ss);
+      split1(i, 'L', chi, ss);
+      env_right(renv_[i + 1], mps_[i], wmr_[i], renv_[i], X_, Y_, dims_[i + 1], dims_[i], d_, Dl_[i], Dr_[i], st_);
+    }
+    e = lanczos1(0, ss);
+    DMRG2_CUDA(cudaMemcpyAsync(mps_[0], theta_, sizeof(T) * (size_t)dims_[0] * d_ * dims_[1],
+                               cudaMemcpyDeviceToDevice, st_));
+    return e;
+  }
+
+  double lanczos1(int i, SweepStats& ss) {
+    const int cL = dims_[i], cR = dims_[i + 1];
+    const int Dl = Db_[i], Dr = Db_[i + 1];
+    const ll n = (ll)cL * d_ * cR;
+    DMRG2_CUDA(cudaMemcpyAsync(theta_, mps_[i], sizeof(T) * (size_t)n, cudaMemcpyDeviceToDevice, st_));
+    auto mv = [&](const T* in, T* out, const int* skip) {
+      heff1_apply(lenv_[i], renv_[i + 1], wml_[i], in, out, X_, Y_, cL, cR, d_, Dl, Dr, skip, st_);
+    };
+    LanczosResult r = lanczos_solve<T>(lw_, theta_, n, cfg_.krylov_max, cfg_.lanczos_tol, cfg_.max_restarts,
+                                       cfg_.seed + 7919u * (unsigned)i, mv, st_);
+    ss.heff_s += r.matvec_s;
+    ss.matvecs += r.matvecs;
+    ss.heff_flops += heff1_flops(cL, cR, d_, Dl, Dr, ST<T>::cplx) * r.matvecs;
+    ss.lanczos_iters += r.iters;
+    if (!r.converged) ss.lanczos_unconverged += 1;
+    return r.energy;
+  }
+
+  void split1(int i, char dir, int chi, SweepStats& ss) {
+    const int cL = dims_[i], cR = dims_[i + 1];
+    DMRG2_CUDA(cudaEventRecord(ev_c_, st_));
+    SvdOut o;
+    if (dir == 'R') {  // theta (cL d) x cR: A[i] = U, then A[i+1] <- (S Vh) A[i+1]
+      o = eig_split(ew_, theta_, cL * d_, cR, 'R', chi, cfg_.cutoff, false, mps_[i], tmp_, st_);
+      const int k = o.k, cR2 = dims_[i + 2];
+      Gemm<T> g;
+      g.M = k; g.N = d_ * cR2; g.K = cR;
+      g.A = tmp_; g.lda = cR;
+      g.B = mps_[i + 1]; g.ldb = (ll)d_ * cR2;
+      g.C = svdX_; g.ldc = (ll)d_ * cR2;
+      launch_gemm(g, st_);
+      DMRG2_CUDA(cudaMemcpyAsync(mps_[i + 1], svdX_, sizeof(T) * (size_t)k * d_ * cR2, cudaMemcpyDeviceToDevice,
+                                 st_));
+      dims_[i + 1] = k;
+    } else {  // theta cL x (d cR): A[i] = Vh, then A[i-1] <- A[i-1] (U S)
+      o = eig_split(ew_, theta_, cL, d_ * cR, 'L', chi, cfg_.cutoff, false, tmp_, mps_[i], st_);
+      const int k = o.k, cL2 = dims_[i - 1];
+      Gemm<T> g;
+      g.M = cL2 * d_; g.N = k; g.K = cL;
+      g.A = mps_[i - 1]; g.lda = cL;
+      g.B = tmp_; g.ldb = k;
+      g.C = svdX_; g.ldc = k;
+      launch_gemm(g, st_);
+      DMRG2_CUDA(cudaMemcpyAsync(mps_[i - 1], svdX_, sizeof(T) * (size_t)cL2 * d_ * k, cudaMemcpyDeviceToDevice,
+                                 st_));
+      dims_[i] = k;
+    }
+    DMRG2_CUDA(cudaEventRecord(ev_d_, st_));
+    DMRG2_CUDA(cudaEventSynchronize(ev_d_));
+    float ms = 0.f;
+    DMRG2_CUDA(cudaEventElapsedTime(&ms, ev_c_, ev_d_));
+    ss.svd_s += ms * 1e-3;
+    ss.trunc_err_max = std::max(ss.trunc_err_max, o.trunc_err);
+    ss.trunc_err_sum += o.trunc_err;
   }
 
   void svd_split(int i, char dir, int chi, SweepStats& ss) {

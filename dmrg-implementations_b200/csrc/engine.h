@@ -27,6 +27,7 @@ struct EngineConfig {
   int jacobi_max_sweeps = 40;
   int svd_method = 0;          // 0: reduced density matrix eigensolver, 1: one-sided block Jacobi
   int precision = 0;           // 0: FP64 matvecs; 1: split-BF16 matvecs on tcgen05, then FP64 refinement
+  int single_site = 0;         // 1: single-site sweeps (the reference's dmrg-gpu driver)
   unsigned seed = 42;
 };
 

@@ -50,7 +50,7 @@ class Config(ctypes.Structure):
         ("tol", ctypes.c_double), ("krylov_max", ctypes.c_int), ("lanczos_tol", ctypes.c_double),
         ("max_restarts", ctypes.c_int), ("cutoff", ctypes.c_double), ("min_sweeps", ctypes.c_int),
         ("device", ctypes.c_int), ("seed", ctypes.c_uint64), ("svd_method", ctypes.c_int),
-        ("precision", ctypes.c_int),
+        ("precision", ctypes.c_int), ("single_site", ctypes.c_int),
     ]
 
 
@@ -199,7 +199,7 @@ class DMRG2GPU:
 
     def __init__(self, L, d, chi_max, D_mpo=None, tol=1e-10, dtype=np.float64, *, krylov_max=100,
                  lanczos_tol=1e-12, max_restarts=0, cutoff=1e-14, min_sweeps=2, device=0, seed=42,
-                 svd_method=0, precision=0):
+                 svd_method=0, precision=0, single_site=False):
         lib = load_library()
         self.L, self.d, self.chi_max, self.D_mpo = int(L), int(d), int(chi_max), D_mpo
         self.dtype = np.dtype(dtype)
@@ -207,7 +207,8 @@ class DMRG2GPU:
         cfg = Config(L=self.L, d=self.d, chi_max=self.chi_max, dtype=self.code, tol=tol,
                      krylov_max=krylov_max, lanczos_tol=lanczos_tol, max_restarts=max_restarts,
                      cutoff=(cutoff if cutoff > 0 else -1.0), min_sweeps=min_sweeps, device=device,
-                     seed=seed, svd_method=svd_method, precision=int(precision))
+                     seed=seed, svd_method=svd_method, precision=int(precision),
+                     single_site=int(bool(single_site)))
         h = ctypes.c_void_p()
         _check(lib.dmrg2_create(ctypes.byref(cfg), ctypes.byref(h)), None, "dmrg2_create")
         self._h = h

@@ -74,6 +74,9 @@ typedef struct dmrg2_config {
   int precision;      /* H_eff arithmetic: 0 = FP64 (default); 1 = precision form: Lanczos on
                          split-BF16 matvecs (tcgen05 tensor cores, FP32 accumulation), then
                          refined with FP64 matvecs from the Ritz vector; energies are FP64 */
+  int single_site;    /* 0 = two-site sweeps (default); 1 = single-site sweeps, the reference's
+                         dmrg-gpu driver (gpu-rocm/dmrg-gpu/src/dmrg_gpu_impl.h:1119-1450):
+                         bond dimensions stay at those of the initial MPS (or shrink) */
 } dmrg2_config;
 
 /* One row per sweep (left-to-right + right-to-left half sweep). */

@@ -268,6 +268,99 @@ def dmrg2(mpo, mps, schedule, cutoff=0.0, tol=1e-10, lanczos_tol=1e-12,
     return out
 
 
+# ----------------------------------------------------------------------------
+# single-site sweep (the reference's dmrg-gpu driver)
+# ----------------------------------------------------------------------------
+
+def apply_heff1(Lenv, Renv, W, A):
+    """A'[a,t,f] = L[a,w,c] A[c,s,e] W[w,v,s,t] R[f,v,e]: the one-site H_eff of
+    gpu-rocm/dmrg-gpu/src/dmrg_gpu_impl.h (apply_heff), restated with tensordots."""
+    X = np.tensordot(Lenv, A, axes=(2, 0))                 # a w s e
+    Y = np.tensordot(X, W, axes=([1, 2], [0, 2]))          # a e v t
+    return np.tensordot(Y, Renv, axes=([1, 2], [2, 1]))    # a t f
+
+
+def optimize_one_site(Lenv, Renv, W, A0, maxiter=50, tol=1e-12, dense_below=32):
+    """Lowest eigenpair of the one-site H_eff (ARPACK, or dense below ``dense_below``)."""
+    shape = A0.shape
+    n = int(np.prod(shape))
+    dtype = np.result_type(A0.dtype, Lenv.dtype, Renv.dtype, W.dtype)
+
+    def mv(v):
+        return apply_heff1(Lenv, Renv, W, v.reshape(shape)).ravel()
+
+    if n < dense_below:
+        H = np.empty((n, n), dtype)
+        e = np.zeros(n, dtype)
+        for j in range(n):
+            e[:] = 0
+            e[j] = 1
+            H[:, j] = mv(e)
+        H = 0.5 * (H + H.conj().T)
+        w, V = np.linalg.eigh(H)
+        return float(w[0]), V[:, 0].reshape(shape)
+    op = LinearOperator((n, n), matvec=mv, dtype=dtype)
+    w, V = eigsh(op, k=1, v0=A0.ravel().astype(dtype), which="SA", maxiter=maxiter * 10, tol=tol)
+    return float(w[0].real), V[:, 0].reshape(shape)
+
+
+def dmrg1(mpo, mps, schedule, cutoff=0.0, tol=1e-10, lanczos_tol=1e-12, lanczos_maxiter=50,
+          min_sweeps=2):
+    """Serial single-site DMRG, restating DMRGGPU::run / sweep_left_to_right /
+    sweep_right_to_left / optimize_site / svd_and_update_mps
+    (gpu-rocm/dmrg-gpu/src/dmrg_gpu_impl.h:1119-1470).
+
+    Left to right, sites 0..L-2 are optimised and split (A[i] = U, S Vh absorbed
+    into A[i+1]); site L-1 is optimised without a split. Right to left, sites
+    L-1..1 are optimised and split (A[i] = Vh, U S absorbed into A[i-1]); site 0
+    is optimised without a split and its eigenvalue is the sweep energy. The
+    truncation is the oracle's truncated_svd (max bond, absolute cutoff), so
+    bond dimensions never grow past those of the initial MPS.
+    """
+    L = len(mpo)
+    A = right_canonicalize(mps)
+    dtype = np.result_type(A[0].dtype, mpo[0].dtype)
+    A = [a.astype(dtype) for a in A]
+    Renv = [None] * (L + 1)
+    Lenv = [None] * (L + 1)
+    Renv[L] = np.ones((1, 1, 1), dtype)
+    Lenv[0] = np.ones((1, 1, 1), dtype)
+    for i in range(L - 1, 0, -1):
+        Renv[i] = update_right_env(Renv[i + 1], A[i], mpo[i])
+    out = dict(energies=[], trunc_err_max=[], max_bond=[], sweeps=0)
+    E_prev, E = None, 0.0
+    for sweep, chi in enumerate(schedule):
+        tmax = 0.0
+        for i in range(L - 1):
+            E, th = optimize_one_site(Lenv[i], Renv[i + 1], mpo[i], A[i], lanczos_maxiter, lanczos_tol)
+            cl, d, cr = th.shape
+            U, S, Vh, te = truncated_svd(th.reshape(cl * d, cr), chi, cutoff)
+            tmax = max(tmax, te)
+            A[i] = U.reshape(cl, d, len(S))
+            A[i + 1] = np.tensordot(S[:, None] * Vh, A[i + 1], axes=(1, 0))
+            Lenv[i + 1] = update_left_env(Lenv[i], A[i], mpo[i])
+        E, A[L - 1] = optimize_one_site(Lenv[L - 1], Renv[L], mpo[L - 1], A[L - 1], lanczos_maxiter, lanczos_tol)
+        for i in range(L - 1, 0, -1):
+            E, th = optimize_one_site(Lenv[i], Renv[i + 1], mpo[i], A[i], lanczos_maxiter, lanczos_tol)
+            cl, d, cr = th.shape
+            U, S, Vh, te = truncated_svd(th.reshape(cl, d * cr), chi, cutoff)
+            tmax = max(tmax, te)
+            A[i] = Vh.reshape(len(S), d, cr)
+            A[i - 1] = np.tensordot(A[i - 1], U * S, axes=(2, 0))
+            Renv[i] = update_right_env(Renv[i + 1], A[i], mpo[i])
+        E, A[0] = optimize_one_site(Lenv[0], Renv[1], mpo[0], A[0], lanczos_maxiter, lanczos_tol)
+        out["energies"].append(E)
+        out["trunc_err_max"].append(tmax)
+        out["max_bond"].append(max(a.shape[2] for a in A))
+        out["sweeps"] = sweep + 1
+        if E_prev is not None and sweep + 1 >= min_sweeps and abs(E - E_prev) < tol:
+            break
+        E_prev = E
+    out["energy"] = E
+    out["mps"] = A
+    return out
+
+
 def ramp_schedule(chis, n_sweeps):
     """Spread the chi values of ``chis`` evenly over ``n_sweeps`` sweeps."""
     per = max(1, n_sweeps // len(chis))

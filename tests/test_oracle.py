@@ -132,3 +132,24 @@ def test_oracle_observables_match_ed():
     nd = O.expect_local(r["mps"], n)
     ned = [np.vdot(v, M._site_op(n, i, L, 3) @ v).real for i in range(L)]
     np.testing.assert_allclose(nd.real, ned, atol=1e-8)
+
+
+def test_single_site_oracle_reaches_ed_at_exact_bond_dimension():
+    """Single-site sweeps (the reference's dmrg-gpu algorithm) from a full-rank
+    random MPS: at an exact bond dimension the energy is the ED ground energy."""
+    L = 8
+    mpo = M.heisenberg_mpo(L)
+    res = O.dmrg1(mpo, O.random_mps(L, 2, 16, seed=3), [16] * 8, cutoff=0.0)
+    e_ed = M.ground_energy(M.ham_heisenberg(L))
+    assert abs(res["energy"] - e_ed) < 1e-10 * abs(e_ed)
+    # the MPS it returns has that energy
+    assert abs(O.mpo_expectation(res["mps"], mpo).real / O.mps_norm2(res["mps"]).real - e_ed) < 1e-9
+
+
+def test_single_site_heff_matches_dense():
+    rng = np.random.default_rng(4)
+    cL, d, cR, D = 3, 2, 4, 5
+    Lenv, Renv = rng.standard_normal((cL, D, cL)), rng.standard_normal((cR, D, cR))
+    W, A = rng.standard_normal((D, D, d, d)), rng.standard_normal((cL, d, cR))
+    ref = np.einsum("awc,cse,wvst,fve->atf", Lenv, A, W, Renv)
+    np.testing.assert_allclose(O.apply_heff1(Lenv, Renv, W, A), ref, atol=1e-12)
