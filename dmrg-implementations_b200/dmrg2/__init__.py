@@ -177,6 +177,31 @@ def _ptr(a):
     return a.ctypes.data_as(ctypes.c_void_p)
 
 
+def minimal_bonds(As):
+    """The same MPS with every bond at most min(d^i, d^(L-i)) (exact QR sweeps, no truncation).
+
+    Generators such as quimb's random MPS keep one bond dimension on every bond, above
+    what the first and last sites can carry; the engine allocates the minimal bonds.
+    """
+    As = [np.asarray(A) for A in As]
+    L = len(As)
+    if L < 2:
+        return As
+    for i in range(L - 1):  # left to right: bond i+1 <= chi_l * d
+        cl, d, cr = As[i].shape
+        if cr > cl * d:
+            Q, R = np.linalg.qr(As[i].reshape(cl * d, cr))
+            As[i] = Q.reshape(cl, d, Q.shape[1])
+            As[i + 1] = np.tensordot(R, As[i + 1], axes=(1, 0))
+    for i in range(L - 1, 0, -1):  # right to left: bond i <= d * chi_r
+        cl, d, cr = As[i].shape
+        if cl > d * cr:
+            Q, R = np.linalg.qr(As[i].reshape(cl, d * cr).T)
+            As[i] = Q.T.reshape(Q.shape[1], d, cr)
+            As[i - 1] = np.tensordot(As[i - 1], R.T, axes=(2, 0))
+    return [np.ascontiguousarray(A) for A in As]
+
+
 def _mpo4(Ws):
     """Accept boundary tensors given as 3-D arrays (npz fixture format)."""
     L = len(Ws)
@@ -250,7 +275,7 @@ class DMRG2GPU:
         _check(self._lib.dmrg2_set_mpo(self._h, ptrs, Dl, None, REFERENCE), self._h, "set_mpo")
 
     def set_mps(self, As):
-        As = [_prep(A, self.code) for A in As]
+        As = minimal_bonds([_prep(A, self.code) for A in As])
         dims = [As[0].shape[0]] + [A.shape[2] for A in As]
         ptrs = (ctypes.c_void_p * self.L)(*[A.ctypes.data for A in As])
         cd = (ctypes.c_int * (self.L + 1))(*dims)
@@ -500,7 +525,7 @@ class Server:
         req.cfg, req.W, req.Dl, req.Dr = cfg, wp, Dl, Dr
         keep = [Ws]
         if mps is not None:
-            As = [_prep(a, code) for a in mps]
+            As = minimal_bonds([_prep(a, code) for a in mps])
             keep.append(As)
             req.A = (ctypes.c_void_p * L)(*[a.ctypes.data for a in As])
             req.bond_dims = (ctypes.c_int * (L + 1))(*([1] + [a.shape[2] for a in As]))

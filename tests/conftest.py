@@ -2,7 +2,12 @@ import os
 import sys
 from pathlib import Path
 
-import pytest
+# The oracle's contractions are small; a multi-threaded BLAS on them spends its time
+# synchronising threads (50x slower on complex d=5 chains). Set before numpy loads.
+for _var in ("OPENBLAS_NUM_THREADS", "OMP_NUM_THREADS", "MKL_NUM_THREADS"):
+    os.environ.setdefault(_var, "1")
+
+import pytest  # noqa: E402
 
 REPO = Path(__file__).resolve().parent.parent
 sys.path.insert(0, str(REPO))

@@ -199,7 +199,7 @@ def test_reference_bin_data_josephson_vs_oracle(golden_dir):
     from dmrg2 import io
     W = io.load_mpo_bin(golden_dir / "josephson_L12_n2_mpo.bin")
     A = io.load_mps_bin(golden_dir / "josephson_L12_n2_chi10_mps.bin")
-    sched = [24] * 4
+    sched = [16] * 2
     eng, rep = gpu_run(W, A, sched, krylov_max=30, max_restarts=4, cutoff=1e-14)
     ref = O.dmrg2(W, A, sched, cutoff=1e-14)
     assert abs(rep[-1]["energy"] - ref["energy"]) <= 1e-10 * abs(ref["energy"])

@@ -69,3 +69,17 @@ def test_npz_fixtures_and_orders(tmp_path, golden_dir):
     io.save_mps_npz(tmp_path / "c.npz", A, energy=-5.14)
     for a, b in zip(A, io.load_mps_npz(tmp_path / "c.npz")):
         np.testing.assert_array_equal(a, b)
+
+
+def test_minimal_bonds_keeps_the_state(golden_dir):
+    """quimb-style MPS with one bond dimension everywhere (the reference's .bin state:
+    bond 1 of 10 at d=5) reduces exactly to the minimal bonds the engine allocates."""
+    import dmrg2
+    A = io.load_mps_bin(golden_dir / "josephson_L12_n2_chi10_mps.bin")
+    assert A[0].shape[2] == 10 and A[0].shape[1] == 5
+    B = dmrg2.minimal_bonds(A)
+    assert B[0].shape[2] == 5 and B[-1].shape[0] == 5
+    W = io.load_mpo_bin(golden_dir / "josephson_L12_n2_mpo.bin")
+    e1 = O.mpo_expectation(A, W) / O.mps_norm2(A)
+    e2 = O.mpo_expectation(B, W) / O.mps_norm2(B)
+    assert abs(e1 - e2) <= 1e-12 * abs(e1)
