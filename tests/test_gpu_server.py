@@ -97,9 +97,8 @@ def test_admission_respects_the_budget(alone):
 def test_failed_request_leaves_the_others_intact(alone):
     reqs, ref = alone
     bad = dict(reqs[0])
-    mps = [a.copy() for a in bad["mps"]]
-    mps[1] = np.zeros((2, 2, 7))  # bond 2 of 7 exceeds min(chi_max, 2^2): set_mps fails on the worker
-    mps[2] = np.zeros((7, 2, mps[2].shape[2]))
+    # middle bonds of 50 exceed chi_max = 32 (and cannot be reduced exactly): set_mps fails on the worker
+    mps = O.random_mps(len(bad["mpo"]), 2, 50, seed=9)
     with dmrg2.Server(max_active=2) as srv:
         i_bad = srv.submit(bad["mpo"], bad["schedule"], mps=mps, tol=1e-300, min_sweeps=100)
         i_ok = srv.submit(reqs[1]["mpo"], reqs[1]["schedule"], mps=reqs[1]["mps"], tol=1e-300, min_sweeps=100)
