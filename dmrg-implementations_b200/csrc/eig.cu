@@ -238,55 +238,63 @@ __global__ void __launch_bounds__(HT_THREADS)
 // ----------------------------------------------------------------------------
 // 1b. Real symmetric G of order n <= 512: the same reduction with the trailing
 //     matrix held in registers. Row r belongs to CTA r % C (local row q = r / C)
-//     and, inside it, to warp q % 16 (slot q / 16 < RW); lane l holds columns
-//     j = l + 32 t, t < NT. Column k's step is one fused pass per warp: with p
+//     and, inside it, to warp q % 16 (slot q / 16 < RW); lane l holds the
+//     column pairs j = 2l + 64u + {0, 1} (NT columns), so the fused pass reads
+//     its vectors with 16-byte shared loads. Column k's step is one fused pass
+//     per warp: with p
 //     and column k+1 pulled from the owners, each warp forms v, w and the next
 //     column x' = column k+1 - (v w^T + w v^T)[:, k+1] for its lane's columns,
 //     applies the rank-2 update to its rows and, in the same pass, accumulates
 //     the next step's symv sum_j G'[r][j] x'[j] (the reflector of x' only
 //     scales it, and every warp derives that reflector itself from x'). Per
 //     column: one CTA barrier after the pull and one cluster barrier after the
-//     owners publish p', column k+2 and the partial sums of s' = p'^T v'.
+//     owners publish p', column k+2 and the partial sums of s' = p'^T v'. The
+//     reflector scalars cost one division.
 // ----------------------------------------------------------------------------
-__device__ inline void house_real(double alpha, double xn2, double& tk, double& sc, double& beta) {
+__device__ inline void house_real1(double alpha, double xn2, double& tk, double& sc, double& beta) {
   if (xn2 == 0.0) {
     tk = 0.0;
     sc = 0.0;
     beta = alpha;
-  } else {
-    beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
-    const double ib = 1.0 / beta;
-    tk = (beta - alpha) * ib;
-    const double dr = alpha - beta;
-    sc = dr * (1.0 / (dr * dr));  // 1 / (alpha - beta)
+    return;
   }
+  beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+  const double dr = alpha - beta;  // |dr| >= sqrt(xn2) > 0
+  const double r = 1.0 / (beta * dr);
+  tk = -dr * dr * r;  // (beta - alpha) / beta
+  sc = beta * r;      // 1 / (alpha - beta)
 }
 
 template <int NT, int RW, int C>
 __global__ void __launch_bounds__(HT_THREADS, 1)
-    hetrd_reg_kernel(double* __restrict__ G, int n, ll ld, double* __restrict__ dg,
-                     double* __restrict__ eg, double* __restrict__ tau) {
+    hetrd_reg2_kernel(double* __restrict__ G, int n, ll ld, double* __restrict__ dg,
+                      double* __restrict__ eg, double* __restrict__ tau) {
   static_assert((C & (C - 1)) == 0 && C <= 32, "cluster size: power of two <= 32");
+  static_assert(NT % 2 == 0, "column slots come in pairs");
   cg::cluster_group cluster = cg::this_cluster();
   constexpr int lgC = (C >= 32) ? 5 : (C >= 16) ? 4 : (C >= 8) ? 3 : (C >= 4) ? 2 : (C >= 2) ? 1 : 0;
-  const int rank = (int)cluster.block_rank();
   constexpr int NW = HT_THREADS / 32;
+  constexpr int NP = NT / 2;  // column pairs per lane
+  const int rank = (int)cluster.block_rank();
   extern __shared__ __align__(16) double hsm[];
-  // pulled p and column k+1 are kept owner-major, padded: row r at pidx(r)
   const int Q = (n + C - 1) >> lgC;  // rows per CTA
-  auto pidx = [&](int r) { return (r & (C - 1)) * (Q + 1) + (r >> lgC); };
-  double* pf = hsm;                   // p of this step, all rows (pulled)
-  double* cf = pf + C * (Q + 1);      // column k+1 before this step, all rows (pulled)
-  double* xs0 = cf + C * (Q + 1);     // column k (parity buffers)
-  double* xs1 = xs0 + n;
-  double* po0 = xs1 + n;  // own p entries by local row r / C (parity buffers)
-  double* po1 = po0 + n;
-  double* co0 = po1 + n;  // own column entries (parity buffers)
-  double* co1 = co0 + n;
-  double* sp0 = co1 + n;  // per-warp partial s (parity buffers, NW each)
+  const int n2 = (n + 1) & ~1;       // even array strides keep every array 16-byte aligned
+  const int Q2 = (Q + 1) & ~1;
+  double* pf = hsm;        // p of this step, natural order (pulled)
+  double* cf = pf + n2;    // column k+1 before this step (pulled)
+  double* xs0 = cf + n2;   // column k (parity buffers)
+  double* xs1 = xs0 + n2;
+  double* po0 = xs1 + n2;  // own p entries by local row (parity buffers)
+  double* po1 = po0 + Q2;
+  double* co0 = po1 + Q2;  // own column entries (parity buffers)
+  double* co1 = co0 + Q2;
+  double* sp0 = co1 + Q2;  // per-warp partial s (parity buffers)
   double* sp1 = sp0 + NW;
   double* sall = sp1 + NW;  // all C * NW partials of s, pulled
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  auto col = [&](int t) { return 2 * lane + 64 * (t >> 1) + (t & 1); };
+  // 16-byte stores into row k of G only when every row start is 16-byte aligned
+  const bool g_pairs = ((ld & 1) == 0) && ((reinterpret_cast<uintptr_t>(G) & 15) == 0);
 
   int rr[RW];
   double g[RW][NT];
@@ -295,7 +303,7 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
     rr[i] = (warp + NW * i) * C + rank;
 #pragma unroll
     for (int t = 0; t < NT; ++t) {
-      const int j = lane + 32 * t;
+      const int j = col(t);
       g[i][t] = (rr[i] < n && j < n) ? G[(ll)rr[i] * ld + j] : 0.0;
     }
   }
@@ -307,7 +315,7 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
     double xn2 = 0.0;
     for (int j = 2 + lane; j < n; j += 32) xn2 += xs0[j] * xs0[j];
     xn2 = warp_sum_d(xn2);
-    house_real(xs0[1], xn2, tk, sc, beta);
+    house_real1(xs0[1], xn2, tk, sc, beta);
     if (rank == 0 && tid == 0) {
       dg[0] = xs0[0];
       eg[0] = beta;
@@ -320,11 +328,11 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
       double acc = 0.0;
 #pragma unroll
       for (int t = 0; t < NT; ++t) {
-        const int j = lane + 32 * t;
+        const int j = col(t);
         if (j >= 2 && j < n) acc += g[i][t] * xs0[j];
       }
       acc = warp_sum_d(acc);
-      const double c1 = __shfl_sync(0xffffffffu, g[i][0], 1);
+      const double c1 = __shfl_sync(0xffffffffu, g[i][1], 0);  // column 1 sits in lane 0, slot 1
       if (r >= 1 && r < n) {
         const double p = tk * (c1 + sc * acc);
         if (lane == 0) {
@@ -348,14 +356,14 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
     double* con = par ? co0 : co1;
     double* spn = par ? sp0 : sp1;
     double* xsn = par ? xs0 : xs1;
-    // (1) pull p and column k+1 from the row owners and every partial of s (one remote
-    //     load per thread and array, all in flight together)
-    {  // thread -> (owner c, local row q): a warp reads consecutive entries of one owner
+    // (1) pull p and column k+1 (a warp reads consecutive entries of one owner) and
+    //     every partial of s
+    {
       const int c = tid / Q, q = tid - c * Q;
       const int r = (q << lgC) + c;
       if (c < C && r >= k + 1 && r < n) {
-        pf[c * (Q + 1) + q] = cluster.map_shared_rank(po, c)[q];
-        cf[c * (Q + 1) + q] = cluster.map_shared_rank(co, c)[q];
+        pf[r] = cluster.map_shared_rank(po, c)[q];
+        cf[r] = cluster.map_shared_rank(co, c)[q];
       }
     }
     if (tid < C * NW) sall[tid] = cluster.map_shared_rank(spr, tid / NW)[tid % NW];
@@ -365,7 +373,7 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
     ssum = warp_sum_d(ssum);
     // (2) w = p - tau s / 2 v; fused rank-2 update + next symv + next column
     const double a2 = -0.5 * tk * ssum;
-    const double wk1 = pf[pidx(k + 1)] + a2;  // v[k+1] = 1
+    const double wk1 = pf[k + 1] + a2;  // v[k+1] = 1
     double vr[RW], wr[RW], acc[RW], c2[RW];
     bool act[RW];
 #pragma unroll
@@ -376,31 +384,20 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
       act[i] = (r >= k + 1 && r < n);
       if (act[i]) {
         vr[i] = (r == k + 1) ? 1.0 : xs[r] * sc;
-        wr[i] = pf[pidx(r)] + a2 * vr[i];
+        wr[i] = pf[r] + a2 * vr[i];
       }
       acc[i] = 0.0;
       c2[i] = 0.0;
     }
     double nrm = 0.0, a_next = 0.0, d_next = 0.0;
     const bool store_v = (rank == 0);
-    // column chunks t < tb lie left of the active block; chunks tb and tb + 1 hold
-    // columns k+1 and k+2 and take the checked path, as does a ragged last chunk
-    const int tb = (k + 1) >> 5;
-    const int pl = (lane & (C - 1)) * (Q + 1) + (lane >> lgC);  // pidx(lane); + t * 32 / C per chunk
-    auto chunk = [&](const int t, const bool edge) {
-      const int j = lane + 32 * t;
-      if (edge && !(j >= k + 1 && j < n)) return;
-      const int pj = pl + t * (32 / C);
-      const double vj = (edge && j == k + 1) ? 1.0 : xs[j] * sc;
-      const double wj = pf[pj] + a2 * vj;
-      const double xn = cf[pj] - vj * wk1 - wj;
+    auto one = [&](const int t, const int j, const double xv, const double pv, const double cv, const bool edge) {
+      const double vj = (edge && j == k + 1) ? 1.0 : xv * sc;
+      const double wj = pv + a2 * vj;
+      const double xn = cv - vj * wk1 - wj;
       if (!edge || j >= k + 3) nrm += xn * xn;
       if (edge && j == k + 2) a_next = xn;
       if (edge && j == k + 1) d_next = xn;
-      if (t % NW == warp) {  // one warp per column chunk publishes x' and the reflector
-        xsn[j] = xn;
-        if (store_v) G[(ll)k * ld + j] = vj;
-      }
 #pragma unroll
       for (int i = 0; i < RW; ++i) {
         if (act[i]) {
@@ -410,19 +407,55 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
           if (edge && j == k + 2) c2[i] = gg;
         }
       }
+      return xn;
     };
 #pragma unroll
-    for (int t = 0; t < NT; ++t) {
-      if (t < tb || 32 * t >= n) continue;
-      if (t <= tb + 1 || 32 * t + 32 > n) chunk(t, true);
-      else chunk(t, false);
+    for (int u = 0; u < NP; ++u) {
+      const int base = 64 * u;
+      if (base + 64 <= k + 1 || base >= n) continue;  // chunk left of the active block or past n
+      const int j0 = base + 2 * lane;
+      const bool mine = (u % NW) == warp;  // this warp publishes x' and the reflector of chunk u
+      if (base >= k + 3 && base + 64 <= n) {
+        const double2 xv = *reinterpret_cast<const double2*>(xs + j0);
+        const double2 pv = *reinterpret_cast<const double2*>(pf + j0);
+        const double2 cv = *reinterpret_cast<const double2*>(cf + j0);
+        double2 xo;
+        xo.x = one(2 * u, j0, xv.x, pv.x, cv.x, false);
+        xo.y = one(2 * u + 1, j0 + 1, xv.y, pv.y, cv.y, false);
+        if (mine) {
+          *reinterpret_cast<double2*>(xsn + j0) = xo;
+          if (store_v) {
+            if (g_pairs) {
+              double2 vv;
+              vv.x = xv.x * sc;
+              vv.y = xv.y * sc;
+              *reinterpret_cast<double2*>(G + (ll)k * ld + j0) = vv;
+            } else {
+              G[(ll)k * ld + j0] = xv.x * sc;
+              G[(ll)k * ld + j0 + 1] = xv.y * sc;
+            }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int j = j0 + h;
+          if (j >= k + 1 && j < n) {
+            const double xn = one(2 * u + h, j, xs[j], pf[j], cf[j], true);
+            if (mine) {
+              xsn[j] = xn;
+              if (store_v) G[(ll)k * ld + j] = (j == k + 1) ? 1.0 : xs[j] * sc;
+            }
+          }
+        }
+      }
     }
     // (3) next reflector (every warp derives the same one), publish p', column k+2, s'
     nrm = warp_sum_d(nrm);
-    a_next = __shfl_sync(0xffffffffu, a_next, (k + 2) & 31);
-    d_next = __shfl_sync(0xffffffffu, d_next, (k + 1) & 31);
+    a_next = __shfl_sync(0xffffffffu, a_next, ((k + 2) & 63) >> 1);
+    d_next = __shfl_sync(0xffffffffu, d_next, ((k + 1) & 63) >> 1);
     double tk2 = 0.0, sc2 = 0.0, beta2 = 0.0;
-    if (k + 2 <= n - 1) house_real(a_next, nrm, tk2, sc2, beta2);
+    if (k + 2 <= n - 1) house_real1(a_next, nrm, tk2, sc2, beta2);
     if (rank == 0 && tid == 32) {
       dg[k + 1] = d_next;
       eg[k + 1] = beta2;
@@ -433,14 +466,14 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
     for (int i = 0; i < RW; ++i) {
       const int r = rr[i];
       const double a = warp_sum_d(acc[i]);
-      const double c = __shfl_sync(0xffffffffu, c2[i], (k + 2) & 31);
+      const double c = __shfl_sync(0xffffffffu, c2[i], ((k + 2) & 63) >> 1);
       if (r >= k + 2 && r < n) {
         const double p = tk2 * (c + sc2 * a);
         if (lane == 0) {
           pon[r >> lgC] = p;
           con[r >> lgC] = c;
         }
-        const double xnr = cf[pidx(r)] - vr[i] * wk1 - wr[i];
+        const double xnr = cf[r] - vr[i] * wk1 - wr[i];
         sp += p * ((r == k + 2) ? 1.0 : xnr * sc2);
       }
     }
@@ -452,17 +485,16 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
 }
 
 template <int NT, int RW, int C>
-static cudaError_t hetrd_reg_launch(double* G, int n, ll ld, double* d, double* e, double* tau,
-                                    cudaStream_t s) {
+static cudaError_t hetrd_reg2_launch(double* G, int n, ll ld, double* d, double* e, double* tau,
+                                     cudaStream_t s) {
   static std::atomic<unsigned long long> attr_cluster{0};
-  func_attr_once(attr_cluster, (const void*)hetrd_reg_kernel<NT, RW, C>,
+  func_attr_once(attr_cluster, (const void*)hetrd_reg2_kernel<NT, RW, C>,
                  cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(C);
   cfg.blockDim = dim3(HT_THREADS);
-  const int Q = (n + C - 1) / C;
-  cfg.dynamicSmemBytes = sizeof(double) * ((size_t)2 * C * (Q + 1) + 6 * (size_t)n + 2 * (HT_THREADS / 32) +
-                                           16 * (HT_THREADS / 32));
+  const size_t n2 = (size_t)((n + 1) & ~1), Q2 = (size_t)((((n + C - 1) / C) + 1) & ~1);
+  cfg.dynamicSmemBytes = sizeof(double) * (4 * n2 + 4 * Q2 + 2 * (HT_THREADS / 32) + 16 * (HT_THREADS / 32));
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -471,7 +503,7 @@ static cudaError_t hetrd_reg_launch(double* G, int n, ll ld, double* d, double* 
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, hetrd_reg_kernel<NT, RW, C>, G, n, ld, d, e, tau);
+  return cudaLaunchKernelEx(&cfg, hetrd_reg2_kernel<NT, RW, C>, G, n, ld, d, e, tau);
 }
 
 // register-resident reduction for real G with 32 <= n <= 512; false when the device
@@ -480,9 +512,9 @@ static bool hetrd_reg(double* G, int n, ll ld, double* d, double* e, double* tau
   static std::atomic<int> refused{0};
   if (n < 32 || n > 512 || refused.load()) return false;
   cudaError_t err;
-  if (n <= 128) err = hetrd_reg_launch<4, 1, 8>(G, n, ld, d, e, tau, s);
-  else if (n <= 256) err = hetrd_reg_launch<8, 1, 16>(G, n, ld, d, e, tau, s);
-  else err = hetrd_reg_launch<16, 2, 16>(G, n, ld, d, e, tau, s);
+  if (n <= 128) err = hetrd_reg2_launch<4, 1, 8>(G, n, ld, d, e, tau, s);
+  else if (n <= 256) err = hetrd_reg2_launch<8, 1, 16>(G, n, ld, d, e, tau, s);
+  else err = hetrd_reg2_launch<16, 2, 16>(G, n, ld, d, e, tau, s);
   if (err == cudaSuccess) return true;
   if (err == cudaErrorInvalidClusterSize || err == cudaErrorLaunchOutOfResources || err == cudaErrorInvalidValue) {
     (void)cudaGetLastError();
