@@ -45,6 +45,10 @@ CUTOFF = 1e-12
 KRYLOV = 30
 RESTARTS = 2
 METRIC = "sweeps/s (two-site DMRG, Heisenberg L=100, chi=256, FP64 plain form)"
+# DRAM bytes of one H_eff application at chi = 256 (dram__bytes_read.sum + dram__bytes_write.sum
+# over its four kernels: step-1 GEMM, MPO mixing, split-K step-3 GEMM, split-K reduce), from one
+# ncu capture of `python -m dmrg2.microbench heff --chi 256`; the algorithmic bytes are 9.4 MB
+HEFF_TRAFFIC_BYTES_CHI256 = 38.9e6
 
 
 def workload_config(n_gpus, extra=None):
@@ -220,6 +224,22 @@ def measure_dgemm_peak():
     return 2.0 * n ** 3 / best / 1e12
 
 
+def replica_reduce(values, world, device):
+    """Max over ranks of per-rank timings (seconds); the identity on one rank. Every rank
+    calls it (the same collective, in the same order)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
+def replica_throughput(units_per_rank, world, t_max):
+    """Whole-job throughput of `world` independent replicas, timed by the slowest one."""
+    return world * units_per_rank / t_max
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -302,16 +322,13 @@ def run_ours(args):
     mv = sum(r["matvecs"] for r in timed)
     n_sw = len(timed)
 
-    t = torch.tensor([dev, t_e2e], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    dev_max, e2e_max = float(t[0]), float(t[1])
+    dev_max, e2e_max = replica_reduce([dev, t_e2e], world, "cuda")
     peak = measure_dgemm_peak()
     if rank != 0:
         if world > 1:
             dist.destroy_process_group()
         return
-    value = world * n_sw / dev_max
+    value = replica_throughput(n_sw, world, dev_max)
     achieved = heff_fl / heff_s / 1e12 if heff_s > 0 else 0.0
     set_cpu_threads()
     mv_per_bond = mv / max(1, n_sw * 2 * (L_SITES - 1))
@@ -326,14 +343,16 @@ def run_ours(args):
         "config": workload_config(world),
         "energy": energy,
         "max_bond": max(dims),
-        "e2e": {"value": world * len(e2e_reports) / e2e_max, "unit": "sweeps/s",
+        "e2e": {"value": replica_throughput(len(e2e_reports), world, e2e_max), "unit": "sweeps/s",
                 "h2d_bytes_per_step": h2d // len(e2e_reports), "d2h_bytes_per_step": d2h // len(e2e_reports),
                 "energy": e2e_energy, "phases_s": e2e_phases,
                 "what": f"{len(e2e_reports)} sweeps at chi={CHI} through dmrg2_create/set_mpo/set_mps/run/get_mps "
                         f"from the host MPS left by the warm-up, host wall clock incl. H2D, environment build, D2H"},
         "roofline": {"kernel": "H_eff contraction (FP64 DMMA GEMMs)", "bound": "tensor",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak if peak else None, "traffic": None,
+                     "frac": achieved / peak if peak else None, "traffic": HEFF_TRAFFIC_BYTES_CHI256,
+                     "traffic_note": "DRAM bytes per H_eff application at chi=256 from an ncu capture of the "
+                                     "same kernels; algorithmic bytes 9.4e6 (L, R, theta in and out)",
                      "peak_source": "cuBLAS DGEMM 8192^3 (torch.matmul float64) measured in this run; "
                                     "MEASURED_PEAKS.json has no FP64 figure"},
         "time_share": {"heff": heff_s / dev, "svd": svd_s / dev, "other": max(0.0, 1 - (heff_s + svd_s) / dev)},
