@@ -94,7 +94,7 @@ def cpu_sample(chis, mv_per_bond, budget_s=20.0, seed=0, profiles=None, min_s=0.
     cache = {}
     t_start = time.perf_counter()
 
-    def timed(f, max_reps=64):
+    def timed(f, max_reps=16):
         f()
         n, t0 = 0, time.perf_counter()
         while n < max_reps and (n == 0 or time.perf_counter() - t0 < min_s):

@@ -11,21 +11,22 @@
 // Pipeline (textbook methods, written for sm_100a):
 //   1. hetrd_cluster: Householder reduction G = Q T Q^H to real symmetric
 //      tridiagonal form (Golub & Van Loan, Alg. 8.3.1) by ONE thread-block
-//      cluster of up to 16 CTAs. Rows are distributed cyclically over the
-//      CTAs; the two reductions per column (the scalar p^H v and the all-gather
-//      of w) go through distributed shared memory with two cluster barriers per
-//      column. Every CTA recomputes the next column from the pre-update row
-//      plus the rank-2 correction, so no third barrier is needed.
+//      cluster of up to 16 CTAs, rows distributed cyclically over the CTAs.
+//      Real G up to order 512 keeps the trailing matrix in registers and does
+//      each column in one fused pass (1b below); complex or larger G keeps it
+//      in shared memory (or L2). Either way the all-gather of p goes through
+//      distributed shared memory with one cluster barrier per column.
 //   2. tridiag_bisect: the K largest eigenvalues of T by Sturm-count
-//      multisection, one warp per eigenvalue.
+//      multisection, one CTA per eigenvalue, 129 points per round.
 //   3. tridiag_invit: eigenvectors of T by inverse iteration with partial
-//      pivoting, one thread per eigenvector, seeded random starts.
+//      pivoting, one thread per eigenvector, seeded random starts, factors and
+//      iterate in shared memory.
 //   4. group_mgs: classical Gram-Schmidt with re-orthogonalisation inside
 //      groups of (numerically) degenerate eigenvalues (SU(2) multiplets, the
 //      tail near the noise floor), then a Newton-Schulz polar step on the whole
 //      block (GEMMs) restores orthogonality to ~eps.
-//   5. apply_q: eigenvectors of G = Q z, each CTA applying all reflectors to
-//      its own slab of columns (columns are independent).
+//   5. apply_q: eigenvectors of G = Q z, each CTA applying all reflectors in
+//      compact-WY blocks to its own slab of columns (columns are independent).
 #include <cooperative_groups.h>
 
 #include "kernels.cuh"
@@ -613,8 +614,8 @@ __global__ void __launch_bounds__(256)
 
 // ----------------------------------------------------------------------------
 // 3. inverse iteration for the k kept eigenvalues: one thread per eigenvector,
-//    LU factors with partial pivoting in scratch [i][K], the recurrences carried
-//    in registers. Columns k..K-1 of Z are zeroed.
+//    LU factors with partial pivoting and the iterate in shared memory, the
+//    recurrences carried in registers. Columns k..K-1 of Z are zeroed.
 // ----------------------------------------------------------------------------
 __device__ inline double hash_unit(unsigned long long x) {
   x += 0x9E3779B97F4A7C15ull;
@@ -628,13 +629,20 @@ __global__ void tridiag_invit_kernel(const double* __restrict__ dg, const double
                                      int n, int K, const double* __restrict__ lam,
                                      const SvdOut* __restrict__ tr, double* __restrict__ Z) {
   extern __shared__ double dsh[];
+  __shared__ double tn_s;
   const int vpb = blockDim.x;  // one vector per thread
   double* d = dsh;
   double* e = dsh + n;
-  double* base = dsh + 2 * n;  // [5][n][vpb]
+  double* base = dsh + 2 * n;  // [6][n][vpb]: factors, then the iterate
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     d[i] = dg[i];
     e[i] = (i < n - 1) ? eg[i] : 0.0;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {  // |T|_inf once per CTA
+    double tn = 0.0;
+    for (int i = 0; i < n; ++i) tn = fmax(tn, fabs(d[i]) + fabs(i > 0 ? e[i - 1] : 0.0) + fabs(e[i]));
+    tn_s = tn;
   }
   __syncthreads();
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -645,11 +653,8 @@ __global__ void tridiag_invit_kernel(const double* __restrict__ dg, const double
   }
   const int t = threadIdx.x;
 #define SX(a, i) base[((ll)(a) * n + (i)) * vpb + t]
-  // arrays: 0 = 1/u0, 1 = u1, 2 = u2, 3 = multiplier, 4 = swap flag
-  double tn = 0.0;
-  for (int i = 0; i < n; ++i)
-    tn = fmax(tn, fabs(d[i]) + fabs(i > 0 ? e[i - 1] : 0.0) + fabs(e[i]));
-  const double tiny = fmax(tn, 1e-300) * 2.2e-16;
+  // arrays: 0 = 1/u0, 1 = u1, 2 = u2, 3 = multiplier, 4 = swap flag, 5 = iterate
+  const double tiny = fmax(tn_s, 1e-300) * 2.2e-16;
   const double sft = lam[j];
   double c0 = d[0] - sft, c1 = e[0];
   for (int i = 0; i < n - 1; ++i) {
@@ -683,8 +688,8 @@ __global__ void tridiag_invit_kernel(const double* __restrict__ dg, const double
   SX(0, n - 1) = 1.0 / c0;
   SX(1, n - 1) = 0.0;
   SX(2, n - 1) = 0.0;
-  // the iterate lives in global memory (column j of Z, coalesced across threads)
-#define IZ(i) Z[(ll)(i) * K + j]
+  // the iterate lives in shared memory next to the factors; column j of Z is written at the end
+#define IZ(i) SX(5, i)
   for (int i = 0; i < n; ++i) IZ(i) = hash_unit(((unsigned long long)(j + 1) << 32) ^ (unsigned long long)i);
   for (int it = 0; it < 2; ++it) {
     double y = IZ(0);
@@ -711,6 +716,7 @@ __global__ void tridiag_invit_kernel(const double* __restrict__ dg, const double
     const double inv = 1.0 / nrm;
     for (int i = 0; i < n; ++i) IZ(i) *= inv;
   }
+  for (int i = 0; i < n; ++i) Z[(ll)i * K + j] = IZ(i);
 #undef IZ
 #undef SX
 }
@@ -1051,7 +1057,8 @@ void hetrd_cluster(T* G, int n, ll ld, double* d, double* e, T* tau, cudaStream_
 }
 
 void tridiag_eigvals(const double* d, const double* e, int n, int K, double* lam, cudaStream_t s) {
-  tridiag_bisect_kernel<<<K, 256, sizeof(double) * 2 * n, s>>>(d, e, n, K, lam);
+  // 129 points per round (7 bits): about 8 rounds to full precision, half the Sturm counts of 257
+  tridiag_bisect_kernel<<<K, 128, sizeof(double) * 2 * n, s>>>(d, e, n, K, lam);
   DMRG2_CHECK_LAUNCH();
 }
 
@@ -1060,7 +1067,7 @@ void tridiag_eigvecs(const double* d, const double* e, int n, int K, const doubl
   (void)scratch;
   static std::atomic<unsigned long long> attr{0};
   set_smem_attr_once(attr, (const void*)tridiag_invit_kernel, 220 * 1024);
-  const size_t per = sizeof(double) * 5 * (size_t)n;
+  const size_t per = sizeof(double) * 6 * (size_t)n;
   int vpb = (int)std::min<size_t>(8, (220 * 1024 - sizeof(double) * 2 * (size_t)n) / per);
   if (vpb < 1) throw std::runtime_error("inverse iteration: matrix order too large");
   const size_t smem = sizeof(double) * 2 * (size_t)n + per * vpb;

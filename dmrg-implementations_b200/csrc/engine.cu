@@ -53,7 +53,21 @@ class Engine final : public EngineBase {
     for (int i = 0; i <= L_; ++i) cap_[i] = (int)ipow_cap(d_, std::min(i, L_ - i), cfg_.chi_max);
     dims_.assign(L_ + 1, 1);
     mps_.assign(L_, nullptr);
-    for (int i = 0; i < L_; ++i) mps_[i] = dalloc((ll)cap_[i] * d_ * cap_[i + 1]);
+    {  // every MPS slot in one allocation, 256-byte aligned slices
+      std::vector<size_t> off(L_);
+      size_t tot = 0;
+      for (int i = 0; i < L_; ++i) {
+        off[i] = tot;
+        tot += round256(sizeof(T) * (size_t)std::max<ll>((ll)cap_[i] * d_ * cap_[i + 1], 1));
+      }
+      void* p = nullptr;
+      DMRG2_CUDA(cudaMalloc(&p, tot));
+      allocs_.push_back(p);
+      for (int i = 0; i < L_; ++i) {
+        mps_[i] = (T*)((char*)p + off[i]);
+        bytes_ += sizeof(T) * (size_t)std::max<ll>((ll)cap_[i] * d_ * cap_[i + 1], 1);
+      }
+    }
     nmax_ = 1;
     for (int i = 0; i + 1 < L_; ++i) nmax_ = std::max(nmax_, (ll)cap_[i] * d_ * d_ * cap_[i + 2]);
     qmax_ = 1;
@@ -136,27 +150,13 @@ class Engine final : public EngineBase {
       hW_[i].resize(n);
       std::memcpy(hW_[i].data(), W[i], n * sizeof(T));
     }
-    wml_.assign(L_, nullptr);
-    wmr_.assign(L_, nullptr);
-    wwt_.assign(L_ - 1, nullptr);
-    std::vector<T> tmp;
+    // host images of the mixing matrices and fused two-site MPOs
+    std::vector<std::vector<T>> hml(L_), hmr(L_), hww(L_ - 1);
     for (int i = 0; i < L_; ++i) {
-      build_wmix_left(hW_[i].data(), Dl[i], Dr[i], d_, tmp);
-      wml_[i] = upload(tmp);
-      build_wmix_right(hW_[i].data(), Dl[i], Dr[i], d_, tmp);
-      wmr_[i] = upload(tmp);
+      build_wmix_left(hW_[i].data(), Dl[i], Dr[i], d_, hml[i]);
+      build_wmix_right(hW_[i].data(), Dl[i], Dr[i], d_, hmr[i]);
     }
-    for (int i = 0; i + 1 < L_; ++i) {
-      build_wwt(hW_[i].data(), hW_[i + 1].data(), Dl[i], Dr[i], Dr[i + 1], d_, tmp);
-      wwt_[i] = upload(tmp);
-    }
-    lenv_.assign(L_ + 1, nullptr);
-    renv_.assign(L_ + 1, nullptr);
-    for (int i = 0; i <= L_; ++i) {
-      ll n = (ll)cap_[i] * cap_[i] * Db_[i];
-      lenv_[i] = dalloc_mpo(n);
-      renv_[i] = dalloc_mpo(n);
-    }
+    for (int i = 0; i + 1 < L_; ++i) build_wwt(hW_[i].data(), hW_[i + 1].data(), Dl[i], Dr[i], Dr[i + 1], d_, hww[i]);
     // contraction scratch
     ll xs = 1;
     const ll dd = (ll)d_ * d_;
@@ -172,8 +172,46 @@ class Engine final : public EngineBase {
       xs = std::max(xs, b * Dr[i] * d_ * a);
       xs = std::max(xs, (ll)d_ * b * Dl[i] * a);
     }
-    X_ = dalloc_mpo(xs);
-    Y_ = dalloc_mpo(xs);
+    // one device allocation for every MPO-dependent buffer, carved in 256-byte aligned
+    // slices; the uploaded matrices form its prefix and cross to the device in one copy
+    auto el = [](ll n) { return sizeof(T) * (size_t)std::max<ll>(n, 1); };
+    size_t up = 0;
+    for (auto& h : hml) up += round256(el((ll)h.size()));
+    for (auto& h : hmr) up += round256(el((ll)h.size()));
+    for (auto& h : hww) up += round256(el((ll)h.size()));
+    size_t total = up + 2 * round256(el(xs));
+    for (int i = 0; i <= L_; ++i) total += 2 * round256(el((ll)cap_[i] * cap_[i] * Db_[i]));
+    DMRG2_CUDA(cudaMalloc(&mpo_slab_, total));
+    std::vector<char> stage(up);
+    size_t off = 0;
+    auto carve = [&](ll n) {
+      T* p = (T*)((char*)mpo_slab_ + off);
+      off += round256(el(n));
+      bytes_mpo_ += el(n);
+      return p;
+    };
+    auto put = [&](const std::vector<T>& h) {
+      if (!h.empty()) std::memcpy(stage.data() + off, h.data(), sizeof(T) * h.size());
+      return carve((ll)h.size());
+    };
+    wml_.assign(L_, nullptr);
+    wmr_.assign(L_, nullptr);
+    wwt_.assign(L_ - 1, nullptr);
+    for (int i = 0; i < L_; ++i) {
+      wml_[i] = put(hml[i]);
+      wmr_[i] = put(hmr[i]);
+    }
+    for (int i = 0; i + 1 < L_; ++i) wwt_[i] = put(hww[i]);
+    DMRG2_CUDA(cudaMemcpy(mpo_slab_, stage.data(), up, cudaMemcpyHostToDevice));
+    lenv_.assign(L_ + 1, nullptr);
+    renv_.assign(L_ + 1, nullptr);
+    for (int i = 0; i <= L_; ++i) {
+      ll n = (ll)cap_[i] * cap_[i] * Db_[i];
+      lenv_[i] = carve(n);
+      renv_[i] = carve(n);
+    }
+    X_ = carve(xs);
+    Y_ = carve(xs);
     mpo_set_ = true;
     envs_valid_ = false;
   }
@@ -311,14 +349,7 @@ class Engine final : public EngineBase {
     bytes_ += b;
     return p;
   }
-  T* dalloc_mpo(ll n) {
-    void* p = nullptr;
-    size_t b = sizeof(T) * (size_t)std::max<ll>(n, 1);
-    DMRG2_CUDA(cudaMalloc(&p, b));
-    mpo_allocs_.push_back(p);
-    bytes_mpo_ += b;
-    return (T*)p;
-  }
+  static size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
   T* dalloc_tmp(ll n) { return (T*)dalloc_tmp_bytes(sizeof(T) * (size_t)std::max<ll>(n, 1)); }
   void* dalloc_tmp_bytes(size_t b) {
     void* p = nullptr;
@@ -331,14 +362,9 @@ class Engine final : public EngineBase {
     tmp_allocs_.clear();
   }
   void free_mpo() {
-    for (void* p : mpo_allocs_) cudaFree(p);
-    mpo_allocs_.clear();
+    if (mpo_slab_) cudaFree(mpo_slab_);
+    mpo_slab_ = nullptr;
     bytes_mpo_ = 0;
-  }
-  T* upload(const std::vector<T>& h) {
-    T* p = dalloc_mpo((ll)h.size());
-    DMRG2_CUDA(cudaMemcpy(p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
-    return p;
   }
 
   // rotation threshold on |<x_p,x_q>| / (|x_p||x_q|): len * eps, as LAPACK's
@@ -619,7 +645,8 @@ class Engine final : public EngineBase {
   int* h_flags_ = nullptr;
   cudaEvent_t ev_c_ = nullptr, ev_d_ = nullptr, ev_s0_ = nullptr, ev_s1_ = nullptr;
   bool envs_valid_ = false;
-  std::vector<void*> allocs_, mpo_allocs_, tmp_allocs_;
+  std::vector<void*> allocs_, tmp_allocs_;
+  void* mpo_slab_ = nullptr;  // every MPO-dependent buffer (mixing matrices, environments, scratch)
   size_t bytes_ = 0, bytes_mpo_ = 0;
   ll nmax_ = 0, qmax_ = 0;
   bool mpo_set_ = false, mps_set_ = false, canonical_ = false;
