@@ -850,6 +850,19 @@ __global__ void wy_build_kernel(const T* __restrict__ R, ll ld, const T* __restr
   }
 }
 
+// one element into shared memory through the async copy path
+__device__ inline void cp_async_elem(double* dst, const double* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ inline void cp_async_elem(zc* dst, const zc* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+
+// Reflector blocks are double-buffered: block blk - 1 is copied from L2 with
+// cp.async while block blk is applied. Entries left of each reflector's first
+// element are masked in the arithmetic instead of zeroed in the copy.
 template <typename T>
 __global__ void __launch_bounds__(AQ_THREADS)
     apply_q_kernel(const T* __restrict__ R, ll ld, const T* __restrict__ Tb, int n, int nb,
@@ -857,7 +870,8 @@ __global__ void __launch_bounds__(AQ_THREADS)
                    T* __restrict__ Zg) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* zs = reinterpret_cast<T*>(smem_raw);  // [AQ_COLS][n] (rows contiguous: conflict-free)
-  T* vb = zs + (ll)n * AQ_COLS;            // [nb][n]
+  T* vbuf0 = zs + (ll)n * AQ_COLS;         // [nb][n], two buffers
+  T* vbuf1 = vbuf0 + (ll)nb * n;
   __shared__ T W[AQ_MAXNB][AQ_COLS];
   __shared__ T W2[AQ_MAXNB][AQ_COLS];
   const int c0 = blockIdx.x * AQ_COLS;
@@ -870,17 +884,25 @@ __global__ void __launch_bounds__(AQ_THREADS)
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nblk = (n - 1 + nb - 1) / nb;
+  auto prefetch = [&](int blk, T* dst) {
+    const int lo = blk * nb;
+    const int cnt = min(n - 2, lo + nb - 1) - lo + 1;
+    for (int e = threadIdx.x; e < cnt * n; e += blockDim.x) {
+      const int q = e / n, r = e % n;
+      cp_async_elem(dst + (ll)q * n + r, R + (ll)(lo + q) * ld + r);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  prefetch(nblk - 1, vbuf0);
   for (int blk = nblk - 1; blk >= 0; --blk) {
     const int lo = blk * nb;
     const int hi = min(n - 2, lo + nb - 1);
     const int cnt = hi - lo + 1;
-    __syncthreads();
-    for (int e = threadIdx.x; e < cnt * n; e += blockDim.x) {
-      const int q = e / n, r = e % n;
-      const int i = lo + q;
-      vb[(ll)q * n + r] = (r > i) ? R[(ll)i * ld + r] : ST<T>::zero();
-    }
-    __syncthreads();
+    T* vb = ((nblk - 1 - blk) & 1) ? vbuf1 : vbuf0;
+    T* vnext = ((nblk - 1 - blk) & 1) ? vbuf0 : vbuf1;
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncthreads();  // block blk has landed; the previous block's buffer is free again
+    if (blk > 0) prefetch(blk - 1, vnext);
     // W = V^H Z  (warp q -> row q of W)
     for (int q = warp; q < cnt; q += AQ_THREADS / 32) {
       T acc[AQ_COLS];
@@ -914,7 +936,7 @@ __global__ void __launch_bounds__(AQ_THREADS)
 #pragma unroll
       for (int c = 0; c < AQ_COLS; ++c) acc[c] = ST<T>::zero();
       for (int q = 0; q < cnt; ++q) {
-        const T vr = vb[(ll)q * n + r];
+        const T vr = (r > lo + q) ? vb[(ll)q * n + r] : ST<T>::zero();
 #pragma unroll
         for (int c = 0; c < AQ_COLS; ++c) acc[c] = acc[c] + ST<T>::mul(vr, W2[q][c]);
       }
@@ -1103,9 +1125,10 @@ void apply_q(const T* R, ll ld, const T* tau, int n, const double* Z, int K, con
     return;
   }
   const size_t cap = 220 * 1024 / sizeof(T);
-  int nb = (int)std::min<size_t>(AQ_MAXNB, cap / (size_t)n > AQ_COLS ? cap / (size_t)n - AQ_COLS : 0);
+  const size_t rows = cap / (size_t)n;  // rows of n elements that fit: AQ_COLS columns + two reflector blocks
+  int nb = (int)std::min<size_t>(AQ_MAXNB, rows > AQ_COLS ? (rows - AQ_COLS) / 2 : 0);
   if (nb < 1) throw std::runtime_error("apply_q: matrix order too large");
-  const size_t smem = sizeof(T) * (size_t)n * (AQ_COLS + nb);
+  const size_t smem = sizeof(T) * (size_t)n * (AQ_COLS + 2 * nb);
   static std::atomic<unsigned long long> attr{0};
   set_smem_attr_once(attr, (const void*)apply_q_kernel<T>, 220 * 1024);
   const int nblk = (n - 1 + nb - 1) / nb;

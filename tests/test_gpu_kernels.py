@@ -7,6 +7,8 @@ golden outputs of the reference modules (tests/golden/ref_primitives.npz).
 Tolerance: 1e-12 relative to the largest output magnitude (FP64 with a
 different summation order).
 """
+import zlib
+
 import numpy as np
 import pytest
 
@@ -39,7 +41,7 @@ GEMM_SHAPES = [(1, 1, 1), (3, 5, 7), (64, 64, 16), (65, 33, 17), (130, 70, 129),
 def test_gemm_dmma(cplx, shape, ta, tb):
     if not cplx and ta in ("C", "R"):
         pytest.skip("conjugation is the identity for real data")
-    rng = np.random.default_rng(hash((cplx, shape, ta, tb)) % 2**32)
+    rng = np.random.default_rng(zlib.crc32(repr((cplx, shape, ta, tb)).encode()))
     M, N, K = shape
     A = rnd(rng, (K, M) if ta in ("T", "C") else (M, K), cplx)
     B = rnd(rng, (N, K) if tb == "T" else (K, N), cplx)
@@ -60,11 +62,12 @@ SPLIT_SHAPES = [(1, 1, 1), (37, 45, 29), (128, 128, 64), (200, 130, 300), (256, 
 @pytest.mark.parametrize("ta,tb", [("N", "N"), ("N", "T"), ("T", "N"), ("C", "T")])
 def test_gemm_bf16x3_tcgen05(cplx, shape, ta, tb):
     """Precision-form GEMM (three-term BF16 split, FP32 accumulation in tensor memory):
-    error below 2.5e-7 sqrt(K) of sum_k |a_ik| |b_kj| per entry against the FP64
-    product (split truncation ~2^-24 per term, FP32 accumulation growing as sqrt(K))."""
+    error below (4e-7 + 2.5e-7 sqrt(K)) of sum_k |a_ik| |b_kj| per entry against the
+    FP64 product (split truncation up to ~3 x 2^-24 per product, FP32 accumulation
+    growing as sqrt(K))."""
     if not cplx and ta == "C":
         pytest.skip("conjugation is the identity for real data")
-    rng = np.random.default_rng(hash((cplx, shape, ta, tb, 7)) % 2**32)
+    rng = np.random.default_rng(zlib.crc32(repr((cplx, shape, ta, tb, 7)).encode()))
     M, N, K = shape
     A = rnd(rng, (K, M) if ta in ("T", "C") else (M, K), cplx)
     B = rnd(rng, (N, K) if tb == "T" else (K, N), cplx)
@@ -74,7 +77,7 @@ def test_gemm_bf16x3_tcgen05(cplx, shape, ta, tb):
     alpha, beta = 0.75, -0.5
     ref = alpha * opA @ opB + beta * C0
     out = dmrg2.gemm_bf16x3(A, B, ta, tb, alpha=alpha, beta=beta, C=C0)
-    bound = 2.5e-7 * np.sqrt(K) * abs(alpha) * (np.abs(opA) @ np.abs(opB)) + 1e-15
+    bound = (4e-7 + 2.5e-7 * np.sqrt(K)) * abs(alpha) * (np.abs(opA) @ np.abs(opB)) + 1e-15
     assert np.all(np.abs(out - ref) <= bound), float(np.max(np.abs(out - ref) / bound))
     # and it is not the FP64 product: the split really ran at reduced precision
     if K >= 64:
