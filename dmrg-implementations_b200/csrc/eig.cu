@@ -29,6 +29,8 @@
 //      compact-WY blocks to its own slab of columns (columns are independent).
 #include <cooperative_groups.h>
 
+#include <cstdlib>
+
 #include "kernels.cuh"
 
 namespace cg = cooperative_groups;
@@ -507,13 +509,347 @@ static cudaError_t hetrd_reg2_launch(double* G, int n, ll ld, double* d, double*
   return cudaLaunchKernelEx(&cfg, hetrd_reg2_kernel<NT, RW, C>, G, n, ld, d, e, tau);
 }
 
+// ----------------------------------------------------------------------------
+// 1c. The register-resident reduction with a push exchange. Instead of a
+//     cluster barrier followed by remote loads, every owner stores (p'_r,
+//     column-(k+2)_r) for its rows and its warps' partials of s' straight into
+//     every other CTA's shared memory with st.async, which counts the bytes on
+//     the receiver's mbarrier (its own entries it stores locally); a CTA starts
+//     step k once its barrier has seen every peer's bytes of step k and its own
+//     threads have passed a CTA barrier. Two parity buffers (and barriers) carry
+//     consecutive steps. A buffer is rewritten two steps after it was read, and
+//     its writer can only get there after receiving the reader's next push,
+//     which the reader issues after its last read (the complete_tx of st.async
+//     is a release at cluster scope, the wait an acquire), so no further
+//     barrier is needed. Waits are bounded: a CTA that gives up marks the whole
+//     cluster failed and the result is poisoned (d[0] = NaN) instead of hanging.
+// ----------------------------------------------------------------------------
+static constexpr int HP_SPIN = 1 << 20;  // polls of one barrier phase before giving up
+
+__device__ inline uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ inline uint32_t cluster_addr(uint32_t a, int cta) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(cta));
+  return r;
+}
+__device__ inline void push_v2(uint32_t dst, double a, double b, uint32_t bar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f64 [%0], {%1, %2}, [%3];"
+               ::"r"(dst), "d"(a), "d"(b), "r"(bar) : "memory");
+}
+__device__ inline void push_f64(uint32_t dst, double a, uint32_t bar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.f64 [%0], %1, [%2];"
+               ::"r"(dst), "d"(a), "r"(bar) : "memory");
+}
+__device__ inline void bar_expect(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// true once the phase of the given parity has completed, false after HP_SPIN polls
+// or when the cluster has been marked failed
+__device__ inline bool bar_wait(uint32_t bar, uint32_t parity, const volatile int* fail) {
+  for (int it = 0; it < HP_SPIN; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (*fail) return false;
+  }
+  return false;
+}
+
+template <int NT, int RW, int C>
+__global__ void __launch_bounds__(HT_THREADS, 1)
+    hetrd_push_kernel(double* __restrict__ G, int n, ll ld, double* __restrict__ dg,
+                      double* __restrict__ eg, double* __restrict__ tau) {
+  static_assert((C & (C - 1)) == 0 && C <= 32, "cluster size: power of two <= 32");
+  static_assert(NT % 2 == 0, "column slots come in pairs");
+  cg::cluster_group cluster = cg::this_cluster();
+  constexpr int NW = HT_THREADS / 32;
+  constexpr int NP = NT / 2;
+  const int rank = (int)cluster.block_rank();
+  extern __shared__ __align__(16) double hsm[];
+  __shared__ __align__(8) unsigned long long bars[2];
+  __shared__ int fail_s;
+  const int n2 = (n + 1) & ~1;
+  double* pc0 = hsm;            // (p_r, c_r) pairs of step parity 0, natural row order (pushed)
+  double* pc1 = pc0 + 2 * n2;   // parity 1
+  double* xs0 = pc1 + 2 * n2;   // column k (parity buffers, computed locally)
+  double* xs1 = xs0 + n2;
+  double* sa0 = xs1 + n2;       // C * NW partials of s (pushed), parity 0
+  double* sa1 = sa0 + C * NW;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  auto col = [&](int t) { return 2 * lane + 64 * (t >> 1) + (t & 1); };
+  const bool g_pairs = ((ld & 1) == 0) && ((reinterpret_cast<uintptr_t>(G) & 15) == 0);
+  const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
+  // bytes pushed by the peers per step: their rows' (p, c) pairs and their warps' partials
+  auto step_bytes = [&]() { return (uint32_t)(16 * (n - (n - rank + C - 1) / C) + 8 * (C - 1) * NW); };
+  // lane d < C, d != rank, pushes to CTA d; lane rank stores into this CTA's buffers
+  // (mapa keeps offsets, so one base address per window: buffers are at fixed offsets
+  // from pc0, the second barrier 8 bytes after the first)
+  uint32_t d_base = 0, d_bar0 = 0;
+  if (lane < C) {
+    d_base = cluster_addr(smem_u32(pc0), lane);
+    d_bar0 = cluster_addr(bar0, lane);
+  }
+  const uint32_t o_pc1 = 16u * (uint32_t)n2, o_sa0 = 48u * (uint32_t)n2, o_sa1 = o_sa0 + 8u * C * NW;
+  volatile int* failv = &fail_s;
+  auto give_up = [&]() {
+    if (!*failv)
+      for (int c = 0; c < C; ++c) {
+        const uint32_t a = cluster_addr(smem_u32(&fail_s), c);
+        asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(a), "r"(1) : "memory");
+      }
+  };
+  if (tid == 0) {
+    fail_s = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar0), "r"(1) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar1), "r"(1) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    bar_expect(bar0, step_bytes());                  // step 0 (pushed by the prologue)
+    if (n - 2 >= 1) bar_expect(bar1, step_bytes());  // step 1
+  }
+
+  int rr[RW];
+  double g[RW][NT];
+#pragma unroll
+  for (int i = 0; i < RW; ++i) {
+    rr[i] = (warp + NW * i) * C + rank;
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+      const int j = col(t);
+      g[i][t] = (rr[i] < n && j < n) ? G[(ll)rr[i] * ld + j] : 0.0;
+    }
+  }
+  for (int j = tid; j < n; j += HT_THREADS) xs0[j] = G[j];
+  // barriers initialised and armed everywhere, every row loaded (rank 0 overwrites row k
+  // from step k on)
+  cluster.sync();
+  // ---- prologue: column 0 (row 0 by symmetry), its reflector, the first symv, pushed
+  double tk, sc, beta;
+  {
+    double xn2 = 0.0;
+    for (int j = 2 + lane; j < n; j += 32) xn2 += xs0[j] * xs0[j];
+    xn2 = warp_sum_d(xn2);
+    house_real1(xs0[1], xn2, tk, sc, beta);
+    if (rank == 0 && tid == 0) {
+      dg[0] = xs0[0];
+      eg[0] = beta;
+      tau[0] = tk;
+    }
+    double sp = 0.0;
+#pragma unroll
+    for (int i = 0; i < RW; ++i) {
+      const int r = rr[i];
+      double acc = 0.0;
+#pragma unroll
+      for (int t = 0; t < NT; ++t) {
+        const int j = col(t);
+        if (j >= 2 && j < n) acc += g[i][t] * xs0[j];
+      }
+      acc = warp_sum_d(acc);
+      const double c1 = __shfl_sync(0xffffffffu, g[i][1], 0);  // column 1 sits in lane 0, slot 1
+      if (r < n) {
+        double p = 0.0;
+        if (r >= 1) {
+          p = tk * (c1 + sc * acc);
+          sp += p * ((r == 1) ? 1.0 : xs0[r] * sc);
+        }
+        if (lane == rank) *reinterpret_cast<double2*>(pc0 + 2 * r) = make_double2(p, c1);
+        else if (lane < C) push_v2(d_base + 16u * (uint32_t)r, p, c1, d_bar0);
+      }
+    }
+    if (lane == rank) sa0[rank * NW + warp] = sp;
+    else if (lane < C) push_f64(d_base + o_sa0 + 8u * (uint32_t)(rank * NW + warp), sp, d_bar0);
+  }
+
+  for (int k = 0; k < n - 1; ++k) {
+    const int par = k & 1;
+    const double* pc = par ? pc1 : pc0;
+    const double* sa = par ? sa1 : sa0;
+    const double* xs = par ? xs1 : xs0;
+    double* xsn = par ? xs0 : xs1;
+    double* pcn = par ? pc0 : pc1;
+    double* san = par ? sa0 : sa1;
+    const uint32_t bar = par ? bar1 : bar0;
+    const uint32_t n_pc = d_base + (par ? 0u : o_pc1), n_sa = d_base + (par ? o_sa0 : o_sa1);
+    const uint32_t n_bar = d_bar0 + (par ? 0u : 8u);
+    // (1) every CTA's pushes of step k have landed
+    if (!bar_wait(bar, (uint32_t)((k >> 1) & 1), failv)) give_up();
+    if (tid == 0 && k + 2 <= n - 2 && !*failv) bar_expect(bar, step_bytes());  // re-arm for step k+2
+    __syncthreads();  // this CTA's own entries and column k (written last step) visible to all
+    double ssum = 0.0;
+    for (int q = lane; q < C * NW; q += 32) ssum += sa[q];
+    ssum = warp_sum_d(ssum);
+    // (2) w = p - tau s / 2 v; fused rank-2 update + next symv + next column
+    const double a2 = -0.5 * tk * ssum;
+    const double wk1 = pc[2 * (k + 1)] + a2;  // v[k+1] = 1
+    double vr[RW], wr[RW], acc[RW], c2[RW];
+    bool act[RW];
+#pragma unroll
+    for (int i = 0; i < RW; ++i) {
+      const int r = rr[i];
+      vr[i] = 0.0;
+      wr[i] = 0.0;
+      act[i] = (r >= k + 1 && r < n);
+      if (act[i]) {
+        vr[i] = (r == k + 1) ? 1.0 : xs[r] * sc;
+        wr[i] = pc[2 * r] + a2 * vr[i];
+      }
+      acc[i] = 0.0;
+      c2[i] = 0.0;
+    }
+    double nrm = 0.0, a_next = 0.0, d_next = 0.0;
+    const bool store_v = (rank == 0);
+    auto one = [&](const int t, const int j, const double xv, const double pv, const double cv, const bool edge) {
+      const double vj = (edge && j == k + 1) ? 1.0 : xv * sc;
+      const double wj = pv + a2 * vj;
+      const double xn = cv - vj * wk1 - wj;
+      if (!edge || j >= k + 3) nrm += xn * xn;
+      if (edge && j == k + 2) a_next = xn;
+      if (edge && j == k + 1) d_next = xn;
+#pragma unroll
+      for (int i = 0; i < RW; ++i) {
+        if (act[i]) {
+          const double gg = g[i][t] - vr[i] * wj - wr[i] * vj;
+          g[i][t] = gg;
+          if (!edge || j >= k + 3) acc[i] += gg * xn;
+          if (edge && j == k + 2) c2[i] = gg;
+        }
+      }
+      return xn;
+    };
+#pragma unroll
+    for (int u = 0; u < NP; ++u) {
+      const int base = 64 * u;
+      if (base + 64 <= k + 1 || base >= n) continue;
+      const int j0 = base + 2 * lane;
+      const bool mine = (u % NW) == warp;
+      if (base >= k + 3 && base + 64 <= n) {
+        const double2 xv = *reinterpret_cast<const double2*>(xs + j0);
+        const double2 q0 = *reinterpret_cast<const double2*>(pc + 2 * j0);      // (p, c) of j0
+        const double2 q1 = *reinterpret_cast<const double2*>(pc + 2 * j0 + 2);  // (p, c) of j0 + 1
+        double2 xo;
+        xo.x = one(2 * u, j0, xv.x, q0.x, q0.y, false);
+        xo.y = one(2 * u + 1, j0 + 1, xv.y, q1.x, q1.y, false);
+        if (mine) {
+          *reinterpret_cast<double2*>(xsn + j0) = xo;
+          if (store_v) {
+            if (g_pairs) {
+              double2 vv;
+              vv.x = xv.x * sc;
+              vv.y = xv.y * sc;
+              *reinterpret_cast<double2*>(G + (ll)k * ld + j0) = vv;
+            } else {
+              G[(ll)k * ld + j0] = xv.x * sc;
+              G[(ll)k * ld + j0 + 1] = xv.y * sc;
+            }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int j = j0 + h;
+          if (j >= k + 1 && j < n) {
+            const double xn = one(2 * u + h, j, xs[j], pc[2 * j], pc[2 * j + 1], true);
+            if (mine) {
+              xsn[j] = xn;
+              if (store_v) G[(ll)k * ld + j] = (j == k + 1) ? 1.0 : xs[j] * sc;
+            }
+          }
+        }
+      }
+    }
+    // (3) next reflector (every warp derives the same one); push p', column k+2, s'
+    nrm = warp_sum_d(nrm);
+    a_next = __shfl_sync(0xffffffffu, a_next, ((k + 2) & 63) >> 1);
+    d_next = __shfl_sync(0xffffffffu, d_next, ((k + 1) & 63) >> 1);
+    double tk2 = 0.0, sc2 = 0.0, beta2 = 0.0;
+    if (k + 2 <= n - 1) house_real1(a_next, nrm, tk2, sc2, beta2);
+    if (rank == 0 && tid == 32) {
+      dg[k + 1] = d_next;
+      eg[k + 1] = beta2;
+      if (k + 1 < n - 1) tau[k + 1] = tk2;
+    }
+    const bool push = (k + 1 <= n - 2);  // step k+1 exists
+    double sp = 0.0;
+#pragma unroll
+    for (int i = 0; i < RW; ++i) {
+      const int r = rr[i];
+      const double a = warp_sum_d(acc[i]);
+      const double c = __shfl_sync(0xffffffffu, c2[i], ((k + 2) & 63) >> 1);
+      if (r < n) {
+        double p = 0.0;
+        if (r >= k + 2) {
+          p = tk2 * (c + sc2 * a);
+          const double xnr = pc[2 * r + 1] - vr[i] * wk1 - wr[i];
+          sp += p * ((r == k + 2) ? 1.0 : xnr * sc2);
+        }
+        if (push) {
+          if (lane == rank) *reinterpret_cast<double2*>(pcn + 2 * r) = make_double2(p, c);
+          else if (lane < C) push_v2(n_pc + 16u * (uint32_t)r, p, c, n_bar);
+        }
+      }
+    }
+    if (push) {
+      if (lane == rank) san[rank * NW + warp] = sp;
+      else if (lane < C) push_f64(n_sa + 8u * (uint32_t)(rank * NW + warp), sp, n_bar);
+    }
+    tk = tk2;
+    sc = sc2;
+  }
+  cluster.sync();  // no CTA leaves while a peer may still address its shared memory
+  if (rank == 0 && tid == 0 && *failv) dg[0] = __longlong_as_double(0x7ff8000000000000ll);
+}
+
+template <int NT, int RW, int C>
+static cudaError_t hetrd_push_launch(double* G, int n, ll ld, double* d, double* e, double* tau,
+                                     cudaStream_t s) {
+  static std::atomic<unsigned long long> attr_cluster{0};
+  func_attr_once(attr_cluster, (const void*)hetrd_push_kernel<NT, RW, C>,
+                 cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(C);
+  cfg.blockDim = dim3(HT_THREADS);
+  const size_t n2 = (size_t)((n + 1) & ~1);
+  cfg.dynamicSmemBytes = sizeof(double) * (6 * n2 + 2 * (size_t)C * (HT_THREADS / 32));
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, hetrd_push_kernel<NT, RW, C>, G, n, ld, d, e, tau);
+}
+
+// exchange used by the register-resident reduction: 1 = push (st.async + mbarrier),
+// 0 = cluster barrier + pull; DMRG2_HETRD_EXCHANGE=pull selects the latter
+static int hetrd_exchange() {
+  static const int v = [] {
+    const char* e = std::getenv("DMRG2_HETRD_EXCHANGE");
+    return (e && std::string(e) == "pull") ? 0 : 1;
+  }();
+  return v;
+}
+
 // register-resident reduction for real G with 32 <= n <= 512; false when the device
 // refused the cluster (the caller then takes the shared-memory kernel)
 static bool hetrd_reg(double* G, int n, ll ld, double* d, double* e, double* tau, cudaStream_t s) {
   static std::atomic<int> refused{0};
   if (n < 32 || n > 512 || refused.load()) return false;
   cudaError_t err;
-  if (n <= 128) err = hetrd_reg2_launch<4, 1, 8>(G, n, ld, d, e, tau, s);
+  if (hetrd_exchange()) {
+    if (n <= 128) err = hetrd_push_launch<4, 1, 8>(G, n, ld, d, e, tau, s);
+    else if (n <= 256) err = hetrd_push_launch<8, 1, 16>(G, n, ld, d, e, tau, s);
+    else err = hetrd_push_launch<16, 2, 16>(G, n, ld, d, e, tau, s);
+  } else if (n <= 128) err = hetrd_reg2_launch<4, 1, 8>(G, n, ld, d, e, tau, s);
   else if (n <= 256) err = hetrd_reg2_launch<8, 1, 16>(G, n, ld, d, e, tau, s);
   else err = hetrd_reg2_launch<16, 2, 16>(G, n, ld, d, e, tau, s);
   if (err == cudaSuccess) return true;
@@ -722,23 +1058,34 @@ __global__ void tridiag_invit_kernel(const double* __restrict__ dg, const double
 }
 
 // ----------------------------------------------------------------------------
-// 4. Gram-Schmidt inside groups of nearly equal eigenvalues. Each CTA takes
-//    candidate group starts j = blockIdx.x + m * gridDim.x and skips those
-//    that do not start a group of two or more.
-//    The group's columns are staged transposed in shared memory (zs[q][i]) when
-//    they fit and orthonormalised by classical Gram-Schmidt with one
-//    re-orthogonalisation pass (CGS2, "twice is enough": Giraud, Langou and
-//    Rozloznik 2005). Per vector the dots with all earlier members are formed
-//    at once, one warp per earlier member, then subtracted in one pass.
+// 4. Gram-Schmidt inside groups of nearly equal eigenvalues. A group is a run
+//    of consecutive eigenvalues (descending) whose neighbours differ by at most
+//    gtol; each CTA takes candidate group starts j = blockIdx.x + m * gridDim.x
+//    and skips those that do not start a group of two or more.
+//    Vector q of a group is orthogonalised against its window: the earlier
+//    members p with lam_p - lam_q <= gtol. Pairs further apart than gtol are
+//    treated like pairs in different groups (their overlap is bounded by the
+//    eigenvector perturbation bound eps |T| / gap and removed by the
+//    Newton-Schulz step that follows). In the dense tail of a DMRG spectrum
+//    the runs chain over tens of eigenvalues while each window holds a few.
+//    Classical Gram-Schmidt with one re-orthogonalisation pass (CGS2, "twice
+//    is enough": Giraud, Langou and Rozloznik 2005): per vector the dots with
+//    the window members are formed at once, one warp per member, then
+//    subtracted in one pass. The window members live in a ring of R vectors
+//    in shared memory (column-contiguous); the next vector is fetched into
+//    registers while the current one is processed. A group whose largest
+//    window does not fit the ring takes the whole-group path on global memory.
 // ----------------------------------------------------------------------------
-static constexpr int GS_THREADS = 256;
+static constexpr int GS_THREADS = 512;
 static constexpr int GS_SMEM = 200 * 1024;
+static constexpr int GS_RP = 4;  // rows per thread of the ring path (n <= GS_RP * GS_THREADS)
 
-__global__ void __launch_bounds__(GS_THREADS)
+__global__ void __launch_bounds__(GS_THREADS, 1)
     group_cgs_kernel(double* __restrict__ Z, int n, int K, const double* __restrict__ lam,
                      const SvdOut* __restrict__ tr, double gtol_rel) {
   extern __shared__ __align__(16) double gsm[];
   __shared__ double red[GS_THREADS / 32 + 1];
+  __shared__ int wmax_s;
   constexpr int NW = GS_THREADS / 32;
   const int kk = tr->k;
   const double gtol = gtol_rel * fmax(fabs(lam[0]), 1e-300);
@@ -750,18 +1097,114 @@ __global__ void __launch_bounds__(GS_THREADS)
     while (end < kk && fabs(lam[end - 1] - lam[end]) <= gtol) ++end;
     const int g = end - j;
     if (g < 2) continue;
-    const bool staged = (size_t)g * n + g <= cap;  // else the vectors stay in global memory
-    double* zs = gsm;
-    double* cf = gsm + (staged ? (size_t)g * n : 0);  // coefficients, g <= cap always (g <= K <= n)
-    auto at = [&](int q, int i) -> double& {
-      return staged ? zs[(ll)q * n + i] : Z[(ll)i * K + j + q];
-    };
-    if (staged)
-      for (ll e = tid; e < (ll)g * n; e += GS_THREADS) {
-        const int q = (int)(e % g), i = (int)(e / g);
-        zs[(ll)q * n + i] = Z[(ll)i * K + j + q];
-      }
+    // shared layout: lam of the group [g], window starts [g] (ints in a double slot each),
+    // window coefficients [g], the ring [R][n]
+    double* lam_s = gsm;
+    int* lo_s = reinterpret_cast<int*>(gsm + g);
+    double* cfs = gsm + 2 * (size_t)g;
+    double* ring = gsm + 3 * (size_t)g;
+    const int R = (int)min((size_t)g, (cap - 3 * (size_t)g) / (size_t)n);
+    if (tid == 0) wmax_s = 0;
+    for (int q = tid; q < g; q += GS_THREADS) lam_s[q] = lam[j + q];
     __syncthreads();
+    for (int q = tid; q < g; q += GS_THREADS) {
+      int lo = q;
+      while (lo > 0 && lam_s[lo - 1] - lam_s[q] <= gtol) --lo;
+      lo_s[q] = lo;
+      atomicMax(&wmax_s, q - lo);
+    }
+    __syncthreads();
+    if (wmax_s <= R - 1 && n <= GS_RP * GS_THREADS) {
+      // ---- windowed ring path (vectors are fetched two ahead into registers)
+      double cur[GS_RP], pre1[GS_RP], pre2[GS_RP];
+#pragma unroll
+      for (int m = 0; m < GS_RP; ++m) {
+        const int i = tid + m * GS_THREADS;
+        pre1[m] = (i < n) ? Z[(ll)i * K + j] : 0.0;
+        pre2[m] = (i < n) ? Z[(ll)i * K + j + 1] : 0.0;  // g >= 2
+      }
+      for (int q = 0; q < g; ++q) {
+        const int sq_slot = q % R;
+        double* vq = ring + (size_t)sq_slot * n;
+#pragma unroll
+        for (int m = 0; m < GS_RP; ++m) {
+          const int i = tid + m * GS_THREADS;
+          cur[m] = pre1[m];
+          pre1[m] = pre2[m];
+          if (i < n) vq[i] = cur[m];
+        }
+        if (q + 2 < g)
+#pragma unroll
+          for (int m = 0; m < GS_RP; ++m) {
+            const int i = tid + m * GS_THREADS;
+            if (i < n) pre2[m] = Z[(ll)i * K + j + q + 2];
+          }
+        const int lo = lo_s[q], w = q - lo;
+        const int lo_slot = lo % R;
+        __syncthreads();  // vector q staged; the previous vector final
+        double sq = 0.0;
+        for (int pass = 0; pass < 2 && w > 0; ++pass) {
+          for (int p = warp; p < w; p += NW) {
+            const int slot = lo_slot + p < R ? lo_slot + p : lo_slot + p - R;
+            const double* vp = ring + (size_t)slot * n;
+            double sum = 0.0;
+            for (int i = lane; i < n; i += 32) sum += vp[i] * vq[i];
+            sum = warp_sum_d(sum);
+            if (lane == 0) cfs[p] = sum;
+          }
+          __syncthreads();  // coefficients ready
+          // a second pass only when the first removed more than half of the (unit) norm:
+          // |v'|^2 = 1 - sum cf^2 < 1/2 (Daniel, Gragg, Kaufman and Stewart 1976)
+          double c2 = 0.0;
+          for (int p = 0; p < w; ++p) c2 += cfs[p] * cfs[p];
+          const bool again = (pass == 0) && (c2 > 0.5);
+          sq = 0.0;
+#pragma unroll
+          for (int m = 0; m < GS_RP; ++m) {
+            const int i = tid + m * GS_THREADS;
+            if (i < n) {
+              double v = cur[m];
+              int slot = lo_slot;
+              for (int p = 0; p < w; ++p) {
+                v -= cfs[p] * ring[(size_t)slot * n + i];
+                slot = (slot + 1 == R) ? 0 : slot + 1;
+              }
+              cur[m] = v;
+              vq[i] = v;
+              sq += v * v;
+            }
+          }
+          if (!again) break;
+          __syncthreads();  // vq updated before the second pass's dots
+        }
+        if (w == 0) {
+#pragma unroll
+          for (int m = 0; m < GS_RP; ++m) sq += cur[m] * cur[m];
+        }
+        sq = warp_sum_d(sq);
+        if (lane == 0) red[warp] = sq;
+        __syncthreads();  // partial norms ready (and every read of the window done)
+        double tot = 0.0;
+#pragma unroll
+        for (int w2 = 0; w2 < NW; ++w2) tot += red[w2];
+        const double inv = tot > 0.0 ? 1.0 / sqrt(tot) : 0.0;
+#pragma unroll
+        for (int m = 0; m < GS_RP; ++m) {
+          const int i = tid + m * GS_THREADS;
+          if (i < n) {
+            const double v = cur[m] * inv;
+            vq[i] = v;
+            Z[(ll)i * K + j + q] = v;
+          }
+        }
+      }
+      __syncthreads();  // the shared area is reused by this CTA's next group
+      continue;
+    }
+    // ---- whole-group path (a window larger than the ring): every earlier member, on
+    //      global memory
+    double* cf = gsm + 3 * (size_t)g;  // coefficients, 4 g <= cap always (g <= K <= n)
+    auto at = [&](int q, int i) -> double& { return Z[(ll)i * K + j + q]; };
     for (int q = 0; q < g; ++q) {
       for (int pass = 0; pass < 2 && q > 0; ++pass) {
         for (int p = warp; p < q; p += NW) {
@@ -797,12 +1240,6 @@ __global__ void __launch_bounds__(GS_THREADS)
       for (int i = tid; i < n; i += GS_THREADS) at(q, i) *= inv;
       __syncthreads();
     }
-    if (staged)
-      for (ll e = tid; e < (ll)g * n; e += GS_THREADS) {
-        const int q = (int)(e % g), i = (int)(e / g);
-        Z[(ll)i * K + j + q] = zs[(ll)q * n + i];
-      }
-    __syncthreads();  // the shared staging area is reused by this CTA's next group
   }
 }
 
@@ -986,38 +1423,47 @@ __global__ void ns_check_kernel(const double* __restrict__ S, int K, SvdOut* out
 }
 
 // ----------------------------------------------------------------------------
-// truncation decision from the eigenvalues (single thread)
+// truncation decision from the eigenvalues (one CTA)
 // ----------------------------------------------------------------------------
-__global__ void eig_truncate_kernel(const double* __restrict__ dg, const double* __restrict__ lam,
-                                    int n, int K, int chi_max, double cutoff, int relative,
-                                    SvdOut* out) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__global__ void __launch_bounds__(256)
+    eig_truncate_kernel(const double* __restrict__ dg, const double* __restrict__ lam, int n, int K,
+                        int chi_max, double cutoff, int relative, SvdOut* out) {
+  __shared__ double sh[33];
+  __shared__ int kmin;
+  const int tid = threadIdx.x;
   double tr = 0.0;
-  for (int i = 0; i < n; ++i) tr += dg[i];
+  for (int i = tid; i < n; i += blockDim.x) tr += dg[i];
+  tr = block_sum_t<double>(tr, sh);
   const double l0 = fmax(lam[0], 0.0);
   // density-matrix rounding floor: eigenvalues below ~16 eps lambda_max are noise
   const double noise = 16.0 * 2.2e-16 * l0;
   double thr = relative ? (cutoff * cutoff) * l0 : cutoff * cutoff;
   thr = fmax(thr, noise);
-  int k = chi_max < K ? chi_max : K;
-  for (int r = 0; r < k; ++r)
-    if (!(lam[r] > thr)) { k = r; break; }
-  if (k < 1) k = 1;
-  double kept = 0.0;
-  int nz = 0;
-  for (int r = 0; r < K; ++r) {
+  const int kcap = chi_max < K ? chi_max : K;
+  if (tid == 0) kmin = kcap;
+  __syncthreads();
+  for (int r = tid; r < kcap; r += blockDim.x)
+    if (!(lam[r] > thr)) atomicMin(&kmin, r);  // the first eigenvalue at or below the threshold
+  __syncthreads();
+  const int k = max(kmin, 1);
+  double kept = 0.0, nz = 0.0;
+  for (int r = tid; r < K; r += blockDim.x) {
     if (r < k) kept += fmax(lam[r], 0.0);
-    if (lam[r] > noise) ++nz;
+    if (lam[r] > noise) nz += 1.0;
   }
-  out->k = k;
-  out->nonzero = nz;
-  out->trunc_err = fmax(tr - kept, 0.0);
-  out->sigma_max = sqrt(l0);
-  out->sigma_max2 = l0;
-  out->fro2 = tr;
-  out->jacobi_sweeps = 0;
-  out->jacobi_err = 0;
-  out->ns_done = 0;
+  kept = block_sum_t<double>(kept, sh);
+  nz = block_sum_t<double>(nz, sh);
+  if (tid == 0) {
+    out->k = k;
+    out->nonzero = (int)nz;
+    out->trunc_err = fmax(tr - kept, 0.0);
+    out->sigma_max = sqrt(l0);
+    out->sigma_max2 = l0;
+    out->fro2 = tr;
+    out->jacobi_sweeps = 0;
+    out->jacobi_err = 0;
+    out->ns_done = 0;
+  }
 }
 
 // ----------------------------------------------------------------------------
@@ -1146,7 +1592,7 @@ void ns_check(const double* S, int K, SvdOut* out, double tol, double* part, uns
 
 void eig_truncate(const double* d, const double* lam, int n, int K, int chi_max, double cutoff,
                   bool relative, SvdOut* out, cudaStream_t s) {
-  eig_truncate_kernel<<<1, 32, 0, s>>>(d, lam, n, K, chi_max, cutoff, relative ? 1 : 0, out);
+  eig_truncate_kernel<<<1, 256, 0, s>>>(d, lam, n, K, chi_max, cutoff, relative ? 1 : 0, out);
   DMRG2_CHECK_LAUNCH();
 }
 

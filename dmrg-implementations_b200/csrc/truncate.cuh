@@ -131,6 +131,8 @@ SvdOut eig_split(EigWork<T>& W, const T* theta, int m, int nt, char dir, int chi
   DMRG2_CUDA(cudaMemcpyAsync(W.h_out, W.out, sizeof(SvdOut), cudaMemcpyDeviceToHost, s));
   DMRG2_CUDA(cudaStreamSynchronize(s));
   SvdOut o = *W.h_out;
+  if (!std::isfinite(o.fro2))
+    throw std::runtime_error("eigensolver: non-finite density matrix or tridiagonal reduction");
   const int k = o.k;
   if (R) {
     copy_cols_conj<T>(W.Zg, K, m, k, left, s);  // U = conj(eigvecs of conj(G))

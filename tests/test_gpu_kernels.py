@@ -246,6 +246,31 @@ def test_svd_large_degenerate_cluster(cplx, cluster):
 
 
 @pytest.mark.parametrize("cplx", [False, True])
+def test_svd_chained_tail_group(cplx):
+    # the tail of a DMRG spectrum: 70 squared singular values 4e-15 apart (below the group
+    # tolerance 1e-14 of the largest), so they chain into one group of 70 whose windows hold
+    # two earlier members each; below them a gap to values under the noise floor. Kept
+    # vectors of values near the floor are accurate to eps / gap ~ 1e-2, hence 5e-8 on the
+    # reconstruction (tail singular values ~5e-7).
+    rng = np.random.default_rng(77 + cplx)
+    n = 512
+    Q1, _ = np.linalg.qr(rnd(rng, (n, n), cplx))
+    Q2, _ = np.linalg.qr(rnd(rng, (n, n), cplx))
+    lam_tail = 3e-13 - 0.4e-14 * np.arange(70)
+    s = np.concatenate([[1.0, 0.7, 0.5, 0.3], np.geomspace(0.1, 1e-5, 100), np.sqrt(lam_tail),
+                        np.geomspace(1e-8, 1e-9, n - 174)])
+    M = (Q1 * s) @ Q2.conj().T
+    keep = 174
+    for direction in ("R", "L"):
+        left, S, right, te = dmrg2.truncated_svd(M, keep + 20, 1e-300, direction)
+        assert left.shape[1] == keep  # the values below 16 eps of the largest are dropped
+        np.testing.assert_allclose(S[:keep] ** 2, s[:keep] ** 2, atol=1e-14)
+        close(left @ right, (Q1[:, :keep] * s[:keep]) @ Q2[:, :keep].conj().T, 5e-8)
+        iso = left.conj().T @ left if direction == "R" else right @ right.conj().T
+        np.testing.assert_allclose(iso, np.eye(keep), atol=1e-12)
+
+
+@pytest.mark.parametrize("cplx", [False, True])
 def test_lanczos_vs_dense(cplx):
     rng = np.random.default_rng(3 + cplx)
     cL, cR, d, D = 6, 7, 2, 3
