@@ -866,28 +866,32 @@ static bool hetrd_reg(double* G, int n, ll ld, double* d, double* e, double* tau
 // 2. K largest eigenvalues of (d, e) by Sturm-count multisection, one CTA per
 //    eigenvalue (blockDim+1 points per round)
 // ----------------------------------------------------------------------------
-// 1/a: hardware reciprocal estimate refined by two Newton-Raphson steps
-// y <- y + y (1 - a y) (each step doubles the correct bits). Only the sign of the
-// Sturm pivots matters, so the last-bit rounding of IEEE division is not needed.
-__device__ inline double rcp_nr(double a) {
-  double y;
-  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
-  double r = fma(-a, y, 1.0);
-  y = fma(y, r, y);
-  r = fma(-a, y, 1.0);
-  return fma(y, r, y);
-}
-
-// Number of eigenvalues of (d, e) below x: negative pivots of the LDL^T
-// factorisation of T - x I (Sturm), q_i = (d_i - x) - e_{i-1}^2 / q_{i-1}.
-__device__ inline int sturm_lt(const double* d, const double* e2, int n, double x, double pivmin) {
-  double q = d[0] - x;
-  if (fabs(q) < pivmin) q = -pivmin;
-  int c = (q < 0.0);
+// Number of eigenvalues of (d, e) below x: sign changes along the leading principal
+// minors P_0 = 1, P_1 = d_0 - x, P_{i+1} = (d_i - x) P_i - e_{i-1}^2 P_{i-1} (Sturm).
+// Compared with the ratio form q_i = P_i / P_{i-1} (LDL^T pivots) it needs no
+// division: one FMA per step on the dependent chain (e^2 P_{i-1} is formed a step
+// ahead), so a count costs a fraction of the ratio form's latency. Each step perturbs
+// d_i - x and e_{i-1}^2 by a few ulps relative, the same backward error as the ratio
+// form. The pair (P_{i-1}, P_i) is rescaled by an exact power of two every other step
+// to stay in range; an exact zero minor is replaced by -2^-60 P_{i-1}, the ratio
+// form's negative tiny pivot.
+__device__ inline int sturm_lt(const double* d, const double* e2, int n, double x) {
+  double a = 1.0, b = d[0] - x;
+  if (b == 0.0) b = -0x1p-60;
+  int c = (b < 0.0);
   for (int i = 1; i < n; ++i) {
-    q = (d[i] - x) - e2[i - 1] * rcp_nr(q);
-    if (fabs(q) < pivmin) q = -pivmin;
-    c += (q < 0.0);
+    const double t = e2[i - 1] * a;
+    double nb = fma(d[i] - x, b, -t);
+    if (nb == 0.0) nb = -0x1p-60 * b;
+    c += ((nb < 0.0) != (b < 0.0));
+    a = b;
+    b = nb;
+    if (i & 1) {
+      const double m = fmax(fabs(a), fabs(b));
+      const double f = (m > 0x1p+500) ? 0x1p-500 : (m < 0x1p-500) ? 0x1p+500 : 1.0;
+      a *= f;
+      b *= f;
+    }
   }
   return c;
 }
@@ -898,27 +902,37 @@ __global__ void __launch_bounds__(256)
   extern __shared__ double sm[];
   double* d = sm;
   double* e2 = sm + n;
-  __shared__ double a_s, b_s, piv_s, afloor_s;
+  __shared__ double a_s, b_s, afloor_s, lo_w[32], hi_w[32];
   __shared__ int tmin;
   const int j = blockIdx.x;
   if (j >= K) return;
+  // Gershgorin bounds, reduced over the block
+  double lo = 1e300, hi = -1e300;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     d[i] = dg[i];
     e2[i] = (i < n - 1) ? eg[i] * eg[i] : 0.0;
+    const double r = (i > 0 ? fabs(eg[i - 1]) : 0.0) + (i < n - 1 ? fabs(eg[i]) : 0.0);
+    lo = fmin(lo, dg[i] - r);
+    hi = fmax(hi, dg[i] + r);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    lo_w[threadIdx.x >> 5] = lo;
+    hi_w[threadIdx.x >> 5] = hi;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    double lo = 1e300, hi = -1e300, em = 0.0;
-    for (int i = 0; i < n; ++i) {
-      double r = (i > 0 ? fabs(eg[i - 1]) : 0.0) + (i < n - 1 ? fabs(eg[i]) : 0.0);
-      lo = fmin(lo, d[i] - r);
-      hi = fmax(hi, d[i] + r);
-      if (i < n - 1) em = fmax(em, e2[i]);
+    for (int w2 = 1; w2 < (int)(blockDim.x >> 5); ++w2) {
+      lo = fmin(lo, lo_w[w2]);
+      hi = fmax(hi, hi_w[w2]);
     }
     double w = fmax(hi - lo, fmax(fabs(hi), 1e-300));
     a_s = lo - 2e-15 * w;
     b_s = hi + 2e-15 * w;
-    piv_s = 1e-290 * fmax(1.0, em);
     afloor_s = 2.2e-16 * fmax(fabs(lo), fabs(hi));  // Sturm counts resolve eps*|T| at best
   }
   __syncthreads();
@@ -928,7 +942,7 @@ __global__ void __launch_bounds__(256)
     const double a = a_s, b = b_s;
     const double step = (b - a) / (double)(NT + 1);
     const double x = a + step * (threadIdx.x + 1);
-    const int c = sturm_lt(d, e2, n, x, piv_s);
+    const int c = sturm_lt(d, e2, n, x);
     if (threadIdx.x == 0) tmin = NT;
     __syncthreads();
     if (c >= t + 1) atomicMin(&tmin, (int)threadIdx.x);
@@ -1248,7 +1262,7 @@ __global__ void __launch_bounds__(GS_THREADS, 1)
 //    Reflectors are grouped in blocks of nb in compact WY form
 //    H_lo ... H_hi = I - V T V^H (Schreiber & Van Loan), T upper triangular
 //    (wy_build); apply_q then costs three barriers per block. Each CTA owns
-//    AQ_COLS columns of Z (columns are independent).
+//    a slab of 2, 4 or 8 columns of Z (columns are independent).
 // ----------------------------------------------------------------------------
 static constexpr int AQ_COLS = 8;
 static constexpr int AQ_MAXNB = 16;
@@ -1300,23 +1314,23 @@ __device__ inline void cp_async_elem(zc* dst, const zc* src) {
 // Reflector blocks are double-buffered: block blk - 1 is copied from L2 with
 // cp.async while block blk is applied. Entries left of each reflector's first
 // element are masked in the arithmetic instead of zeroed in the copy.
-template <typename T>
-__global__ void __launch_bounds__(AQ_THREADS)
+template <typename T, int COLS>
+__global__ void __launch_bounds__(AQ_THREADS, 1)
     apply_q_kernel(const T* __restrict__ R, ll ld, const T* __restrict__ Tb, int n, int nb,
                    const double* __restrict__ Z, int K, const SvdOut* __restrict__ tr,
                    T* __restrict__ Zg) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* zs = reinterpret_cast<T*>(smem_raw);  // [AQ_COLS][n] (rows contiguous: conflict-free)
-  T* vbuf0 = zs + (ll)n * AQ_COLS;         // [nb][n], two buffers
+  T* zs = reinterpret_cast<T*>(smem_raw);  // [COLS][n] (rows contiguous: conflict-free)
+  T* vbuf0 = zs + (ll)n * COLS;         // [nb][n], two buffers
   T* vbuf1 = vbuf0 + (ll)nb * n;
-  __shared__ T W[AQ_MAXNB][AQ_COLS];
-  __shared__ T W2[AQ_MAXNB][AQ_COLS];
-  const int c0 = blockIdx.x * AQ_COLS;
+  __shared__ T W[AQ_MAXNB][COLS];
+  __shared__ T W2[AQ_MAXNB][COLS];
+  const int c0 = blockIdx.x * COLS;
   const int kk = min(tr->k, K);
   if (c0 >= kk) return;
-  const int nc = min(AQ_COLS, kk - c0);
-  for (int e = threadIdx.x; e < n * AQ_COLS; e += blockDim.x) {
-    int i = e / AQ_COLS, c = e % AQ_COLS;
+  const int nc = min(COLS, kk - c0);
+  for (int e = threadIdx.x; e < n * COLS; e += blockDim.x) {
+    int i = e / COLS, c = e % COLS;
     zs[(ll)c * n + i] = (c < nc) ? ST<T>::make(Z[(ll)i * K + c0 + c], 0.0) : ST<T>::zero();
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1342,25 +1356,25 @@ __global__ void __launch_bounds__(AQ_THREADS)
     if (blk > 0) prefetch(blk - 1, vnext);
     // W = V^H Z  (warp q -> row q of W)
     for (int q = warp; q < cnt; q += AQ_THREADS / 32) {
-      T acc[AQ_COLS];
+      T acc[COLS];
 #pragma unroll
-      for (int c = 0; c < AQ_COLS; ++c) acc[c] = ST<T>::zero();
+      for (int c = 0; c < COLS; ++c) acc[c] = ST<T>::zero();
       const T* vq = vb + (ll)q * n;
       for (int r = lo + q + 1 + lane; r < n; r += 32) {
         const T vr = ST<T>::conj(vq[r]);
 #pragma unroll
-        for (int c = 0; c < AQ_COLS; ++c) acc[c] = acc[c] + ST<T>::mul(vr, zs[(ll)c * n + r]);
+        for (int c = 0; c < COLS; ++c) acc[c] = acc[c] + ST<T>::mul(vr, zs[(ll)c * n + r]);
       }
 #pragma unroll
-      for (int c = 0; c < AQ_COLS; ++c) {
+      for (int c = 0; c < COLS; ++c) {
         T sm2 = warp_sum_t<T>(acc[c]);
         if (lane == 0) W[q][c] = sm2;
       }
     }
     __syncthreads();
     // W2 = T W  (T upper triangular)
-    if (threadIdx.x < cnt * AQ_COLS) {
-      const int q = threadIdx.x / AQ_COLS, c = threadIdx.x % AQ_COLS;
+    if (threadIdx.x < cnt * COLS) {
+      const int q = threadIdx.x / COLS, c = threadIdx.x % COLS;
       const T* Tm = Tb + (ll)blk * AQ_MAXNB * AQ_MAXNB;
       T acc = ST<T>::zero();
       for (int p = q; p < cnt; ++p) acc = acc + ST<T>::mul(Tm[q * AQ_MAXNB + p], W[p][c]);
@@ -1369,21 +1383,21 @@ __global__ void __launch_bounds__(AQ_THREADS)
     __syncthreads();
     // Z -= V W2
     for (int r = lo + 1 + threadIdx.x; r < n; r += blockDim.x) {
-      T acc[AQ_COLS];
+      T acc[COLS];
 #pragma unroll
-      for (int c = 0; c < AQ_COLS; ++c) acc[c] = ST<T>::zero();
+      for (int c = 0; c < COLS; ++c) acc[c] = ST<T>::zero();
       for (int q = 0; q < cnt; ++q) {
         const T vr = (r > lo + q) ? vb[(ll)q * n + r] : ST<T>::zero();
 #pragma unroll
-        for (int c = 0; c < AQ_COLS; ++c) acc[c] = acc[c] + ST<T>::mul(vr, W2[q][c]);
+        for (int c = 0; c < COLS; ++c) acc[c] = acc[c] + ST<T>::mul(vr, W2[q][c]);
       }
 #pragma unroll
-      for (int c = 0; c < AQ_COLS; ++c) zs[(ll)c * n + r] = zs[(ll)c * n + r] - acc[c];
+      for (int c = 0; c < COLS; ++c) zs[(ll)c * n + r] = zs[(ll)c * n + r] - acc[c];
     }
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < n * AQ_COLS; e += blockDim.x) {
-    int i = e / AQ_COLS, c = e % AQ_COLS;
+  for (int e = threadIdx.x; e < n * COLS; e += blockDim.x) {
+    int i = e / COLS, c = e % COLS;
     if (c < nc) Zg[(ll)i * K + c0 + c] = zs[(ll)c * n + i];
   }
 }
@@ -1563,24 +1577,46 @@ static void copy_real_cols(const double* Z, int n, int K, T* Zg, cudaStream_t s)
   DMRG2_CHECK_LAUNCH();
 }
 
+// slab width (columns per CTA) and reflector block size of the back-transform
+template <typename T>
+static void aq_plan(int n, int K, int& cols, int& nb) {
+  const size_t cap = 220 * 1024 / sizeof(T);
+  const size_t rows = cap / (size_t)n;  // rows of n elements that fit: the column slab + two reflector blocks
+  // the narrowest slab that still fills one wave of CTAs (2 columns: K = 256 -> 128 CTAs)
+  cols = (K + 1) / 2 <= 160 ? 2 : (K + 3) / 4 <= 160 ? 4 : AQ_COLS;
+  nb = (int)std::min<size_t>(AQ_MAXNB, rows > (size_t)cols ? (rows - cols) / 2 : 0);
+  if (nb < 1) throw std::runtime_error("apply_q: matrix order too large");
+}
+
+template <typename T>
+void wy_build(const T* R, ll ld, const T* tau, int n, int K, T* Tb, cudaStream_t s) {
+  if (n < 2) return;
+  int cols, nb;
+  aq_plan<T>(n, K, cols, nb);
+  const int nblk = (n - 1 + nb - 1) / nb;
+  wy_build_kernel<T><<<nblk, 256, 0, s>>>(R, ld, tau, n, nb, Tb);
+  DMRG2_CHECK_LAUNCH();
+}
+
 template <typename T>
 void apply_q(const T* R, ll ld, const T* tau, int n, const double* Z, int K, const SvdOut* tr, T* Zg,
-             T* Tb, cudaStream_t s) {
+             T* Tb, cudaStream_t s, bool wy_ready) {
   if (n < 2) {  // Q = I
     copy_real_cols(Z, n, K, Zg, s);
     return;
   }
-  const size_t cap = 220 * 1024 / sizeof(T);
-  const size_t rows = cap / (size_t)n;  // rows of n elements that fit: AQ_COLS columns + two reflector blocks
-  int nb = (int)std::min<size_t>(AQ_MAXNB, rows > AQ_COLS ? (rows - AQ_COLS) / 2 : 0);
-  if (nb < 1) throw std::runtime_error("apply_q: matrix order too large");
-  const size_t smem = sizeof(T) * (size_t)n * (AQ_COLS + 2 * nb);
-  static std::atomic<unsigned long long> attr{0};
-  set_smem_attr_once(attr, (const void*)apply_q_kernel<T>, 220 * 1024);
-  const int nblk = (n - 1 + nb - 1) / nb;
-  wy_build_kernel<T><<<nblk, 256, 0, s>>>(R, ld, tau, n, nb, Tb);
-  DMRG2_CHECK_LAUNCH();
-  apply_q_kernel<T><<<(K + AQ_COLS - 1) / AQ_COLS, AQ_THREADS, smem, s>>>(R, ld, Tb, n, nb, Z, K, tr, Zg);
+  int cols, nb;
+  aq_plan<T>(n, K, cols, nb);
+  const size_t smem = sizeof(T) * (size_t)n * (cols + 2 * nb);
+  if (!wy_ready) wy_build<T>(R, ld, tau, n, K, Tb, s);
+  auto launch = [&](auto kern, int c, std::atomic<unsigned long long>& attr) {
+    set_smem_attr_once(attr, (const void*)kern, 220 * 1024);
+    kern<<<(K + c - 1) / c, AQ_THREADS, smem, s>>>(R, ld, Tb, n, nb, Z, K, tr, Zg);
+  };
+  static std::atomic<unsigned long long> attr2{0}, attr4{0}, attr8{0};
+  if (cols == 2) launch(apply_q_kernel<T, 2>, 2, attr2);
+  else if (cols == 4) launch(apply_q_kernel<T, 4>, 4, attr4);
+  else launch(apply_q_kernel<T, AQ_COLS>, AQ_COLS, attr8);
   DMRG2_CHECK_LAUNCH();
 }
 
@@ -1639,8 +1675,10 @@ template void transpose_conj<zc>(const zc*, ll, int, int, zc*, cudaStream_t);
 template void hetrd_cluster<double>(double*, int, ll, double*, double*, double*, cudaStream_t);
 template void hetrd_cluster<zc>(zc*, int, ll, double*, double*, zc*, cudaStream_t);
 template void apply_q<double>(const double*, ll, const double*, int, const double*, int,
-                              const SvdOut*, double*, double*, cudaStream_t);
+                              const SvdOut*, double*, double*, cudaStream_t, bool);
 template void apply_q<zc>(const zc*, ll, const zc*, int, const double*, int, const SvdOut*, zc*, zc*,
-                          cudaStream_t);
+                          cudaStream_t, bool);
+template void wy_build<double>(const double*, ll, const double*, int, int, double*, cudaStream_t);
+template void wy_build<zc>(const zc*, ll, const zc*, int, int, zc*, cudaStream_t);
 
 }  // namespace dmrg2

@@ -95,9 +95,13 @@ void tridiag_eigvecs(const double* d, const double* e, int n, int K, const doubl
                      const SvdOut* tr, double* Z, double* scratch, cudaStream_t s);
 void group_mgs(double* Z, int n, int K, const double* lam, const SvdOut* tr, double gtol_rel,
                cudaStream_t s);
+// compact-WY triangles of the reflector blocks that apply_q uses for (n, K); apply_q builds
+// them itself unless wy_ready says they were built already (e.g. on a side stream)
+template <typename T>
+void wy_build(const T* R, ll ld, const T* tau, int n, int K, T* Tb, cudaStream_t s);
 template <typename T>
 void apply_q(const T* R, ll ld, const T* tau, int n, const double* Z, int K, const SvdOut* tr, T* Zg,
-             T* Tb, cudaStream_t s);
+             T* Tb, cudaStream_t s, bool wy_ready = false);
 void ns_check(const double* S, int K, SvdOut* out, double tol, double* part, unsigned* counter,
               cudaStream_t s);
 void eig_truncate(const double* d, const double* lam, int n, int K, int chi_max, double cutoff,

@@ -231,7 +231,6 @@ __global__ void __launch_bounds__(VEC_THREADS)
   const ll x1 = (x0 + ch < n) ? x0 + ch : n;
   const int len = (x1 > x0) ? (int)(x1 - x0) : 0;
   const int ncoef = (PHASE == 2) ? 0 : nv;
-  const int stride = 2 * (nv + 1);
 
   if (PHASE >= 1) {
     for (int i = threadIdx.x; i < 2 * nv; i += blockDim.x) csh[i] = st->coef[i];
@@ -262,23 +261,28 @@ __global__ void __launch_bounds__(VEC_THREADS)
     }
     sr = warp_sum(sr);
     if (CPLX) si = warp_sum(si);
-    if (lane == 0) {
-      part[(ll)blockIdx.x * stride + 2 * i] = sr;
-      part[(ll)blockIdx.x * stride + 2 * i + 1] = si;
+    if (lane == 0) {  // partials are coefficient-major: part[idx][block]
+      part[(ll)(2 * i) * nblk + blockIdx.x] = sr;
+      part[(ll)(2 * i + 1) * nblk + blockIdx.x] = si;
     }
   }
   ww = block_sum(ww, red);
-  if (threadIdx.x == 0) part[(ll)blockIdx.x * stride + 2 * nv] = ww;
+  if (threadIdx.x == 0) part[(ll)(2 * nv) * nblk + blockIdx.x] = ww;
 
   if (!arrive_last(counter, nblk)) return;
 
-  // ---- finalize (last block): deterministic fixed-order sums
-  for (int c = threadIdx.x; c < 2 * ncoef + 1; c += blockDim.x) {
-    int idx = (c == 2 * ncoef) ? 2 * nv : c;
+  // ---- finalize (last block): deterministic fixed-order sums, one warp per coefficient
+  //      (lane l adds blocks l, l+32, ... in order, then a fixed shuffle tree)
+  for (int c = wid; c < 2 * ncoef + 1; c += NW) {
+    const int idx = (c == 2 * ncoef) ? 2 * nv : c;
+    const double* pc = part + (ll)idx * nblk;
     double s = 0.0;
-    for (int b = 0; b < nblk; ++b) s += part[(ll)b * stride + idx];
-    if (c == 2 * ncoef) st->nrm2 = s;
-    else st->coef[c] = s;
+    for (int b = lane; b < nblk; b += 32) s += pc[b];
+    s = warp_sum(s);
+    if (lane == 0) {
+      if (c == 2 * ncoef) st->nrm2 = s;
+      else st->coef[c] = s;
+    }
   }
   __syncthreads();
   __threadfence_block();
@@ -336,11 +340,14 @@ __global__ void norm2_kernel(const T* __restrict__ x, ll n, double* out, double*
   s = block_sum(s, red);
   if (threadIdx.x == 0) part[blockIdx.x] = s;
   if (!arrive_last(counter, gridDim.x)) return;
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < 32) {  // fixed order: lane l adds blocks l, l+32, ..., then a shuffle tree
     double t = 0.0;
-    for (int b = 0; b < (int)gridDim.x; ++b) t += part[b];
-    *out = t;
-    *counter = 0u;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += 32) t += part[b];
+    t = warp_sum(t);
+    if (threadIdx.x == 0) {
+      *out = t;
+      *counter = 0u;
+    }
   }
 }
 

@@ -30,6 +30,8 @@ struct EigWork {
   unsigned* counter = nullptr;
   SvdOut* out = nullptr;
   SvdOut* h_out = nullptr;
+  cudaStream_t side = nullptr;  // builds the compact-WY triangles while the eigenvectors are computed
+  cudaEvent_t ev_refl = nullptr, ev_wy = nullptr;
   int nmax = 0, Kmax = 0;
   size_t bytes = 0;
   std::vector<void*> owned;
@@ -61,12 +63,20 @@ struct EigWork {
     DMRG2_CUDA(cudaMemset(counter, 0, sizeof(unsigned) * 4));
     out = (SvdOut*)alloc(sizeof(SvdOut));
     DMRG2_CUDA(cudaMallocHost(&h_out, sizeof(SvdOut)));
+    DMRG2_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    DMRG2_CUDA(cudaEventCreateWithFlags(&ev_refl, cudaEventDisableTiming));
+    DMRG2_CUDA(cudaEventCreateWithFlags(&ev_wy, cudaEventDisableTiming));
   }
   void release() {
     for (void* p : owned) cudaFree(p);
     owned.clear();
     if (h_out) cudaFreeHost(h_out);
     h_out = nullptr;
+    if (side) cudaStreamDestroy(side);
+    if (ev_refl) cudaEventDestroy(ev_refl);
+    if (ev_wy) cudaEventDestroy(ev_wy);
+    side = nullptr;
+    ev_refl = ev_wy = nullptr;
   }
 };
 
@@ -102,6 +112,11 @@ SvdOut eig_split(EigWork<T>& W, const T* theta, int m, int nt, char dir, int chi
     launch_gemm(g, s);
   }
   hetrd_cluster<T>(W.G, n, n, W.d, W.e, W.tau, s);
+  // the back-transform's WY triangles need only the reflectors: build them on the side stream
+  DMRG2_CUDA(cudaEventRecord(W.ev_refl, s));
+  DMRG2_CUDA(cudaStreamWaitEvent(W.side, W.ev_refl, 0));
+  wy_build<T>(W.G, n, W.tau, n, K, W.Tb, W.side);
+  DMRG2_CUDA(cudaEventRecord(W.ev_wy, W.side));
   tridiag_eigvals(W.d, W.e, n, K, W.lam, s);
   eig_truncate(W.d, W.lam, n, K, chi, cutoff, relative, W.out, s);  // k decided before any vector
   tridiag_eigvecs(W.d, W.e, n, K, W.lam, W.out, W.Z, W.scr, s);
@@ -127,7 +142,8 @@ SvdOut eig_split(EigWork<T>& W, const T* theta, int m, int nt, char dir, int chi
     launch_gemm(g2, s);
     std::swap(W.Z, W.Z2);
   }
-  apply_q<T>(W.G, n, W.tau, n, W.Z, K, W.out, W.Zg, W.Tb, s);
+  DMRG2_CUDA(cudaStreamWaitEvent(s, W.ev_wy, 0));
+  apply_q<T>(W.G, n, W.tau, n, W.Z, K, W.out, W.Zg, W.Tb, s, true);
   DMRG2_CUDA(cudaMemcpyAsync(W.h_out, W.out, sizeof(SvdOut), cudaMemcpyDeviceToHost, s));
   DMRG2_CUDA(cudaStreamSynchronize(s));
   SvdOut o = *W.h_out;
