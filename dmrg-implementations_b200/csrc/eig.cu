@@ -17,7 +17,7 @@
 //      in shared memory (or L2). Either way the all-gather of p goes through
 //      distributed shared memory with one cluster barrier per column.
 //   2. tridiag_bisect: the K largest eigenvalues of T by Sturm-count
-//      multisection, one CTA per eigenvalue, 129 points per round.
+//      multisection, one CTA per eigenvalue, 64 points per round.
 //   3. tridiag_invit: eigenvectors of T by inverse iteration with partial
 //      pivoting, one thread per eigenvector, seeded random starts, factors and
 //      iterate in shared memory.
@@ -869,29 +869,61 @@ static bool hetrd_reg(double* G, int n, ll ld, double* d, double* e, double* tau
 // Number of eigenvalues of (d, e) below x: sign changes along the leading principal
 // minors P_0 = 1, P_1 = d_0 - x, P_{i+1} = (d_i - x) P_i - e_{i-1}^2 P_{i-1} (Sturm).
 // Compared with the ratio form q_i = P_i / P_{i-1} (LDL^T pivots) it needs no
-// division: one FMA per step on the dependent chain (e^2 P_{i-1} is formed a step
-// ahead), so a count costs a fraction of the ratio form's latency. Each step perturbs
-// d_i - x and e_{i-1}^2 by a few ulps relative, the same backward error as the ratio
-// form. The pair (P_{i-1}, P_i) is rescaled by an exact power of two every other step
-// to stay in range; an exact zero minor is replaced by -2^-60 P_{i-1}, the ratio
-// form's negative tiny pivot.
+// division. Each step perturbs d_i - x and e_{i-1}^2 by a few ulps relative, the
+// same backward error as the ratio form. The pair (P_{i-1}, P_i) is rescaled by an
+// exact power of two every four steps to stay in range; an exact zero minor is
+// replaced by -2^-60 P_{i-1}, the ratio form's negative tiny pivot. The steps run in
+// groups of 8 with the next group's shared loads issued ahead of the current group's
+// chain.
 __device__ inline int sturm_lt(const double* d, const double* e2, int n, double x) {
+  constexpr int G = 8;
   double a = 1.0, b = d[0] - x;
   if (b == 0.0) b = -0x1p-60;
   int c = (b < 0.0);
-  for (int i = 1; i < n; ++i) {
-    const double t = e2[i - 1] * a;
-    double nb = fma(d[i] - x, b, -t);
+  const int ng = (n - 1) / G;  // full groups cover steps 1 .. ng G
+  double dd[G], ee[G];
+  if (ng > 0) {
+#pragma unroll
+    for (int u = 0; u < G; ++u) {
+      dd[u] = d[1 + u];
+      ee[u] = e2[u];
+    }
+  }
+  for (int g = 0; g < ng; ++g) {
+    double dn[G], en[G];
+    const int base = 1 + (g + 1) * G;
+#pragma unroll
+    for (int u = 0; u < G; ++u) {  // next group (clamped reads past the end are not used)
+      const int i = min(base + u, n - 1);
+      dn[u] = d[i];
+      en[u] = e2[i - 1];
+    }
+#pragma unroll
+    for (int u = 0; u < G; ++u) {
+      double nb = fma(dd[u] - x, b, -ee[u] * a);
+      if (nb == 0.0) nb = -0x1p-60 * b;
+      c += ((nb < 0.0) != (b < 0.0));
+      a = b;
+      b = nb;
+      if (u == 3 || u == 7) {
+        const double m = fmax(fabs(a), fabs(b));
+        const double f = (m > 0x1p+256) ? 0x1p-256 : (m < 0x1p-256) ? 0x1p+256 : 1.0;
+        a *= f;
+        b *= f;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < G; ++u) {
+      dd[u] = dn[u];
+      ee[u] = en[u];
+    }
+  }
+  for (int i = 1 + ng * G; i < n; ++i) {
+    double nb = fma(d[i] - x, b, -e2[i - 1] * a);
     if (nb == 0.0) nb = -0x1p-60 * b;
     c += ((nb < 0.0) != (b < 0.0));
     a = b;
     b = nb;
-    if (i & 1) {
-      const double m = fmax(fabs(a), fabs(b));
-      const double f = (m > 0x1p+500) ? 0x1p-500 : (m < 0x1p-500) ? 0x1p+500 : 1.0;
-      a *= f;
-      b *= f;
-    }
   }
   return c;
 }
@@ -966,6 +998,19 @@ __global__ void __launch_bounds__(256)
 // 3. inverse iteration for the k kept eigenvalues: one thread per eigenvector,
 //    LU factors with partial pivoting and the iterate in shared memory, the
 //    recurrences carried in registers. Columns k..K-1 of Z are zeroed.
+//    A numerically degenerate cluster (neighbours within 8 eps |T|: SU(2)
+//    multiplets, exactly repeated singular values) splits T into nearly
+//    decoupled blocks; with its own eigenvalue as shift every member would
+//    converge to the block whose eigenvalue happens to lie nearest, i.e. to the
+//    same vector. Its members therefore share one shift placed 4 max(width,
+//    8 eps |T|) outside the cluster, on the side of the larger gap: every
+//    cluster direction is amplified alike (to 25%), the random starts give a
+//    well-conditioned basis of the cluster space that the group Gram-Schmidt
+//    orthonormalises, and a neighbour at distance gap is damped by
+//    (shift distance / gap)^2 over the two iterations. Where either gap is
+//    below 1e4 times the shift distance, or where the cluster is wider than the group
+//    tolerance (its members would not all share one Gram-Schmidt window), the
+//    members keep their own shifts.
 // ----------------------------------------------------------------------------
 __device__ inline double hash_unit(unsigned long long x) {
   x += 0x9E3779B97F4A7C15ull;
@@ -977,7 +1022,7 @@ __device__ inline double hash_unit(unsigned long long x) {
 
 __global__ void tridiag_invit_kernel(const double* __restrict__ dg, const double* __restrict__ eg,
                                      int n, int K, const double* __restrict__ lam,
-                                     const SvdOut* __restrict__ tr, double* __restrict__ Z) {
+                                     const SvdOut* __restrict__ tr, double* __restrict__ Z, double gtol_rel) {
   extern __shared__ double dsh[];
   __shared__ double tn_s;
   const int vpb = blockDim.x;  // one vector per thread
@@ -1005,7 +1050,25 @@ __global__ void tridiag_invit_kernel(const double* __restrict__ dg, const double
 #define SX(a, i) base[((ll)(a) * n + (i)) * vpb + t]
   // arrays: 0 = 1/u0, 1 = u1, 2 = u2, 3 = multiplier, 4 = swap flag, 5 = iterate
   const double tiny = fmax(tn_s, 1e-300) * 2.2e-16;
-  const double sft = lam[j];
+  double sft = lam[j];
+  {
+    const double tight = 8.0 * tiny;
+    int first = j, last = j;
+    while (first > 0 && lam[first - 1] - lam[first] <= tight) --first;
+    while (last + 1 < K && lam[last] - lam[last + 1] <= tight) ++last;
+    // the group Gram-Schmidt must see the whole cluster in every member's window: its
+    // width stays within the group tolerance
+    if (last > first && lam[first] - lam[last] <= gtol_rel * fabs(lam[0])) {
+      const double width = lam[first] - lam[last];
+      const double shift = 4.0 * fmax(width, tight);
+      // eigenvalues past the K computed ones are unknown: no gap below is taken as known
+      const double gap_up = (first > 0) ? lam[first - 1] - lam[first] : 1e300;
+      const double gap_dn = (last + 1 < K) ? lam[last] - lam[last + 1] : 0.0;
+      // only where both gaps keep a neighbour's share below 1e-8 after two iterations (the
+      // neighbour on the far side is damped only by shift / (gap + shift) per iteration)
+      if (fmin(gap_up, gap_dn) >= 1e4 * shift) sft = (gap_up >= gap_dn) ? lam[first] + shift : lam[last] - shift;
+    }
+  }
   double c0 = d[0] - sft, c1 = e[0];
   for (int i = 0; i < n - 1; ++i) {
     const double s = e[i];
@@ -1539,13 +1602,14 @@ void hetrd_cluster(T* G, int n, ll ld, double* d, double* e, T* tau, cudaStream_
 }
 
 void tridiag_eigvals(const double* d, const double* e, int n, int K, double* lam, cudaStream_t s) {
-  // 129 points per round (7 bits): about 8 rounds to full precision, half the Sturm counts of 257
-  tridiag_bisect_kernel<<<K, 128, sizeof(double) * 2 * n, s>>>(d, e, n, K, lam);
+  // 64 points per round (6 bits), about 9 rounds: the counts are issue-bound, and fewer points
+  // per round cost fewer counts in all
+  tridiag_bisect_kernel<<<K, 64, sizeof(double) * 2 * n, s>>>(d, e, n, K, lam);
   DMRG2_CHECK_LAUNCH();
 }
 
 void tridiag_eigvecs(const double* d, const double* e, int n, int K, const double* lam,
-                     const SvdOut* tr, double* Z, double* scratch, cudaStream_t s) {
+                     const SvdOut* tr, double* Z, double* scratch, double gtol_rel, cudaStream_t s) {
   (void)scratch;
   static std::atomic<unsigned long long> attr{0};
   set_smem_attr_once(attr, (const void*)tridiag_invit_kernel, 220 * 1024);
@@ -1553,7 +1617,7 @@ void tridiag_eigvecs(const double* d, const double* e, int n, int K, const doubl
   int vpb = (int)std::min<size_t>(8, (220 * 1024 - sizeof(double) * 2 * (size_t)n) / per);
   if (vpb < 1) throw std::runtime_error("inverse iteration: matrix order too large");
   const size_t smem = sizeof(double) * 2 * (size_t)n + per * vpb;
-  tridiag_invit_kernel<<<(K + vpb - 1) / vpb, vpb, smem, s>>>(d, e, n, K, lam, tr, Z);
+  tridiag_invit_kernel<<<(K + vpb - 1) / vpb, vpb, smem, s>>>(d, e, n, K, lam, tr, Z, gtol_rel);
   DMRG2_CHECK_LAUNCH();
 }
 

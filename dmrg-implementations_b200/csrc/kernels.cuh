@@ -91,8 +91,9 @@ void svd_gather(const T* X, const T* Q, const int* perm, int nvec, ll len, int k
 template <typename T>
 void hetrd_cluster(T* G, int n, ll ld, double* d, double* e, T* tau, cudaStream_t s);
 void tridiag_eigvals(const double* d, const double* e, int n, int K, double* lam, cudaStream_t s);
+// gtol_rel: the group tolerance (relative to lam[0]) that group_mgs will use on the result
 void tridiag_eigvecs(const double* d, const double* e, int n, int K, const double* lam,
-                     const SvdOut* tr, double* Z, double* scratch, cudaStream_t s);
+                     const SvdOut* tr, double* Z, double* scratch, double gtol_rel, cudaStream_t s);
 void group_mgs(double* Z, int n, int K, const double* lam, const SvdOut* tr, double gtol_rel,
                cudaStream_t s);
 // compact-WY triangles of the reflector blocks that apply_q uses for (n, K); apply_q builds

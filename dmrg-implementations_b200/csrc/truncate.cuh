@@ -119,8 +119,9 @@ SvdOut eig_split(EigWork<T>& W, const T* theta, int m, int nt, char dir, int chi
   DMRG2_CUDA(cudaEventRecord(W.ev_wy, W.side));
   tridiag_eigvals(W.d, W.e, n, K, W.lam, s);
   eig_truncate(W.d, W.lam, n, K, chi, cutoff, relative, W.out, s);  // k decided before any vector
-  tridiag_eigvecs(W.d, W.e, n, K, W.lam, W.out, W.Z, W.scr, s);
-  group_mgs(W.Z, n, K, W.lam, W.out, 1e-14, s);
+  constexpr double gtol_rel = 1e-14;  // groups: neighbours within 1e-14 lambda_max
+  tridiag_eigvecs(W.d, W.e, n, K, W.lam, W.out, W.Z, W.scr, gtol_rel, s);
+  group_mgs(W.Z, n, K, W.lam, W.out, gtol_rel, s);
   for (int it = 0; it < 3; ++it) {  // Newton-Schulz polar step: Z <- Z (3I - Z^T Z) / 2
     Gemm<double> g1;
     g1.ta = true;
