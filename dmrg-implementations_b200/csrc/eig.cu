@@ -13,9 +13,10 @@
 //      tridiagonal form (Golub & Van Loan, Alg. 8.3.1) by ONE thread-block
 //      cluster of up to 16 CTAs, rows distributed cyclically over the CTAs.
 //      Real G up to order 512 keeps the trailing matrix in registers and does
-//      each column in one fused pass (1b below); complex or larger G keeps it
-//      in shared memory (or L2). Either way the all-gather of p goes through
-//      distributed shared memory with one cluster barrier per column.
+//      each column in one register pass (1b, 1c below), exchanging p by bulk
+//      copies into the peers' shared memory; complex or larger G keeps it in
+//      shared memory (or L2) and pulls p through distributed shared memory
+//      after one cluster barrier per column.
 //   2. tridiag_bisect: the K largest eigenvalues of T by Sturm-count
 //      multisection, one CTA per eigenvalue, 64 points per round.
 //   3. tridiag_invit: eigenvectors of T by inverse iteration with partial
@@ -510,19 +511,24 @@ static cudaError_t hetrd_reg2_launch(double* G, int n, ll ld, double* d, double*
 }
 
 // ----------------------------------------------------------------------------
-// 1c. The register-resident reduction with a push exchange. Instead of a
-//     cluster barrier followed by remote loads, every owner stores (p'_r,
-//     column-(k+2)_r) for its rows and its warps' partials of s' straight into
-//     every other CTA's shared memory with st.async, which counts the bytes on
-//     the receiver's mbarrier (its own entries it stores locally); a CTA starts
-//     step k once its barrier has seen every peer's bytes of step k and its own
-//     threads have passed a CTA barrier. Two parity buffers (and barriers) carry
-//     consecutive steps. A buffer is rewritten two steps after it was read, and
-//     its writer can only get there after receiving the reader's next push,
-//     which the reader issues after its last read (the complete_tx of st.async
-//     is a release at cluster scope, the wait an acquire), so no further
-//     barrier is needed. Waits are bounded: a CTA that gives up marks the whole
-//     cluster failed and the result is poisoned (d[0] = NaN) instead of hanging.
+// 1c. The register-resident reduction with a push exchange and a split step.
+//     Exchange: instead of a cluster barrier followed by remote loads, every CTA
+//     writes one block per step into its own slot of its inbox, [(p'_r, column
+//     (k+2)_r) of its rows][its warps' partials of s'], and copies that block
+//     into the same slot of every peer's inbox with cp.async.bulk (shared::cta to
+//     shared::cluster, no multicast), which counts the bytes on the receiver's
+//     mbarrier; a CTA starts step k once its barrier has seen every peer's block
+//     of step k. Two parity inboxes (and barriers) carry consecutive steps. A
+//     slot is rewritten two steps after it was read, and its writer can only get
+//     there after receiving the reader's next block, which the reader sends after
+//     its last read (behind a CTA barrier; the copy's complete_tx releases at
+//     cluster scope, the wait acquires), so no further barrier is needed.
+//     Step: (a) one thread per column forms v_j, w_j and the next column x'_j
+//     (and the reflector row); after a CTA barrier (b) every warp derives the
+//     next reflector from the shared norm partials and (c) applies the rank-2
+//     update to its rows with the next symv in the same register pass.
+//     Waits are bounded: a CTA that gives up marks the whole cluster failed and
+//     the result is poisoned (d[0] = NaN) instead of hanging.
 // ----------------------------------------------------------------------------
 static constexpr int HP_SPIN = 1 << 20;  // polls of one barrier phase before giving up
 
@@ -533,14 +539,6 @@ __device__ inline uint32_t cluster_addr(uint32_t a, int cta) {
   uint32_t r;
   asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(cta));
   return r;
-}
-__device__ inline void push_v2(uint32_t dst, double a, double b, uint32_t bar) {
-  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f64 [%0], {%1, %2}, [%3];"
-               ::"r"(dst), "d"(a), "d"(b), "r"(bar) : "memory");
-}
-__device__ inline void push_f64(uint32_t dst, double a, uint32_t bar) {
-  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.f64 [%0], %1, [%2];"
-               ::"r"(dst), "d"(a), "r"(bar) : "memory");
 }
 __device__ inline void bar_expect(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
@@ -571,33 +569,47 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
   static_assert(NT % 2 == 0, "column slots come in pairs");
   cg::cluster_group cluster = cg::this_cluster();
   constexpr int NW = HT_THREADS / 32;
+  constexpr int lgC = (C >= 32) ? 5 : (C >= 16) ? 4 : (C >= 8) ? 3 : (C >= 4) ? 2 : (C >= 2) ? 1 : 0;
   constexpr int NP = NT / 2;
   const int rank = (int)cluster.block_rank();
   extern __shared__ __align__(16) double hsm[];
   __shared__ __align__(8) unsigned long long bars[2];
   __shared__ int fail_s;
   const int n2 = (n + 1) & ~1;
-  double* pc0 = hsm;            // (p_r, c_r) pairs of step parity 0, natural row order (pushed)
-  double* pc1 = pc0 + 2 * n2;   // parity 1
-  double* xs0 = pc1 + 2 * n2;   // column k (parity buffers, computed locally)
+  // inbox of a step: one block per CTA, [Q (p, c) pairs of its rows by local index][NW partials
+  // of s]; a CTA writes its own block and bulk-copies it into the same slot of every peer
+  constexpr int Q = RW * NW;
+  constexpr int BLK = 2 * Q + NW;  // doubles; a multiple of 2 (16-byte blocks)
+  double* ib0 = hsm;               // inbox, step parity 0
+  double* ib1 = ib0 + C * BLK;     // parity 1
+  double* xs0 = ib1 + C * BLK;     // column k (parity buffers, computed locally)
   double* xs1 = xs0 + n2;
-  double* sa0 = xs1 + n2;       // C * NW partials of s (pushed), parity 0
-  double* sa1 = sa0 + C * NW;
+  double* vv = xs1 + n2;           // v of this step by column (0 outside the active block)
+  double* ww = vv + n2;            // w of this step by column
+  double* xa = ww + n2;            // next column where it enters the next symv (j >= k+3), else 0
+  __shared__ double nrmw[NW], anext_s, dnext_s;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   auto col = [&](int t) { return 2 * lane + 64 * (t >> 1) + (t & 1); };
-  const bool g_pairs = ((ld & 1) == 0) && ((reinterpret_cast<uintptr_t>(G) & 15) == 0);
   const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
-  // bytes pushed by the peers per step: their rows' (p, c) pairs and their warps' partials
-  auto step_bytes = [&]() { return (uint32_t)(16 * (n - (n - rank + C - 1) / C) + 8 * (C - 1) * NW); };
-  // lane d < C, d != rank, pushes to CTA d; lane rank stores into this CTA's buffers
-  // (mapa keeps offsets, so one base address per window: buffers are at fixed offsets
-  // from pc0, the second barrier 8 bytes after the first)
-  uint32_t d_base = 0, d_bar0 = 0;
-  if (lane < C) {
-    d_base = cluster_addr(smem_u32(pc0), lane);
-    d_bar0 = cluster_addr(bar0, lane);
+  // bytes the peers copy in per step: one block each
+  auto step_bytes = [&]() { return (uint32_t)(8 * BLK * (C - 1)); };
+  // thread d < C, d != rank, copies this CTA's block to CTA d
+  uint32_t d_ib0 = 0, d_bar0 = 0;
+  if (tid < C) {
+    d_ib0 = cluster_addr(smem_u32(ib0 + rank * BLK), tid);
+    d_bar0 = cluster_addr(bar0, tid);
   }
-  const uint32_t o_pc1 = 16u * (uint32_t)n2, o_sa0 = 48u * (uint32_t)n2, o_sa1 = o_sa0 + 8u * C * NW;
+  const uint32_t o_ib1 = 8u * C * BLK;  // bytes from ib0 to ib1
+  auto send_block = [&](int parity) {   // after a CTA barrier that follows the block's writes
+    if (tid < C && tid != rank) {
+      const uint32_t src = smem_u32((parity ? ib1 : ib0) + rank * BLK);
+      asm volatile(
+          "cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+              d_ib0 + (parity ? o_ib1 : 0u)),
+          "r"(src), "r"(8u * BLK), "r"(d_bar0 + (parity ? 8u : 0u))
+          : "memory");
+    }
+  };
   volatile int* failv = &fail_s;
   auto give_up = [&]() {
     if (!*failv)
@@ -660,95 +672,101 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
           p = tk * (c1 + sc * acc);
           sp += p * ((r == 1) ? 1.0 : xs0[r] * sc);
         }
-        if (lane == rank) *reinterpret_cast<double2*>(pc0 + 2 * r) = make_double2(p, c1);
-        else if (lane < C) push_v2(d_base + 16u * (uint32_t)r, p, c1, d_bar0);
+        if (lane == 0) *reinterpret_cast<double2*>(ib0 + rank * BLK + 2 * (r >> lgC)) = make_double2(p, c1);
       }
     }
-    if (lane == rank) sa0[rank * NW + warp] = sp;
-    else if (lane < C) push_f64(d_base + o_sa0 + 8u * (uint32_t)(rank * NW + warp), sp, d_bar0);
+    if (lane == 0) ib0[rank * BLK + 2 * Q + warp] = sp;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    send_block(0);
   }
 
   for (int k = 0; k < n - 1; ++k) {
     const int par = k & 1;
-    const double* pc = par ? pc1 : pc0;
-    const double* sa = par ? sa1 : sa0;
+    const double* ib = par ? ib1 : ib0;
+    double* ibn = par ? ib0 : ib1;
     const double* xs = par ? xs1 : xs0;
     double* xsn = par ? xs0 : xs1;
-    double* pcn = par ? pc0 : pc1;
-    double* san = par ? sa0 : sa1;
     const uint32_t bar = par ? bar1 : bar0;
-    const uint32_t n_pc = d_base + (par ? 0u : o_pc1), n_sa = d_base + (par ? o_sa0 : o_sa1);
-    const uint32_t n_bar = d_bar0 + (par ? 0u : 8u);
+    auto pval = [&](int j) { return ib[(j & (C - 1)) * BLK + 2 * (j >> lgC)]; };
+    auto cval = [&](int j) { return ib[(j & (C - 1)) * BLK + 2 * (j >> lgC) + 1]; };
     // (1) every CTA's pushes of step k have landed
     if (!bar_wait(bar, (uint32_t)((k >> 1) & 1), failv)) give_up();
     if (tid == 0 && k + 2 <= n - 2 && !*failv) bar_expect(bar, step_bytes());  // re-arm for step k+2
     __syncthreads();  // this CTA's own entries and column k (written last step) visible to all
     double ssum = 0.0;
-    for (int q = lane; q < C * NW; q += 32) ssum += sa[q];
+    for (int q = lane; q < C * NW; q += 32) ssum += ib[(q / NW) * BLK + 2 * Q + (q % NW)];
     ssum = warp_sum_d(ssum);
-    // (2) w = p - tau s / 2 v; fused rank-2 update + next symv + next column
+    // (2a) one column per thread: v, w and the next column x' = column k+1 after the
+    //      rank-2 update, its norm partial and the reflector row (rank 0)
     const double a2 = -0.5 * tk * ssum;
-    const double wk1 = pc[2 * (k + 1)] + a2;  // v[k+1] = 1
+    const double wk1 = pval(k + 1) + a2;  // v[k+1] = 1
+    {
+      double nr = 0.0;
+      for (int j = tid; j < n; j += HT_THREADS) {
+        double vj = 0.0, wj = 0.0, xj = 0.0;
+        if (j >= k + 1) {
+          vj = (j == k + 1) ? 1.0 : xs[j] * sc;
+          wj = pval(j) + a2 * vj;
+          const double xn = cval(j) - vj * wk1 - wj;
+          xsn[j] = xn;
+          if (j >= k + 3) {
+            xj = xn;
+            nr += xn * xn;
+          }
+          if (j == k + 2) anext_s = xn;
+          if (j == k + 1) dnext_s = xn;
+          if (rank == 0) G[(ll)k * ld + j] = vj;
+        }
+        vv[j] = vj;
+        ww[j] = wj;
+        xa[j] = xj;
+      }
+      nr = warp_sum_d(nr);
+      if (lane == 0) nrmw[warp] = nr;
+    }
+    __syncthreads();  // v, w, x' and the norm partials visible to every warp
+    // (3a) next reflector (every warp derives the same one, in a fixed order)
+    double nrm = (lane < NW) ? nrmw[lane] : 0.0;
+    nrm = warp_sum_d(nrm);
+    const double a_next = anext_s, d_next = dnext_s;
+    double tk2 = 0.0, sc2 = 0.0, beta2 = 0.0;
+    if (k + 2 <= n - 1) house_real1(a_next, nrm, tk2, sc2, beta2);
+    if (rank == 0 && tid == 32) {
+      dg[k + 1] = d_next;
+      eg[k + 1] = beta2;
+      if (k + 1 < n - 1) tau[k + 1] = tk2;
+    }
+    // (2b) rank-2 update of this warp's rows and the next symv sum_j G'[r][j] x'[j]
     double vr[RW], wr[RW], acc[RW], c2[RW];
     bool act[RW];
 #pragma unroll
     for (int i = 0; i < RW; ++i) {
       const int r = rr[i];
-      vr[i] = 0.0;
-      wr[i] = 0.0;
       act[i] = (r >= k + 1 && r < n);
-      if (act[i]) {
-        vr[i] = (r == k + 1) ? 1.0 : xs[r] * sc;
-        wr[i] = pc[2 * r] + a2 * vr[i];
-      }
+      vr[i] = act[i] ? vv[r] : 0.0;
+      wr[i] = act[i] ? ww[r] : 0.0;
       acc[i] = 0.0;
       c2[i] = 0.0;
     }
-    double nrm = 0.0, a_next = 0.0, d_next = 0.0;
-    const bool store_v = (rank == 0);
-    auto one = [&](const int t, const int j, const double xv, const double pv, const double cv, const bool edge) {
-      const double vj = (edge && j == k + 1) ? 1.0 : xv * sc;
-      const double wj = pv + a2 * vj;
-      const double xn = cv - vj * wk1 - wj;
-      if (!edge || j >= k + 3) nrm += xn * xn;
-      if (edge && j == k + 2) a_next = xn;
-      if (edge && j == k + 1) d_next = xn;
-#pragma unroll
-      for (int i = 0; i < RW; ++i) {
-        if (act[i]) {
-          const double gg = g[i][t] - vr[i] * wj - wr[i] * vj;
-          g[i][t] = gg;
-          if (!edge || j >= k + 3) acc[i] += gg * xn;
-          if (edge && j == k + 2) c2[i] = gg;
-        }
-      }
-      return xn;
-    };
 #pragma unroll
     for (int u = 0; u < NP; ++u) {
       const int base = 64 * u;
       if (base + 64 <= k + 1 || base >= n) continue;
       const int j0 = base + 2 * lane;
-      const bool mine = (u % NW) == warp;
       if (base >= k + 3 && base + 64 <= n) {
-        const double2 xv = *reinterpret_cast<const double2*>(xs + j0);
-        const double2 q0 = *reinterpret_cast<const double2*>(pc + 2 * j0);      // (p, c) of j0
-        const double2 q1 = *reinterpret_cast<const double2*>(pc + 2 * j0 + 2);  // (p, c) of j0 + 1
-        double2 xo;
-        xo.x = one(2 * u, j0, xv.x, q0.x, q0.y, false);
-        xo.y = one(2 * u + 1, j0 + 1, xv.y, q1.x, q1.y, false);
-        if (mine) {
-          *reinterpret_cast<double2*>(xsn + j0) = xo;
-          if (store_v) {
-            if (g_pairs) {
-              double2 vv;
-              vv.x = xv.x * sc;
-              vv.y = xv.y * sc;
-              *reinterpret_cast<double2*>(G + (ll)k * ld + j0) = vv;
-            } else {
-              G[(ll)k * ld + j0] = xv.x * sc;
-              G[(ll)k * ld + j0 + 1] = xv.y * sc;
-            }
+        const double2 v2 = *reinterpret_cast<const double2*>(vv + j0);
+        const double2 w2 = *reinterpret_cast<const double2*>(ww + j0);
+        const double2 x2 = *reinterpret_cast<const double2*>(xa + j0);
+#pragma unroll
+        for (int i = 0; i < RW; ++i) {
+          if (act[i]) {
+            const double g0 = g[i][2 * u] - vr[i] * w2.x - wr[i] * v2.x;
+            const double g1 = g[i][2 * u + 1] - vr[i] * w2.y - wr[i] * v2.y;
+            g[i][2 * u] = g0;
+            g[i][2 * u + 1] = g1;
+            acc[i] += g0 * x2.x;
+            acc[i] += g1 * x2.y;
           }
         }
       } else {
@@ -756,25 +774,19 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
         for (int h = 0; h < 2; ++h) {
           const int j = j0 + h;
           if (j >= k + 1 && j < n) {
-            const double xn = one(2 * u + h, j, xs[j], pc[2 * j], pc[2 * j + 1], true);
-            if (mine) {
-              xsn[j] = xn;
-              if (store_v) G[(ll)k * ld + j] = (j == k + 1) ? 1.0 : xs[j] * sc;
+            const double vj = vv[j], wj = ww[j], xj = xa[j];
+#pragma unroll
+            for (int i = 0; i < RW; ++i) {
+              if (act[i]) {
+                const double gg = g[i][2 * u + h] - vr[i] * wj - wr[i] * vj;
+                g[i][2 * u + h] = gg;
+                acc[i] += gg * xj;
+                if (j == k + 2) c2[i] = gg;
+              }
             }
           }
         }
       }
-    }
-    // (3) next reflector (every warp derives the same one); push p', column k+2, s'
-    nrm = warp_sum_d(nrm);
-    a_next = __shfl_sync(0xffffffffu, a_next, ((k + 2) & 63) >> 1);
-    d_next = __shfl_sync(0xffffffffu, d_next, ((k + 1) & 63) >> 1);
-    double tk2 = 0.0, sc2 = 0.0, beta2 = 0.0;
-    if (k + 2 <= n - 1) house_real1(a_next, nrm, tk2, sc2, beta2);
-    if (rank == 0 && tid == 32) {
-      dg[k + 1] = d_next;
-      eg[k + 1] = beta2;
-      if (k + 1 < n - 1) tau[k + 1] = tk2;
     }
     const bool push = (k + 1 <= n - 2);  // step k+1 exists
     double sp = 0.0;
@@ -787,18 +799,16 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
         double p = 0.0;
         if (r >= k + 2) {
           p = tk2 * (c + sc2 * a);
-          const double xnr = pc[2 * r + 1] - vr[i] * wk1 - wr[i];
-          sp += p * ((r == k + 2) ? 1.0 : xnr * sc2);
+          sp += p * ((r == k + 2) ? 1.0 : xsn[r] * sc2);
         }
-        if (push) {
-          if (lane == rank) *reinterpret_cast<double2*>(pcn + 2 * r) = make_double2(p, c);
-          else if (lane < C) push_v2(n_pc + 16u * (uint32_t)r, p, c, n_bar);
-        }
+        if (push && lane == 0) *reinterpret_cast<double2*>(ibn + rank * BLK + 2 * (warp + NW * i)) = make_double2(p, c);
       }
     }
     if (push) {
-      if (lane == rank) san[rank * NW + warp] = sp;
-      else if (lane < C) push_f64(n_sa + 8u * (uint32_t)(rank * NW + warp), sp, n_bar);
+      if (lane == 0) ibn[rank * BLK + 2 * Q + warp] = sp;
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncthreads();  // the block is complete
+      send_block(par ^ 1);
     }
     tk = tk2;
     sc = sc2;
@@ -809,7 +819,7 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
 
 template <int NT, int RW, int C>
 static cudaError_t hetrd_push_launch(double* G, int n, ll ld, double* d, double* e, double* tau,
-                                     cudaStream_t s) {
+                                      cudaStream_t s) {
   static std::atomic<unsigned long long> attr_cluster{0};
   func_attr_once(attr_cluster, (const void*)hetrd_push_kernel<NT, RW, C>,
                  cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
@@ -817,7 +827,8 @@ static cudaError_t hetrd_push_launch(double* G, int n, ll ld, double* d, double*
   cfg.gridDim = dim3(C);
   cfg.blockDim = dim3(HT_THREADS);
   const size_t n2 = (size_t)((n + 1) & ~1);
-  cfg.dynamicSmemBytes = sizeof(double) * (6 * n2 + 2 * (size_t)C * (HT_THREADS / 32));
+  constexpr size_t NW = HT_THREADS / 32, BLK = 2 * RW * NW + NW;
+  cfg.dynamicSmemBytes = sizeof(double) * (5 * n2 + 2 * (size_t)C * BLK);
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
