@@ -122,6 +122,14 @@ SvdOut eig_split(EigWork<T>& W, const T* theta, int m, int nt, char dir, int chi
   constexpr double gtol_rel = 1e-14;  // groups: neighbours within 1e-14 lambda_max
   tridiag_eigvecs(W.d, W.e, n, K, W.lam, W.out, W.Z, W.scr, gtol_rel, s);
   group_mgs(W.Z, n, K, W.lam, W.out, gtol_rel, s);
+  // Newton-Schulz GEMMs have K x K (or n x K) outputs, a few 64 x 64 tiles at chi = 256:
+  // split their long dimension over CTAs, partials in the (otherwise idle) scratch area
+  const size_t scr_len = (size_t)5 * W.nmax * W.Kmax;
+  auto split_for = [&](int M, int N, int Kd) {
+    int sk = std::min(8, std::max(1, Kd / 64));
+    while (sk > 1 && (size_t)sk * M * N > scr_len) --sk;
+    return sk;
+  };
   for (int it = 0; it < 3; ++it) {  // Newton-Schulz polar step: Z <- Z (3I - Z^T Z) / 2
     Gemm<double> g1;
     g1.ta = true;
@@ -130,6 +138,8 @@ SvdOut eig_split(EigWork<T>& W, const T* theta, int m, int nt, char dir, int chi
     g1.B = W.Z; g1.ldb = K;
     g1.C = W.S; g1.ldc = K;
     g1.skip = &W.out->ns_done;
+    g1.splitk = split_for(K, K, n);
+    g1.ws = W.scr;
     launch_gemm(g1, s);
     ns_check(W.S, K, W.out, 4e-16 * (double)n, W.part, W.counter, s);
     DMRG2_CUDA(cudaMemcpyAsync(W.Z2, W.Z, sizeof(double) * (size_t)n * K, cudaMemcpyDeviceToDevice, s));
@@ -140,6 +150,8 @@ SvdOut eig_split(EigWork<T>& W, const T* theta, int m, int nt, char dir, int chi
     g2.C = W.Z2; g2.ldc = K;
     g2.alpha = -0.5; g2.beta = 1.5;
     g2.skip = &W.out->ns_done;
+    g2.splitk = split_for(n, K, K);
+    g2.ws = W.scr;
     launch_gemm(g2, s);
     std::swap(W.Z, W.Z2);
   }
