@@ -130,7 +130,10 @@ SvdOut eig_split(EigWork<T>& W, const T* theta, int m, int nt, char dir, int chi
     while (sk > 1 && (size_t)sk * M * N > scr_len) --sk;
     return sk;
   };
-  for (int it = 0; it < 3; ++it) {  // Newton-Schulz polar step: Z <- Z (3I - Z^T Z) / 2
+  // Newton-Schulz polar step Z <- Z (3I - Z^T Z) / 2; an orthogonality error e becomes
+  // ~1.5 e^2 per iteration, and iterations after convergence only launch kernels that
+  // return at once
+  auto ns_iteration = [&]() {
     Gemm<double> g1;
     g1.ta = true;
     g1.M = K; g1.N = K; g1.K = n;
@@ -154,7 +157,8 @@ SvdOut eig_split(EigWork<T>& W, const T* theta, int m, int nt, char dir, int chi
     g2.ws = W.scr;
     launch_gemm(g2, s);
     std::swap(W.Z, W.Z2);
-  }
+  };
+  for (int it = 0; it < 3; ++it) ns_iteration();
   DMRG2_CUDA(cudaStreamWaitEvent(s, W.ev_wy, 0));
   apply_q<T>(W.G, n, W.tau, n, W.Z, K, W.out, W.Zg, W.Tb, s, true);
   DMRG2_CUDA(cudaMemcpyAsync(W.h_out, W.out, sizeof(SvdOut), cudaMemcpyDeviceToHost, s));
@@ -162,6 +166,13 @@ SvdOut eig_split(EigWork<T>& W, const T* theta, int m, int nt, char dir, int chi
   SvdOut o = *W.h_out;
   if (!std::isfinite(o.fro2))
     throw std::runtime_error("eigensolver: non-finite density matrix or tridiagonal reduction");
+  if (!o.ns_done) {
+    // not orthonormal after three iterations: close tail eigenvalues just outside one
+    // Gram-Schmidt window can leave overlaps near 0.15, which two more iterations bring
+    // below 1e-13; then the back-transform again (its WY triangles are still valid)
+    for (int it = 0; it < 2; ++it) ns_iteration();
+    apply_q<T>(W.G, n, W.tau, n, W.Z, K, W.out, W.Zg, W.Tb, s, true);
+  }
   const int k = o.k;
   if (R) {
     copy_cols_conj<T>(W.Zg, K, m, k, left, s);  // U = conj(eigvecs of conj(G))
