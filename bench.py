@@ -345,7 +345,10 @@ def run_ours(args):
         "max_bond": max(dims),
         "e2e": {"value": replica_throughput(len(e2e_reports), world, e2e_max), "unit": "sweeps/s",
                 "h2d_bytes_per_step": h2d // len(e2e_reports), "d2h_bytes_per_step": d2h // len(e2e_reports),
-                "energy": e2e_energy, "phases_s": e2e_phases,
+                "energy": e2e_energy,
+                # the same sweeps from the same state: the two legs must agree to rounding
+                "rel_dE_vs_device_leg": abs(e2e_energy - energy) / max(abs(energy), 1e-300),
+                "phases_s": e2e_phases,
                 "what": f"{len(e2e_reports)} sweeps at chi={CHI} through dmrg2_create/set_mpo/set_mps/run/get_mps "
                         f"from the host MPS left by the warm-up, host wall clock incl. H2D, environment build, D2H"},
         "roofline": {"kernel": "H_eff contraction (FP64 DMMA GEMMs)", "bound": "tensor",
