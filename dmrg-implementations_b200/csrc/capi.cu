@@ -45,6 +45,9 @@ int guarded(dmrg2_handle* h, F&& f) {
     (h ? h->err : g_err) = e.what();
     (void)cudaGetLastError();  // clear a non-sticky error so the next call starts clean
     return DMRG2_ERR_CUDA;
+  } catch (const NumericError& e) {
+    (h ? h->err : g_err) = e.what();
+    return DMRG2_ERR_NUMERIC;
   } catch (const std::invalid_argument& e) {
     (h ? h->err : g_err) = e.what();
     return DMRG2_ERR_ARG;

@@ -64,6 +64,11 @@ struct CudaError : public std::runtime_error {
   explicit CudaError(const std::string& s) : std::runtime_error(s) {}
 };
 
+// A numerical method did not reach its accuracy (reported as DMRG2_ERR_NUMERIC).
+struct NumericError : public std::runtime_error {
+  explicit NumericError(const std::string& s) : std::runtime_error(s) {}
+};
+
 #define DMRG2_CUDA(call)                                                              \
   do {                                                                                \
     cudaError_t e_ = (call);                                                          \
@@ -84,6 +89,13 @@ std::atomic<long long>& launch_counter();  // kernels launched by this library (
   } while (0)
 
 inline int ceil_div(ll a, ll b) { return (int)((a + b - 1) / b); }
+
+// Test hook for the bounded device waits: with DMRG2_TEST_UNSIGNALLED_WAITS=1 in the
+// environment, the kernels that wait on a completion (the tensor-core commit of the
+// split GEMM, the grid barrier of the cooperative Jacobi SVD) wait on one that nothing
+// signals, with a short poll limit, so a test can see the timeout reported as
+// DMRG2_ERR_NUMERIC while the device stays usable.
+bool test_unsignalled_waits();
 
 // cudaFuncSetAttribute acts on the current device only; `done` records, one bit
 // per device ordinal (mod 64), where the attribute was already set.

@@ -240,20 +240,16 @@ __global__ void __launch_bounds__(HT_THREADS)
 }
 
 // ----------------------------------------------------------------------------
-// 1b. Real symmetric G of order n <= 512: the same reduction with the trailing
-//     matrix held in registers. Row r belongs to CTA r % C (local row q = r / C)
-//     and, inside it, to warp q % 16 (slot q / 16 < RW); lane l holds the
-//     column pairs j = 2l + 64u + {0, 1} (NT columns), so the fused pass reads
-//     its vectors with 16-byte shared loads. Column k's step is one fused pass
-//     per warp: with p
-//     and column k+1 pulled from the owners, each warp forms v, w and the next
-//     column x' = column k+1 - (v w^T + w v^T)[:, k+1] for its lane's columns,
-//     applies the rank-2 update to its rows and, in the same pass, accumulates
-//     the next step's symv sum_j G'[r][j] x'[j] (the reflector of x' only
-//     scales it, and every warp derives that reflector itself from x'). Per
-//     column: one CTA barrier after the pull and one cluster barrier after the
-//     owners publish p', column k+2 and the partial sums of s' = p'^T v'. The
-//     reflector scalars cost one division.
+// 1b. Real symmetric G of order n <= 512 with the trailing matrix held in
+//     registers. Row r belongs to CTA r % C (local row q = r / C) and, inside
+//     it, to warp q % 16 (slot q / 16 < RW); lane l holds the column pairs
+//     j = 2l + 64u + {0, 1} (NT columns), so the fused pass reads its vectors
+//     with 16-byte shared loads. Each warp forms v, w and the next column
+//     x' = column k+1 - (v w^T + w v^T)[:, k+1], applies the rank-2 update to its
+//     rows and, in the same pass, accumulates the next step's symv
+//     sum_j G'[r][j] x'[j] (the reflector of x' only scales it, and every warp
+//     derives that reflector itself from x'). The reflector scalars cost one
+//     division (house_real1).
 // ----------------------------------------------------------------------------
 __device__ inline void house_real1(double alpha, double xn2, double& tk, double& sc, double& beta) {
   if (xn2 == 0.0) {
@@ -267,247 +263,6 @@ __device__ inline void house_real1(double alpha, double xn2, double& tk, double&
   const double r = 1.0 / (beta * dr);
   tk = -dr * dr * r;  // (beta - alpha) / beta
   sc = beta * r;      // 1 / (alpha - beta)
-}
-
-template <int NT, int RW, int C>
-__global__ void __launch_bounds__(HT_THREADS, 1)
-    hetrd_reg2_kernel(double* __restrict__ G, int n, ll ld, double* __restrict__ dg,
-                      double* __restrict__ eg, double* __restrict__ tau) {
-  static_assert((C & (C - 1)) == 0 && C <= 32, "cluster size: power of two <= 32");
-  static_assert(NT % 2 == 0, "column slots come in pairs");
-  cg::cluster_group cluster = cg::this_cluster();
-  constexpr int lgC = (C >= 32) ? 5 : (C >= 16) ? 4 : (C >= 8) ? 3 : (C >= 4) ? 2 : (C >= 2) ? 1 : 0;
-  constexpr int NW = HT_THREADS / 32;
-  constexpr int NP = NT / 2;  // column pairs per lane
-  const int rank = (int)cluster.block_rank();
-  extern __shared__ __align__(16) double hsm[];
-  const int Q = (n + C - 1) >> lgC;  // rows per CTA
-  const int n2 = (n + 1) & ~1;       // even array strides keep every array 16-byte aligned
-  const int Q2 = (Q + 1) & ~1;
-  double* pf = hsm;        // p of this step, natural order (pulled)
-  double* cf = pf + n2;    // column k+1 before this step (pulled)
-  double* xs0 = cf + n2;   // column k (parity buffers)
-  double* xs1 = xs0 + n2;
-  double* po0 = xs1 + n2;  // own p entries by local row (parity buffers)
-  double* po1 = po0 + Q2;
-  double* co0 = po1 + Q2;  // own column entries (parity buffers)
-  double* co1 = co0 + Q2;
-  double* sp0 = co1 + Q2;  // per-warp partial s (parity buffers)
-  double* sp1 = sp0 + NW;
-  double* sall = sp1 + NW;  // all C * NW partials of s, pulled
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  auto col = [&](int t) { return 2 * lane + 64 * (t >> 1) + (t & 1); };
-  // 16-byte stores into row k of G only when every row start is 16-byte aligned
-  const bool g_pairs = ((ld & 1) == 0) && ((reinterpret_cast<uintptr_t>(G) & 15) == 0);
-
-  int rr[RW];
-  double g[RW][NT];
-#pragma unroll
-  for (int i = 0; i < RW; ++i) {
-    rr[i] = (warp + NW * i) * C + rank;
-#pragma unroll
-    for (int t = 0; t < NT; ++t) {
-      const int j = col(t);
-      g[i][t] = (rr[i] < n && j < n) ? G[(ll)rr[i] * ld + j] : 0.0;
-    }
-  }
-  // ---- prologue: column 0 (row 0 by symmetry), its reflector, the first symv
-  for (int j = tid; j < n; j += HT_THREADS) xs0[j] = G[j];
-  __syncthreads();
-  double tk, sc, beta;
-  {
-    double xn2 = 0.0;
-    for (int j = 2 + lane; j < n; j += 32) xn2 += xs0[j] * xs0[j];
-    xn2 = warp_sum_d(xn2);
-    house_real1(xs0[1], xn2, tk, sc, beta);
-    if (rank == 0 && tid == 0) {
-      dg[0] = xs0[0];
-      eg[0] = beta;
-      tau[0] = tk;
-    }
-    double sp = 0.0;
-#pragma unroll
-    for (int i = 0; i < RW; ++i) {
-      const int r = rr[i];
-      double acc = 0.0;
-#pragma unroll
-      for (int t = 0; t < NT; ++t) {
-        const int j = col(t);
-        if (j >= 2 && j < n) acc += g[i][t] * xs0[j];
-      }
-      acc = warp_sum_d(acc);
-      const double c1 = __shfl_sync(0xffffffffu, g[i][1], 0);  // column 1 sits in lane 0, slot 1
-      if (r >= 1 && r < n) {
-        const double p = tk * (c1 + sc * acc);
-        if (lane == 0) {
-          po0[r >> lgC] = p;
-          co0[r >> lgC] = c1;
-        }
-        sp += p * ((r == 1) ? 1.0 : xs0[r] * sc);
-      }
-    }
-    if (lane == 0) sp0[warp] = sp;
-  }
-  cluster.sync();  // all rows loaded (rank 0 overwrites row k from step k on), step-0 data published
-
-  for (int k = 0; k < n - 1; ++k) {
-    const int par = k & 1;
-    const double* po = par ? po1 : po0;
-    const double* co = par ? co1 : co0;
-    const double* spr = par ? sp1 : sp0;
-    const double* xs = par ? xs1 : xs0;
-    double* pon = par ? po0 : po1;
-    double* con = par ? co0 : co1;
-    double* spn = par ? sp0 : sp1;
-    double* xsn = par ? xs0 : xs1;
-    // (1) pull p and column k+1 (a warp reads consecutive entries of one owner) and
-    //     every partial of s
-    {
-      const int c = tid / Q, q = tid - c * Q;
-      const int r = (q << lgC) + c;
-      if (c < C && r >= k + 1 && r < n) {
-        pf[r] = cluster.map_shared_rank(po, c)[q];
-        cf[r] = cluster.map_shared_rank(co, c)[q];
-      }
-    }
-    if (tid < C * NW) sall[tid] = cluster.map_shared_rank(spr, tid / NW)[tid % NW];
-    __syncthreads();
-    double ssum = 0.0;
-    for (int q = lane; q < C * NW; q += 32) ssum += sall[q];
-    ssum = warp_sum_d(ssum);
-    // (2) w = p - tau s / 2 v; fused rank-2 update + next symv + next column
-    const double a2 = -0.5 * tk * ssum;
-    const double wk1 = pf[k + 1] + a2;  // v[k+1] = 1
-    double vr[RW], wr[RW], acc[RW], c2[RW];
-    bool act[RW];
-#pragma unroll
-    for (int i = 0; i < RW; ++i) {
-      const int r = rr[i];
-      vr[i] = 0.0;
-      wr[i] = 0.0;
-      act[i] = (r >= k + 1 && r < n);
-      if (act[i]) {
-        vr[i] = (r == k + 1) ? 1.0 : xs[r] * sc;
-        wr[i] = pf[r] + a2 * vr[i];
-      }
-      acc[i] = 0.0;
-      c2[i] = 0.0;
-    }
-    double nrm = 0.0, a_next = 0.0, d_next = 0.0;
-    const bool store_v = (rank == 0);
-    auto one = [&](const int t, const int j, const double xv, const double pv, const double cv, const bool edge) {
-      const double vj = (edge && j == k + 1) ? 1.0 : xv * sc;
-      const double wj = pv + a2 * vj;
-      const double xn = cv - vj * wk1 - wj;
-      if (!edge || j >= k + 3) nrm += xn * xn;
-      if (edge && j == k + 2) a_next = xn;
-      if (edge && j == k + 1) d_next = xn;
-#pragma unroll
-      for (int i = 0; i < RW; ++i) {
-        if (act[i]) {
-          const double gg = g[i][t] - vr[i] * wj - wr[i] * vj;
-          g[i][t] = gg;
-          if (!edge || j >= k + 3) acc[i] += gg * xn;
-          if (edge && j == k + 2) c2[i] = gg;
-        }
-      }
-      return xn;
-    };
-#pragma unroll
-    for (int u = 0; u < NP; ++u) {
-      const int base = 64 * u;
-      if (base + 64 <= k + 1 || base >= n) continue;  // chunk left of the active block or past n
-      const int j0 = base + 2 * lane;
-      const bool mine = (u % NW) == warp;  // this warp publishes x' and the reflector of chunk u
-      if (base >= k + 3 && base + 64 <= n) {
-        const double2 xv = *reinterpret_cast<const double2*>(xs + j0);
-        const double2 pv = *reinterpret_cast<const double2*>(pf + j0);
-        const double2 cv = *reinterpret_cast<const double2*>(cf + j0);
-        double2 xo;
-        xo.x = one(2 * u, j0, xv.x, pv.x, cv.x, false);
-        xo.y = one(2 * u + 1, j0 + 1, xv.y, pv.y, cv.y, false);
-        if (mine) {
-          *reinterpret_cast<double2*>(xsn + j0) = xo;
-          if (store_v) {
-            if (g_pairs) {
-              double2 vv;
-              vv.x = xv.x * sc;
-              vv.y = xv.y * sc;
-              *reinterpret_cast<double2*>(G + (ll)k * ld + j0) = vv;
-            } else {
-              G[(ll)k * ld + j0] = xv.x * sc;
-              G[(ll)k * ld + j0 + 1] = xv.y * sc;
-            }
-          }
-        }
-      } else {
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int j = j0 + h;
-          if (j >= k + 1 && j < n) {
-            const double xn = one(2 * u + h, j, xs[j], pf[j], cf[j], true);
-            if (mine) {
-              xsn[j] = xn;
-              if (store_v) G[(ll)k * ld + j] = (j == k + 1) ? 1.0 : xs[j] * sc;
-            }
-          }
-        }
-      }
-    }
-    // (3) next reflector (every warp derives the same one), publish p', column k+2, s'
-    nrm = warp_sum_d(nrm);
-    a_next = __shfl_sync(0xffffffffu, a_next, ((k + 2) & 63) >> 1);
-    d_next = __shfl_sync(0xffffffffu, d_next, ((k + 1) & 63) >> 1);
-    double tk2 = 0.0, sc2 = 0.0, beta2 = 0.0;
-    if (k + 2 <= n - 1) house_real1(a_next, nrm, tk2, sc2, beta2);
-    if (rank == 0 && tid == 32) {
-      dg[k + 1] = d_next;
-      eg[k + 1] = beta2;
-      if (k + 1 < n - 1) tau[k + 1] = tk2;
-    }
-    double sp = 0.0;
-#pragma unroll
-    for (int i = 0; i < RW; ++i) {
-      const int r = rr[i];
-      const double a = warp_sum_d(acc[i]);
-      const double c = __shfl_sync(0xffffffffu, c2[i], ((k + 2) & 63) >> 1);
-      if (r >= k + 2 && r < n) {
-        const double p = tk2 * (c + sc2 * a);
-        if (lane == 0) {
-          pon[r >> lgC] = p;
-          con[r >> lgC] = c;
-        }
-        const double xnr = cf[r] - vr[i] * wk1 - wr[i];
-        sp += p * ((r == k + 2) ? 1.0 : xnr * sc2);
-      }
-    }
-    if (lane == 0) spn[warp] = sp;
-    tk = tk2;
-    sc = sc2;
-    cluster.sync();
-  }
-}
-
-template <int NT, int RW, int C>
-static cudaError_t hetrd_reg2_launch(double* G, int n, ll ld, double* d, double* e, double* tau,
-                                     cudaStream_t s) {
-  static std::atomic<unsigned long long> attr_cluster{0};
-  func_attr_once(attr_cluster, (const void*)hetrd_reg2_kernel<NT, RW, C>,
-                 cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(C);
-  cfg.blockDim = dim3(HT_THREADS);
-  const size_t n2 = (size_t)((n + 1) & ~1), Q2 = (size_t)((((n + C - 1) / C) + 1) & ~1);
-  cfg.dynamicSmemBytes = sizeof(double) * (4 * n2 + 4 * Q2 + 2 * (HT_THREADS / 32) + 16 * (HT_THREADS / 32));
-  cfg.stream = s;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = C;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, hetrd_reg2_kernel<NT, RW, C>, G, n, ld, d, e, tau);
 }
 
 // ----------------------------------------------------------------------------
@@ -528,7 +283,14 @@ static cudaError_t hetrd_reg2_launch(double* G, int n, ll ld, double* d, double*
 //     next reflector from the shared norm partials and (c) applies the rank-2
 //     update to its rows with the next symv in the same register pass.
 //     Waits are bounded: a CTA that gives up marks the whole cluster failed and
-//     the result is poisoned (d[0] = NaN) instead of hanging.
+//     the result is poisoned (d[0] = NaN) instead of hanging. A failed cluster
+//     drains before it exits: once every CTA has left its loop (so no further
+//     copy is issued), each publishes the last step it sent, and each receiver
+//     waits for exactly the blocks that were sent to it and not yet consumed
+//     (the bytes of peers that never sent are completed on its own barrier).
+//     A sender is at most one step ahead of any receiver, so at most one phase
+//     per barrier is outstanding. Only then does the final cluster barrier let
+//     the CTAs exit, so no bulk copy can land in a CTA that has left.
 // ----------------------------------------------------------------------------
 static constexpr int HP_SPIN = 1 << 20;  // polls of one barrier phase before giving up
 
@@ -542,6 +304,25 @@ __device__ inline uint32_t cluster_addr(uint32_t a, int cta) {
 }
 __device__ inline void bar_expect(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// counts bytes that will never arrive as arrived (drain of a failed cluster)
+__device__ inline void bar_complete(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.complete_tx.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// bounded wait for the phase of the given parity, without the failure shortcut
+__device__ inline bool bar_wait_drain(uint32_t bar, uint32_t parity) {
+  for (int it = 0; it < HP_SPIN; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
 }
 // true once the phase of the given parity has completed, false after HP_SPIN polls
 // or when the cluster has been marked failed
@@ -575,6 +356,7 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
   extern __shared__ __align__(16) double hsm[];
   __shared__ __align__(8) unsigned long long bars[2];
   __shared__ int fail_s;
+  __shared__ int peer_sent[C];  // last step each peer sent to this CTA (published after the loop)
   const int n2 = (n + 1) & ~1;
   // inbox of a step: one block per CTA, [Q (p, c) pairs of its rows by local index][NW partials
   // of s]; a CTA writes its own block and bulk-copies it into the same slot of every peer
@@ -626,6 +408,10 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
     bar_expect(bar0, step_bytes());                  // step 0 (pushed by the prologue)
     if (n - 2 >= 1) bar_expect(bar1, step_bytes());  // step 1
   }
+  // drain bookkeeping (uniform in the CTA; arming is done by thread 0)
+  int sent_last = 0;                       // the prologue sends step 0
+  int waited = n - 1;                      // steps 0 .. waited-1 were consumed
+  int armed_last = (n - 2 >= 1) ? 1 : 0;   // steps 0 .. armed_last have an armed phase
 
   int rr[RW];
   double g[RW][NT];
@@ -690,10 +476,19 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
     const uint32_t bar = par ? bar1 : bar0;
     auto pval = [&](int j) { return ib[(j & (C - 1)) * BLK + 2 * (j >> lgC)]; };
     auto cval = [&](int j) { return ib[(j & (C - 1)) * BLK + 2 * (j >> lgC) + 1]; };
-    // (1) every CTA's pushes of step k have landed
-    if (!bar_wait(bar, (uint32_t)((k >> 1) & 1), failv)) give_up();
-    if (tid == 0 && k + 2 <= n - 2 && !*failv) bar_expect(bar, step_bytes());  // re-arm for step k+2
-    __syncthreads();  // this CTA's own entries and column k (written last step) visible to all
+    // (1) every CTA's pushes of step k have landed; a CTA that gave up, or learned
+    //     that a peer did, leaves the loop as a whole (step k not consumed)
+    const bool got = bar_wait(bar, (uint32_t)((k >> 1) & 1), failv);
+    if (!got) give_up();
+    // also makes this CTA's own entries and column k (written last step) visible to all
+    if (__syncthreads_or(!got || *failv)) {
+      waited = k;
+      break;
+    }
+    if (k + 2 <= n - 2) {  // re-arm for step k+2
+      if (tid == 0) bar_expect(bar, step_bytes());
+      armed_last = k + 2;
+    }
     double ssum = 0.0;
     for (int q = lane; q < C * NW; q += 32) ssum += ib[(q / NW) * BLK + 2 * Q + (q % NW)];
     ssum = warp_sum_d(ssum);
@@ -809,11 +604,40 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncthreads();  // the block is complete
       send_block(par ^ 1);
+      sent_last = k + 1;
     }
     tk = tk2;
     sc = sc2;
   }
-  cluster.sync();  // no CTA leaves while a peer may still address its shared memory
+  // publish the last step this CTA sent (peers need it only if the cluster failed,
+  // which a CTA cannot know yet)
+  if (tid < C && tid != rank) {
+    const uint32_t a = cluster_addr(smem_u32(&peer_sent[rank]), tid);
+    asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(a), "r"(sent_last) : "memory");
+  }
+  // every CTA has left its loop: no further copy is issued, every failure mark and
+  // published step is visible
+  cluster.sync();
+  if (*failv && tid == 0) {
+    // wait for the blocks sent to this CTA and not consumed: steps waited and waited+1
+    int max_s = -1;
+    for (int c = 0; c < C; ++c)
+      if (c != rank) max_s = max(max_s, peer_sent[c]);
+    for (int st = waited; st <= max_s && st <= waited + 1; ++st) {
+      int senders = 0;
+      for (int c = 0; c < C; ++c)
+        if (c != rank && peer_sent[c] >= st) ++senders;
+      const uint32_t expect = (uint32_t)(8 * BLK * senders);
+      const uint32_t b = (st & 1) ? bar1 : bar0;
+      if (st <= armed_last) {
+        if (step_bytes() > expect) bar_complete(b, step_bytes() - expect);
+      } else {
+        bar_expect(b, expect);
+      }
+      (void)bar_wait_drain(b, (uint32_t)((st >> 1) & 1));
+    }
+  }
+  cluster.sync();  // no CTA leaves while a copy into it may be in flight
   if (rank == 0 && tid == 0 && *failv) dg[0] = __longlong_as_double(0x7ff8000000000000ll);
 }
 
@@ -840,29 +664,15 @@ static cudaError_t hetrd_push_launch(double* G, int n, ll ld, double* d, double*
   return cudaLaunchKernelEx(&cfg, hetrd_push_kernel<NT, RW, C>, G, n, ld, d, e, tau);
 }
 
-// exchange used by the register-resident reduction: 1 = push (st.async + mbarrier),
-// 0 = cluster barrier + pull; DMRG2_HETRD_EXCHANGE=pull selects the latter
-static int hetrd_exchange() {
-  static const int v = [] {
-    const char* e = std::getenv("DMRG2_HETRD_EXCHANGE");
-    return (e && std::string(e) == "pull") ? 0 : 1;
-  }();
-  return v;
-}
-
 // register-resident reduction for real G with 32 <= n <= 512; false when the device
 // refused the cluster (the caller then takes the shared-memory kernel)
 static bool hetrd_reg(double* G, int n, ll ld, double* d, double* e, double* tau, cudaStream_t s) {
   static std::atomic<int> refused{0};
   if (n < 32 || n > 512 || refused.load()) return false;
   cudaError_t err;
-  if (hetrd_exchange()) {
-    if (n <= 128) err = hetrd_push_launch<4, 1, 8>(G, n, ld, d, e, tau, s);
-    else if (n <= 256) err = hetrd_push_launch<8, 1, 16>(G, n, ld, d, e, tau, s);
-    else err = hetrd_push_launch<16, 2, 16>(G, n, ld, d, e, tau, s);
-  } else if (n <= 128) err = hetrd_reg2_launch<4, 1, 8>(G, n, ld, d, e, tau, s);
-  else if (n <= 256) err = hetrd_reg2_launch<8, 1, 16>(G, n, ld, d, e, tau, s);
-  else err = hetrd_reg2_launch<16, 2, 16>(G, n, ld, d, e, tau, s);
+  if (n <= 128) err = hetrd_push_launch<4, 1, 8>(G, n, ld, d, e, tau, s);
+  else if (n <= 256) err = hetrd_push_launch<8, 1, 16>(G, n, ld, d, e, tau, s);
+  else err = hetrd_push_launch<16, 2, 16>(G, n, ld, d, e, tau, s);
   if (err == cudaSuccess) return true;
   if (err == cudaErrorInvalidClusterSize || err == cudaErrorLaunchOutOfResources || err == cudaErrorInvalidValue) {
     (void)cudaGetLastError();

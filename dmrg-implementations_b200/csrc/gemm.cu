@@ -1,4 +1,6 @@
 // Host launcher and instantiations of the DMMA GEMM.
+#include <cstdlib>
+
 #include "gemm.cuh"
 
 namespace dmrg2 {
@@ -6,6 +8,14 @@ namespace dmrg2 {
 std::atomic<long long>& launch_counter() {
   static std::atomic<long long> c{0};
   return c;
+}
+
+bool test_unsignalled_waits() {
+  static const bool on = [] {
+    const char* e = std::getenv("DMRG2_TEST_UNSIGNALLED_WAITS");
+    return e && e[0] == '1';
+  }();
+  return on;
 }
 
 template <typename T>

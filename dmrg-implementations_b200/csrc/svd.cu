@@ -34,7 +34,9 @@ struct JacobiCfg<zc> {
 
 static constexpr int JT = 256;  // threads per Jacobi CTA
 
-__device__ bool jacobi_grid_sync(JacobiCtl* c, unsigned nblocks) {
+// grid barrier; `arrivals` is the block count (one more under the unsignalled-wait
+// test hook, so nothing completes it), `spin_max` the polls before it gives up
+__device__ bool jacobi_grid_sync(JacobiCtl* c, unsigned nblocks, long long spin_max) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -51,7 +53,7 @@ __device__ bool jacobi_grid_sync(JacobiCtl* c, unsigned nblocks) {
       long long spins = 0;
       while (*genp == g) {
         if (*((volatile int*)&c->err)) { ok = 0; break; }
-        if (++spins > (1LL << 25)) { atomicExch(&c->err, 2); ok = 0; break; }
+        if (++spins > spin_max) { atomicExch(&c->err, 2); ok = 0; break; }
         __nanosleep(64);
       }
     }
@@ -77,7 +79,7 @@ __device__ inline T conjT(T v) { return ST<T>::conj(v); }
 template <typename T>
 __global__ void __launch_bounds__(JT)
     jacobi_kernel(T* __restrict__ X, T* __restrict__ Q, int nvec, ll len, int nb, JacobiCtl* ctl,
-                  int max_sweeps, double tol, const double* fro2_dev) {
+                  int max_sweeps, double tol, const double* fro2_dev, int unsignalled) {
   constexpr int B = JacobiCfg<T>::B, P = 2 * B, CH = JacobiCfg<T>::CH;
   __shared__ T G[P][P + 1];
   __shared__ T J[P][P + 1];
@@ -229,7 +231,8 @@ __global__ void __launch_bounds__(JT)
         if (tid == 0) ctl->rotated[sweep] = 1;
         __syncthreads();
       }
-      alive = jacobi_grid_sync(ctl, gridDim.x);
+      alive = unsignalled ? jacobi_grid_sync(ctl, gridDim.x + 1, 1LL << 14)
+                          : jacobi_grid_sync(ctl, gridDim.x, 1LL << 25);
     }
     if (!alive) break;
     if (!*((volatile int*)&ctl->rotated[sweep])) { ++sweep; break; }
@@ -256,7 +259,8 @@ void svd_jacobi(T* X, T* Q, int nvec, ll len, JacobiCtl* ctl, int max_sweeps, do
   }
   int grid = nb / 2;
   if (grid > max_coresident) grid = max_coresident;
-  void* args[] = {&X, &Q, &nvec, &len, &nb, &ctl, &max_sweeps, &tol, (void*)&fro2_dev};
+  int unsignalled = test_unsignalled_waits() ? 1 : 0;
+  void* args[] = {&X, &Q, &nvec, &len, &nb, &ctl, &max_sweeps, &tol, (void*)&fro2_dev, &unsignalled};
   DMRG2_CUDA(cudaLaunchCooperativeKernel((const void*)jacobi_kernel<T>, dim3(grid), dim3(JT), args,
                                          0, s));
   DMRG2_CHECK_LAUNCH();

@@ -33,6 +33,7 @@ struct EigWork {
   cudaStream_t side = nullptr;  // builds the compact-WY triangles while the eigenvectors are computed
   cudaEvent_t ev_refl = nullptr, ev_wy = nullptr;
   int nmax = 0, Kmax = 0;
+  long long ns_extra = 0;  // truncations that needed the two extra Newton-Schulz iterations
   size_t bytes = 0;
   std::vector<void*> owned;
 
@@ -172,6 +173,12 @@ SvdOut eig_split(EigWork<T>& W, const T* theta, int m, int nt, char dir, int chi
     // below 1e-13; then the back-transform again (its WY triangles are still valid)
     for (int it = 0; it < 2; ++it) ns_iteration();
     apply_q<T>(W.G, n, W.tau, n, W.Z, K, W.out, W.Zg, W.Tb, s, true);
+    DMRG2_CUDA(cudaMemcpyAsync(W.h_out, W.out, sizeof(SvdOut), cudaMemcpyDeviceToHost, s));
+    DMRG2_CUDA(cudaStreamSynchronize(s));
+    if (!W.h_out->ns_done)
+      throw NumericError("eigensolver: kept eigenvectors not orthonormal to 2e-13 after five Newton-Schulz "
+                         "iterations (order " + std::to_string(n) + ", " + std::to_string(K) + " vectors)");
+    ++W.ns_extra;
   }
   const int k = o.k;
   if (R) {

@@ -52,6 +52,7 @@ constexpr int UM_THREADS = 128;
 constexpr int UM_PIECE_BYTES = UM_BM * UM_BK * 2;  // one 128 x 64 BF16 tile (16 KB)
 constexpr int UM_SMEM = 6 * UM_PIECE_BYTES;        // three A pieces + three B pieces
 constexpr int UM_SPIN = 1 << 22;                   // mbarrier polls before giving up
+constexpr int UM_SPIN_TEST = 1 << 10;              // the same under the unsignalled-wait test hook
 
 ll round_up(ll x, ll m) { return (x + m - 1) / m * m; }
 
@@ -73,8 +74,8 @@ __device__ inline uint64_t umma_sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo
 
 __device__ inline uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-__device__ inline bool mbar_wait(uint32_t bar, uint32_t parity, int* err) {
-  for (int it = 0; it < UM_SPIN; ++it) {
+__device__ inline bool mbar_wait(uint32_t bar, uint32_t parity, int* err, int spin) {
+  for (int it = 0; it < spin; ++it) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -156,7 +157,8 @@ template <typename T>
 __global__ void __launch_bounds__(UM_THREADS, 1)
     umma_bf16x3_kernel(const __nv_bfloat16* __restrict__ Ap, const __nv_bfloat16* __restrict__ Bp, int Mp,
                        int Np, int Kp, int nbA, int nbB, int M, int N, double alpha, double beta,
-                       T* __restrict__ C, ll ldc, ll sC, int* __restrict__ err, const int* skip) {
+                       T* __restrict__ C, ll ldc, ll sC, int* __restrict__ err, const int* skip,
+                       int unsignalled) {
   if (skip && *((volatile const int*)skip)) return;  // uniform: before any TMEM allocation
   extern __shared__ __align__(1024) unsigned char usm[];
   __shared__ __align__(8) uint64_t bar;
@@ -186,8 +188,11 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
 
   const int nk = Kp / UM_BK;
   const uint32_t idesc = umma_idesc_bf16(UM_BM, UM_BN);
+  const int spin = unsignalled ? UM_SPIN_TEST : UM_SPIN;
   bool ok = true;
-  for (int kt = 0; kt < nk && ok; ++kt) {
+  int kt_issued = -1;  // last K tile whose MMAs and commit were issued (thread 0)
+  int kt = 0;
+  for (; kt < nk && ok; ++kt) {
     // six pieces x 128 rows x 8 chunks of 16 bytes
     for (int q = tid; q < 6 * UM_BM * 8; q += UM_THREADS) {
       const int piece = q / (UM_BM * 8);
@@ -202,7 +207,8 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
     asm volatile("cp.async.wait_group 0;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
-    if (tid == 0) {
+    if (tid == 0 && !unsignalled) {
+      kt_issued = kt;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       constexpr int pa[6] = {0, 0, 1, 1, 0, 2};
       constexpr int pb[6] = {0, 1, 0, 1, 2, 0};
@@ -223,8 +229,17 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(sbar)
                    : "memory");
     }
-    ok = mbar_wait(sbar, (uint32_t)(kt & 1), err);
-    __syncthreads();  // every thread has seen the tile consumed before it is overwritten
+    // uniform in the CTA (a barrier also orders the tile's consumption before its refill)
+    ok = __syncthreads_and(mbar_wait(sbar, (uint32_t)(kt & 1), err, spin)) != 0;
+  }
+  if (!ok) {
+    // timed out: let the MMAs of the last issued tile finish (bounded) before the
+    // accumulator is released; the result is not read
+    if (tid == 0 && kt_issued == kt - 1) {
+      int dummy = 0;
+      (void)mbar_wait(sbar, (uint32_t)(kt_issued & 1), &dummy, UM_SPIN);
+    }
+    __syncthreads();
   }
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   // epilogue: warp w reads TMEM lanes 32w + lane (tile row), 128 FP32 columns
@@ -236,7 +251,7 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
   double* Cd = reinterpret_cast<double*>(C + (ll)b * sC);
   const int ew = ST<T>::cplx ? 2 : 1;
 #pragma unroll 1
-  for (int col = 0; col < UM_BN; col += 8) {
+  for (int col = 0; col < UM_BN && ok; col += 8) {
     uint32_t v[8];
     const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)col;
     asm volatile(
@@ -292,7 +307,7 @@ void gemm_bf16x3(int ta, int tb, int M, int N, int K, T alpha, const T* A, ll ld
   dim3 g((unsigned)(Np / UM_BN), (unsigned)(Mp / UM_BM), (unsigned)nbatch);
   umma_bf16x3_kernel<T><<<g, UM_THREADS, UM_SMEM, s>>>(Ap, Bp, (int)Mp, (int)Np, (int)Kp, nbA, nbB, M, N,
                                                       ST<T>::re(alpha), ST<T>::re(beta), C, ldc, sC, ws.err,
-                                                      skip);
+                                                      skip, test_unsignalled_waits() ? 1 : 0);
   DMRG2_CHECK_LAUNCH();
 }
 

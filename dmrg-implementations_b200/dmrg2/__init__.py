@@ -27,6 +27,7 @@ LIB_PATH = _HERE / "libdmrg2_b200.so"
 F64, C128 = 0, 1
 ROWMAJOR, REFERENCE = 0, 1
 INIT_RANDOM, INIT_PRODUCT, INIT_NEEL = 0, 1, 2
+OK, ERR_ARG, ERR_CUDA, ERR_STATE, ERR_NUMERIC, ERR_INTERNAL = 0, 1, 2, 3, 4, 5
 
 EXPORTED = [
     "dmrg2_create", "dmrg2_destroy", "dmrg2_set_mpo", "dmrg2_set_mps", "dmrg2_init_mps",

@@ -1,12 +1,15 @@
 """dmrg2_op_heff_noalloc: H_eff on device pointers with static scratch.
 
-Compared through the C ABI with the host-buffer entry point dmrg2_op_heff on
+Compared through the C ABI with the host-buffer entry point dmrg2_op_heff and
+with the CPU oracle's apply_heff (the reference's numpy contraction restated) on
 the same inputs, for two calls in a row (the second reuses the scratch the
 first left behind), tolerance 1e-12 relative to the largest output entry (the
 fused two-site MPO is built on the device instead of the host, so entries may
 differ in the last bit). Also checks that calls after the first leave the
-device's free memory unchanged and that oversized shapes are rejected. This
-file is collected last so it runs both alone and after every other GPU test.
+device's free memory unchanged, that oversized shapes are rejected, and (on a
+machine without a GPU) that shapes whose scratch size would overflow are
+rejected before any device work. This file is collected last so it runs both
+alone and after every other GPU test.
 """
 import ctypes
 
@@ -14,8 +17,8 @@ import numpy as np
 import pytest
 
 import dmrg2
+from oracle import dmrg2_oracle as O
 
-pytestmark = pytest.mark.gpu
 RTOL = 1e-12
 SCRATCH_BYTES = 64 << 20
 
@@ -63,6 +66,7 @@ def call_noalloc(torch, lib, code, shape, Ld, Rd, WLd, WRd, thd, outd):
                                      p(outd), stream)
 
 
+@pytest.mark.gpu
 @pytest.mark.parametrize("case", CASES)
 def test_noalloc_matches_op_heff_twice(torch_cuda, case):
     torch = torch_cuda
@@ -86,12 +90,13 @@ def test_noalloc_matches_op_heff_twice(torch_cuda, case):
         free_after.append(torch.cuda.mem_get_info()[0])
         outs.append(outd.cpu().numpy())
     for th, got in zip(thetas, outs):
-        ref = dmrg2.apply_heff(L, R, WL, WR, th)
-        close(got, ref)
+        close(got, dmrg2.apply_heff(L, R, WL, WR, th))
+        close(got, O.apply_heff(L, R, WL, WR, th))
     # the second call launched kernels only: the device's free memory is unchanged
     assert free_after[1] == free_after[0]
 
 
+@pytest.mark.gpu
 def test_noalloc_rejects_shapes_above_the_static_limit(torch_cuda):
     torch = torch_cuda
     lib = dmrg2.load_library()
@@ -109,3 +114,21 @@ def test_noalloc_rejects_shapes_above_the_static_limit(torch_cuda):
     assert rc == 1
     assert b"static limit" in lib.dmrg2_last_error(None)
     torch.cuda.synchronize()
+
+
+def test_noalloc_rejects_overflowing_shapes_before_device_work():
+    """Shapes whose scratch size would wrap around size_t are refused with
+    DMRG2_ERR_ARG before the entry point touches the device. Runs only where no
+    CUDA device is visible: the pointers are stand-ins that nothing may read."""
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("runs on a machine without a CUDA device")
+    lib = dmrg2.load_library()
+    fake = ctypes.c_void_p(256)
+    big = 1 << 30
+    for shape in [(big, big, 2, 5, 5, 5), (64, 64, 65536, 5, 5, 5), (big, 4, 2, 4096, 5, 4096)]:
+        cL, cR, d, Dl, Dm, Dr = shape
+        rc = lib.dmrg2_op_heff_noalloc(dmrg2.F64, cL, cR, d, Dl, Dm, Dr, fake, fake, fake, fake, fake, fake,
+                                       ctypes.c_void_p(0))
+        assert rc == 1, shape
+        assert b"static limit" in lib.dmrg2_last_error(None)
