@@ -331,6 +331,8 @@ EngineConfig engine_config(const dmrg2_config* cfg) {
   c.precision = cfg->precision;
   if (cfg->single_site != 0 && cfg->single_site != 1) throw std::invalid_argument("single_site must be 0 or 1");
   c.single_site = cfg->single_site;
+  if (cfg->truncation != 0 && cfg->truncation != 1) throw std::invalid_argument("unknown truncation");
+  c.truncation = cfg->truncation;
   return c;
 }
 void check_pos(std::initializer_list<int> v) {
@@ -484,6 +486,8 @@ static void fill_reports(const std::vector<SweepStats>& st, dmrg2_sweep_report* 
     r.jacobi_sweeps_max = st[s].jacobi_sweeps_max;
     r.device_s = st[s].device_s;
     r.lowprec_matvecs = st[s].lowprec_matvecs;
+    r.warm_splits = st[s].warm_splits;
+    r.warm_fallbacks = st[s].warm_fallbacks;
   }
 }
 

@@ -1,0 +1,28 @@
+// Cholesky factorisation and the row triangular solve of CholeskyQR (real FP64),
+// the orthonormalisation step of the warm-started subspace truncation.
+#pragma once
+
+#include "common.cuh"
+
+namespace dmrg2 {
+
+constexpr int CHOL_NB = 32;     // tile edge
+constexpr int CHOL_MAX = 512;   // largest order factorised (16 x 16 tiles)
+
+inline int chol_padded(int k) { return (k + CHOL_NB - 1) / CHOL_NB * CHOL_NB; }
+
+// Lower Cholesky factor of the symmetric positive definite k x k matrix in A (row-major,
+// lda >= chol_padded(k), the buffer holding chol_padded(k) rows; only the lower triangle
+// is read). On exit the lower triangle of the padded matrix holds L (the padding is the
+// identity), rdiag[j] = 1 / L_jj. *status becomes 1 (and stays so until the caller
+// clears it) when a pivot falls below rel_tol times the largest diagonal entry of A: the
+// matrix is then not numerically positive definite at that tolerance and L is not valid.
+// One 8-CTA cluster; enqueued on s.
+void chol_factor(double* A, int k, ll lda, double* rdiag, int* status, double rel_tol, cudaStream_t s);
+
+// Y <- Y L^{-T} in place for the m x k row-major Y (ldy): the orthonormal factor of
+// CholeskyQR when L L^T = Y^T Y. L and rdiag as chol_factor left them.
+void chol_solve_rows(double* Y, ll m, int k, ll ldy, const double* L, ll lda, const double* rdiag,
+                     const int* status, cudaStream_t s);
+
+}  // namespace dmrg2

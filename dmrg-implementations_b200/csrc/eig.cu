@@ -1325,7 +1325,7 @@ __global__ void ns_check_kernel(const double* __restrict__ S, int K, SvdOut* out
 // ----------------------------------------------------------------------------
 __global__ void __launch_bounds__(256)
     eig_truncate_kernel(const double* __restrict__ dg, const double* __restrict__ lam, int n, int K,
-                        int chi_max, double cutoff, int relative, SvdOut* out) {
+                        int chi_max, double cutoff, int relative, double floor_rel, SvdOut* out) {
   __shared__ double sh[33];
   __shared__ int kmin;
   const int tid = threadIdx.x;
@@ -1334,7 +1334,9 @@ __global__ void __launch_bounds__(256)
   tr = block_sum_t<double>(tr, sh);
   const double l0 = fmax(lam[0], 0.0);
   // density-matrix rounding floor: eigenvalues below ~16 eps lambda_max are noise
-  const double noise = 16.0 * 2.2e-16 * l0;
+  // (floor_rel; a caller may raise it where the vectors of a noise cluster did not
+  // come out orthonormal)
+  const double noise = floor_rel * l0;
   double thr = relative ? (cutoff * cutoff) * l0 : cutoff * cutoff;
   thr = fmax(thr, noise);
   const int kcap = chi_max < K ? chi_max : K;
@@ -1512,8 +1514,8 @@ void ns_check(const double* S, int K, SvdOut* out, double tol, double* part, uns
 }
 
 void eig_truncate(const double* d, const double* lam, int n, int K, int chi_max, double cutoff,
-                  bool relative, SvdOut* out, cudaStream_t s) {
-  eig_truncate_kernel<<<1, 256, 0, s>>>(d, lam, n, K, chi_max, cutoff, relative ? 1 : 0, out);
+                  bool relative, SvdOut* out, cudaStream_t s, double floor_rel) {
+  eig_truncate_kernel<<<1, 256, 0, s>>>(d, lam, n, K, chi_max, cutoff, relative ? 1 : 0, floor_rel, out);
   DMRG2_CHECK_LAUNCH();
 }
 

@@ -17,6 +17,7 @@
 #include <chrono>
 #include <cstring>
 #include <random>
+#include <type_traits>
 
 #include "contract.cuh"
 #include "engine.h"
@@ -26,6 +27,12 @@
 namespace dmrg2 {
 
 namespace {
+// the warm-started subspace split is built for real data, the density-matrix route and
+// bond caps of at most 512
+bool warm_capable(const EngineConfig& c) {
+  return !c.complex && c.truncation == 0 && c.svd_method == 0 && !c.single_site && c.chi_max <= CHOL_MAX;
+}
+
 ll ipow_cap(int d, int e, ll cap) {
   ll v = 1;
   for (int i = 0; i < e; ++i) {
@@ -84,6 +91,11 @@ class Engine final : public EngineBase {
     bytes_ += lw_.bytes(nmax_);
     ew_.init((int)qmax_, cfg_.chi_max);
     bytes_ += ew_.bytes;
+    if (warm_capable(cfg_)) {
+      wst_.init((int)qmax_, cfg_.chi_max);
+      bytes_ += wst_.bytes;
+    }
+    last_chi_.assign(L_ + 1, 0);
     sigma_ = (double*)dalloc_bytes(sizeof(double) * qmax_);
     perm_ = (int*)dalloc_bytes(sizeof(int) * qmax_);
     svdout_ = (SvdOut*)dalloc_bytes(sizeof(SvdOut));
@@ -112,6 +124,7 @@ class Engine final : public EngineBase {
     split_.release();
     lw_.release();
     ew_.release();
+    wst_.release();
     cudaEventDestroy(ev_c_);
     cudaEventDestroy(ev_d_);
     cudaEventDestroy(ev_s0_);
@@ -234,6 +247,7 @@ class Engine final : public EngineBase {
     mps_set_ = true;
     canonical_ = false;
     envs_valid_ = false;
+    std::fill(last_chi_.begin(), last_chi_.end(), 0);
   }
 
   void get_mps(std::vector<void*>& out) override {
@@ -252,6 +266,7 @@ class Engine final : public EngineBase {
       if (c < 1 || c > cfg_.chi_max) throw std::runtime_error("run: schedule chi outside [1, chi_max]");
     auto t0 = std::chrono::steady_clock::now();
     right_canonicalize();
+    std::fill(last_chi_.begin(), last_chi_.end(), 0);
     build_right_envs();
     DMRG2_CUDA(cudaStreamSynchronize(st_));
     env_build_s_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -585,10 +600,35 @@ class Engine final : public EngineBase {
     ss.trunc_err_sum += o.trunc_err;
   }
 
+  // the warm-started split applies when this sweep repeats the bond cap the last split of
+  // this bond used and that split kept the full cap (its factor next to theta is then an
+  // orthonormal basis of a chi-dimensional kept space)
+  bool warm_split_applies(int i, int chi, ll m, ll nc) const {
+    return wst_.kmax >= chi && last_chi_[i + 1] == chi && dims_[i + 1] == chi && std::min(m, nc) > chi;
+  }
+
   void svd_split(int i, char dir, int chi, SweepStats& ss) {
     const int cL = dims_[i], cR = dims_[i + 2];
     const ll m = (ll)cL * d_, nc = (ll)d_ * cR;
     DMRG2_CUDA(cudaEventRecord(ev_c_, st_));
+    if constexpr (std::is_same<T, double>::value) {
+      if (warm_split_applies(i, chi, m, nc)) {
+        double te = 0.0;
+        const double* warm = (dir == 'R') ? mps_[i + 1] : mps_[i];
+        if (wst_split(wst_, red_, theta_, (int)m, (int)nc, dir, chi, warm, mps_[i], mps_[i + 1], te, st_)) {
+          DMRG2_CUDA(cudaEventRecord(ev_d_, st_));
+          DMRG2_CUDA(cudaEventSynchronize(ev_d_));
+          float ms = 0.f;
+          DMRG2_CUDA(cudaEventElapsedTime(&ms, ev_c_, ev_d_));
+          ss.svd_s += ms * 1e-3;
+          ss.warm_splits += 1;
+          ss.trunc_err_max = std::max(ss.trunc_err_max, te);
+          ss.trunc_err_sum += te;
+          return;  // dims_[i + 1] stays chi
+        }
+        ss.warm_fallbacks += 1;
+      }
+    }
     SvdOut o;
     if (cfg_.svd_method == 1) {
       int nvec;
@@ -618,6 +658,7 @@ class Engine final : public EngineBase {
     ss.svd_s += ms * 1e-3;
     ss.jacobi_sweeps_max = std::max(ss.jacobi_sweeps_max, o.jacobi_sweeps);
     dims_[i + 1] = o.k;
+    last_chi_[i + 1] = chi;
     ss.trunc_err_max = std::max(ss.trunc_err_max, o.trunc_err);
     ss.trunc_err_sum += o.trunc_err;
   }
@@ -633,6 +674,8 @@ class Engine final : public EngineBase {
     *svdQ_ = nullptr, *tmp_ = nullptr;
   LanczosWork<T> lw_;
   EigWork<T> ew_;
+  WstWork wst_;                 // warm-started subspace split (real data)
+  std::vector<int> last_chi_;   // bond cap of the last split of each bond (0: none since the last set-up)
   double* sigma_ = nullptr;
   int* perm_ = nullptr;
   SvdOut* svdout_ = nullptr;
@@ -680,6 +723,7 @@ size_t engine_footprint(const EngineConfig& c, const std::vector<int>& Dl, const
          sizeof(double) * kk * kk + sizeof(double) * 5 * nn * kk + sb * nn * kk + sb * 256 * (nn + 1) +
          sizeof(double) * 64 + sizeof(unsigned) * 4 + sizeof(SvdOut);
   }
+  if (warm_capable(c)) b += wst_bytes(qmax, chi);
   b += sizeof(double) * (size_t)qmax + sizeof(int) * (size_t)qmax + sizeof(SvdOut) + sizeof(JacobiCtl) +
        sizeof(double) * 16 + sizeof(double) * (size_t)nblk * 2 * (KRYLOV_CAP + 2) + sizeof(unsigned) * 4 +
        sizeof(int) * (size_t)(L + 1);

@@ -28,6 +28,8 @@ struct EngineConfig {
   int svd_method = 0;          // 0: reduced density matrix eigensolver, 1: one-sided block Jacobi
   int precision = 0;           // 0: FP64 matvecs; 1: split-BF16 matvecs on tcgen05, then FP64 refinement
   int single_site = 0;         // 1: single-site sweeps (the reference's dmrg-gpu driver)
+  int truncation = 0;          // 0: warm-started subspace split on sweeps that repeat the previous
+                               //    sweep's bond cap (real data), exact otherwise; 1: exact always
   unsigned seed = 42;
 };
 
@@ -48,6 +50,8 @@ struct SweepStats {
   int jacobi_sweeps_max = 0;
   double device_s = 0.0;     // device time of the whole sweep (CUDA events on the engine stream)
   long long lowprec_matvecs = 0;  // precision form: matvecs on the split-BF16 operator
+  int warm_splits = 0;       // bonds split by the warm-started subspace truncation
+  int warm_fallbacks = 0;    // bonds where it gave up and the exact split ran
 };
 
 class EngineBase {

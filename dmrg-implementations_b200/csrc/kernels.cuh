@@ -105,8 +105,11 @@ void apply_q(const T* R, ll ld, const T* tau, int n, const double* Z, int K, con
              T* Tb, cudaStream_t s, bool wy_ready = false);
 void ns_check(const double* S, int K, SvdOut* out, double tol, double* part, unsigned* counter,
               cudaStream_t s);
+// k from the eigenvalues: min(chi_max, K, #lam above max(cutoff^2 (x lam_max if relative),
+// floor_rel lam_max)); eigenvalues at or below floor_rel lam_max are rounding noise
+constexpr double EIG_NOISE_FLOOR = 16.0 * 2.2e-16;
 void eig_truncate(const double* d, const double* lam, int n, int K, int chi_max, double cutoff,
-                  bool relative, SvdOut* out, cudaStream_t s);
+                  bool relative, SvdOut* out, cudaStream_t s, double floor_rel = EIG_NOISE_FLOOR);
 template <typename T>
 void copy_cols_conj(const T* in, ll ldi, int rows, int k, T* out, cudaStream_t s);
 template <typename T>

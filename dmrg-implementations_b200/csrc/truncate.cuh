@@ -4,9 +4,11 @@
 #pragma once
 
 #include <algorithm>
+#include <cstring>
 #include <stdexcept>
 #include <vector>
 
+#include "cholqr.cuh"
 #include "common.cuh"
 #include "gemm.cuh"
 #include "kernels.cuh"
@@ -33,7 +35,8 @@ struct EigWork {
   cudaStream_t side = nullptr;  // builds the compact-WY triangles while the eigenvectors are computed
   cudaEvent_t ev_refl = nullptr, ev_wy = nullptr;
   int nmax = 0, Kmax = 0;
-  long long ns_extra = 0;  // truncations that needed the two extra Newton-Schulz iterations
+  long long ns_extra = 0;      // truncations that needed the two extra Newton-Schulz iterations
+  long long floor_raised = 0;  // recomputations with a raised noise floor
   size_t bytes = 0;
   std::vector<void*> owned;
 
@@ -167,19 +170,35 @@ SvdOut eig_split(EigWork<T>& W, const T* theta, int m, int nt, char dir, int chi
   SvdOut o = *W.h_out;
   if (!std::isfinite(o.fro2))
     throw std::runtime_error("eigensolver: non-finite density matrix or tridiagonal reduction");
+  auto read_out = [&]() {
+    DMRG2_CUDA(cudaMemcpyAsync(W.h_out, W.out, sizeof(SvdOut), cudaMemcpyDeviceToHost, s));
+    DMRG2_CUDA(cudaStreamSynchronize(s));
+    o = *W.h_out;
+  };
   if (!o.ns_done) {
     // not orthonormal after three iterations: close tail eigenvalues just outside one
     // Gram-Schmidt window can leave overlaps near 0.15, which two more iterations bring
     // below 1e-13; then the back-transform again (its WY triangles are still valid)
     for (int it = 0; it < 2; ++it) ns_iteration();
     apply_q<T>(W.G, n, W.tau, n, W.Z, K, W.out, W.Zg, W.Tb, s, true);
-    DMRG2_CUDA(cudaMemcpyAsync(W.h_out, W.out, sizeof(SvdOut), cudaMemcpyDeviceToHost, s));
-    DMRG2_CUDA(cudaStreamSynchronize(s));
-    if (!W.h_out->ns_done)
-      throw NumericError("eigensolver: kept eigenvectors not orthonormal to 2e-13 after five Newton-Schulz "
-                         "iterations (order " + std::to_string(n) + ", " + std::to_string(K) + " vectors)");
+    read_out();
     ++W.ns_extra;
   }
+  // Still not orthonormal: kept eigenvalues just above the rounding floor, within rounding
+  // of one another, have ill-determined and nearly dependent vectors. Raise the floor
+  // (those Schmidt values are below ~3e-7 resp. 3e-6 of the largest) and recompute.
+  for (int attempt = 0; !o.ns_done && attempt < 2; ++attempt) {
+    eig_truncate(W.d, W.lam, n, K, chi, cutoff, relative, W.out, s, attempt == 0 ? 1e-13 : 1e-11);
+    tridiag_eigvecs(W.d, W.e, n, K, W.lam, W.out, W.Z, W.scr, gtol_rel, s);
+    group_mgs(W.Z, n, K, W.lam, W.out, gtol_rel, s);
+    for (int it = 0; it < 5; ++it) ns_iteration();
+    apply_q<T>(W.G, n, W.tau, n, W.Z, K, W.out, W.Zg, W.Tb, s, true);
+    read_out();
+    ++W.floor_raised;
+  }
+  if (!o.ns_done)
+    throw NumericError("eigensolver: kept eigenvectors not orthonormal to 2e-13 (order " + std::to_string(n) +
+                       ", " + std::to_string(K) + " vectors) even with the noise floor at 1e-11");
   const int k = o.k;
   if (R) {
     copy_cols_conj<T>(W.Zg, K, m, k, left, s);  // U = conj(eigvecs of conj(G))
@@ -204,6 +223,143 @@ SvdOut eig_split(EigWork<T>& W, const T* theta, int m, int nt, char dir, int chi
     DMRG2_CUDA(cudaStreamSynchronize(s));
   }
   return o;
+}
+
+
+// ============================================================================
+// Warm-started subspace truncation (real FP64).
+//
+// In a sweep that repeats the previous sweep's bond dimension k, the kept
+// subspace of a bond barely moves between sweeps, and the MPS already holds an
+// orthonormal basis of last sweep's kept space next to the optimised theta: for
+// a left-to-right step the right-canonical site B (k x nt, B B^T = 1), for a
+// right-to-left step the left-canonical site A (m x k, A^T A = 1). Three
+// half-steps of block power iteration on theta from that basis, each
+// orthonormalised by CholeskyQR (the last one twice), give the kept left (or
+// right) isometry; the other factor is its projection of theta, so the split is
+// exact for the kept subspace and its discarded weight is |theta|^2 - |kept|^2:
+//   'R': U1 = qr(theta B^T), V1 = qr(theta^T U1), U = qr2(theta V1),
+//        left = U, right = U^T theta
+//   'L': V1 = qr(theta^T A), U1 = qr(theta V1), V = qr2(theta^T U1),
+//        right = V^T, left = theta V
+// A Cholesky pivot below 1e-12 of the largest diagonal entry (a kept singular
+// value below ~1e-6 of the largest) makes it give up; the caller then runs the
+// exact split of the bond.
+// ============================================================================
+struct WstWork {
+  double* Ya = nullptr;  // qmax x kmax
+  double* Yb = nullptr;
+  double* G = nullptr;   // np x np, np = chol_padded(kmax)
+  double* rd = nullptr;  // np
+  double* nrm = nullptr; // |theta|^2, |kept factor|^2
+  int* status = nullptr;
+  double* h_buf = nullptr;  // pinned: status (as double), |theta|^2, |kept|^2
+  int qmax = 0, kmax = 0, np = 0;
+  size_t bytes = 0;
+  std::vector<void*> owned;
+
+  void* alloc(size_t b) {
+    void* p = nullptr;
+    DMRG2_CUDA(cudaMalloc(&p, std::max<size_t>(b, 16)));
+    owned.push_back(p);
+    bytes += b;
+    return p;
+  }
+  void init(int qmax_, int kmax_) {
+    qmax = std::max(qmax_, 1);
+    kmax = std::max(std::min(kmax_, CHOL_MAX), 1);
+    np = chol_padded(kmax);
+    Ya = (double*)alloc(sizeof(double) * (size_t)qmax * kmax);
+    Yb = (double*)alloc(sizeof(double) * (size_t)qmax * kmax);
+    G = (double*)alloc(sizeof(double) * (size_t)np * np);
+    rd = (double*)alloc(sizeof(double) * (size_t)np);
+    nrm = (double*)alloc(sizeof(double) * 4);
+    status = (int*)alloc(sizeof(int) * 4);
+    DMRG2_CUDA(cudaMallocHost(&h_buf, sizeof(double) * 4));
+  }
+  void release() {
+    for (void* p : owned) cudaFree(p);
+    owned.clear();
+    if (h_buf) cudaFreeHost(h_buf);
+    h_buf = nullptr;
+  }
+};
+
+// device bytes WstWork::init(qmax, kmax) allocates
+inline size_t wst_bytes(ll qmax, ll kmax) {
+  qmax = std::max<ll>(qmax, 1);
+  kmax = std::max<ll>(std::min<ll>(kmax, CHOL_MAX), 1);
+  const ll np = chol_padded((int)kmax);
+  return sizeof(double) * (size_t)(2 * qmax * kmax + np * np + np + 4) + sizeof(int) * 4;
+}
+
+// Y (rows x k) <- an orthonormal basis of its columns (CholeskyQR, `passes` times)
+inline void wst_qr(WstWork& W, double* Y, ll rows, int k, int passes, cudaStream_t s) {
+  for (int it = 0; it < passes; ++it) {
+    Gemm<double> g;  // G = Y^T Y
+    g.ta = true;
+    g.M = k; g.N = k; g.K = (int)rows;
+    g.A = Y; g.lda = k;
+    g.B = Y; g.ldb = k;
+    g.C = W.G; g.ldc = W.np;
+    launch_gemm(g, s);
+    chol_factor(W.G, k, W.np, W.rd, W.status, 1e-12, s);
+    chol_solve_rows(Y, rows, k, k, W.G, W.np, W.rd, W.status, s);
+  }
+}
+
+// Warm-started split of theta (m x nt) at kept rank k; `warm` is B (k x nt) for 'R',
+// A (m x k) for 'L'. Writes left (m x k) and right (k x nt) and returns true, or returns
+// false (left / right undefined) when CholeskyQR gave up. The host waits once.
+inline bool wst_split(WstWork& W, RedScratch& red, const double* theta, int m, int nt, char dir, int k,
+                      const double* warm, double* left, double* right, double& trunc_err, cudaStream_t s) {
+  if (k > W.kmax || m > W.qmax || nt > W.qmax) throw std::runtime_error("wst_split: workspace too small");
+  DMRG2_CUDA(cudaMemsetAsync(W.status, 0, sizeof(int), s));
+  auto mul = [&](bool ta, const double* A, ll lda, int M, int Kd, const double* B, ll ldb, bool tb, double* C) {
+    Gemm<double> g;  // C (M x k) = op(A) op(B)
+    g.ta = ta; g.tb = tb;
+    g.M = M; g.N = k; g.K = Kd;
+    g.A = A; g.lda = lda;
+    g.B = B; g.ldb = ldb;
+    g.C = C; g.ldc = k;
+    launch_gemm(g, s);
+  };
+  if (dir == 'R') {
+    mul(false, theta, nt, m, nt, warm, nt, true, W.Ya);  // theta B^T
+    wst_qr(W, W.Ya, m, k, 1, s);
+    mul(true, theta, nt, nt, m, W.Ya, k, false, W.Yb);   // theta^T U1
+    wst_qr(W, W.Yb, nt, k, 1, s);
+    mul(false, theta, nt, m, nt, W.Yb, k, false, left);  // theta V1
+    wst_qr(W, left, m, k, 2, s);
+    Gemm<double> g;  // right = U^T theta
+    g.ta = true;
+    g.M = k; g.N = nt; g.K = m;
+    g.A = left; g.lda = k;
+    g.B = theta; g.ldb = nt;
+    g.C = right; g.ldc = nt;
+    launch_gemm(g, s);
+    norm2(right, (ll)k * nt, W.nrm + 1, red, s);
+  } else {
+    mul(true, theta, nt, nt, m, warm, k, false, W.Ya);   // theta^T A
+    wst_qr(W, W.Ya, nt, k, 1, s);
+    mul(false, theta, nt, m, nt, W.Ya, k, false, W.Yb);  // theta V1
+    wst_qr(W, W.Yb, m, k, 1, s);
+    mul(true, theta, nt, nt, m, W.Yb, k, false, W.Ya);   // theta^T U1
+    wst_qr(W, W.Ya, nt, k, 2, s);
+    transpose(W.Ya, right, (ll)nt, (ll)k, s);            // right = V^T
+    mul(false, theta, nt, m, nt, W.Ya, k, false, left);  // left = theta V
+    norm2(left, (ll)m * k, W.nrm + 1, red, s);
+  }
+  norm2(theta, (ll)m * nt, W.nrm, red, s);
+  DMRG2_CUDA(cudaMemcpyAsync(W.h_buf + 1, W.nrm, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
+  int st = 0;
+  DMRG2_CUDA(cudaMemcpyAsync(W.h_buf, W.status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  DMRG2_CUDA(cudaStreamSynchronize(s));
+  std::memcpy(&st, W.h_buf, sizeof(int));
+  if (st) return false;
+  trunc_err = std::max(W.h_buf[1] - W.h_buf[2], 0.0);
+  if (!std::isfinite(W.h_buf[1]) || !std::isfinite(W.h_buf[2])) return false;
+  return true;
 }
 
 }  // namespace dmrg2

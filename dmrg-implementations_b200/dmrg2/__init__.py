@@ -51,7 +51,7 @@ class Config(ctypes.Structure):
         ("tol", ctypes.c_double), ("krylov_max", ctypes.c_int), ("lanczos_tol", ctypes.c_double),
         ("max_restarts", ctypes.c_int), ("cutoff", ctypes.c_double), ("min_sweeps", ctypes.c_int),
         ("device", ctypes.c_int), ("seed", ctypes.c_uint64), ("svd_method", ctypes.c_int),
-        ("precision", ctypes.c_int), ("single_site", ctypes.c_int),
+        ("precision", ctypes.c_int), ("single_site", ctypes.c_int), ("truncation", ctypes.c_int),
     ]
 
 
@@ -63,7 +63,7 @@ class SweepReport(ctypes.Structure):
         ("heff_s", ctypes.c_double), ("heff_flops", ctypes.c_double),
         ("lanczos_iters", ctypes.c_longlong), ("lanczos_unconverged", ctypes.c_int),
         ("svd_s", ctypes.c_double), ("jacobi_sweeps_max", ctypes.c_int), ("device_s", ctypes.c_double),
-        ("lowprec_matvecs", ctypes.c_longlong),
+        ("lowprec_matvecs", ctypes.c_longlong), ("warm_splits", ctypes.c_int), ("warm_fallbacks", ctypes.c_int),
     ]
 
     def as_dict(self):
@@ -225,7 +225,7 @@ class DMRG2GPU:
 
     def __init__(self, L, d, chi_max, D_mpo=None, tol=1e-10, dtype=np.float64, *, krylov_max=100,
                  lanczos_tol=1e-12, max_restarts=0, cutoff=1e-14, min_sweeps=2, device=0, seed=42,
-                 svd_method=0, precision=0, single_site=False):
+                 svd_method=0, precision=0, single_site=False, truncation=0):
         lib = load_library()
         self.L, self.d, self.chi_max, self.D_mpo = int(L), int(d), int(chi_max), D_mpo
         self.dtype = np.dtype(dtype)
@@ -234,7 +234,7 @@ class DMRG2GPU:
                      krylov_max=krylov_max, lanczos_tol=lanczos_tol, max_restarts=max_restarts,
                      cutoff=(cutoff if cutoff > 0 else -1.0), min_sweeps=min_sweeps, device=device,
                      seed=seed, svd_method=svd_method, precision=int(precision),
-                     single_site=int(bool(single_site)))
+                     single_site=int(bool(single_site)), truncation=int(truncation))
         h = ctypes.c_void_p()
         _check(lib.dmrg2_create(ctypes.byref(cfg), ctypes.byref(h)), None, "dmrg2_create")
         self._h = h
@@ -504,7 +504,7 @@ class Server:
 
     def submit(self, mpo, schedule, mps=None, init=INIT_RANDOM, seed=0, dtype=None, tol=1e-10,
                krylov_max=30, lanczos_tol=1e-12, max_restarts=2, cutoff=1e-14, min_sweeps=2, chi_max=None,
-               precision=0):
+               precision=0, truncation=0):
         """Queue one solve; returns its id. mpo: L tensors (Dl, Dr, d, d)."""
         Ws = _mpo4(mpo)
         L, d = len(Ws), Ws[0].shape[2]
@@ -519,6 +519,7 @@ class Server:
         cfg.max_restarts, cfg.min_sweeps, cfg.seed = max_restarts, min_sweeps, int(seed)
         cfg.cutoff = cutoff if cutoff > 0 else -1.0
         cfg.precision = int(precision)
+        cfg.truncation = int(truncation)
         wp = (ctypes.c_void_p * L)(*[w.ctypes.data for w in Ws])
         Dl = (ctypes.c_int * L)(*[w.shape[0] for w in Ws])
         Dr = (ctypes.c_int * L)(*[w.shape[1] for w in Ws])

@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define DMRG2_ABI_VERSION 2
+#define DMRG2_ABI_VERSION 3
 
 enum dmrg2_status {
   DMRG2_OK = 0,
@@ -77,6 +77,12 @@ typedef struct dmrg2_config {
   int single_site;    /* 0 = two-site sweeps (default); 1 = single-site sweeps, the reference's
                          dmrg-gpu driver (gpu-rocm/dmrg-gpu/src/dmrg_gpu_impl.h:1119-1450):
                          bond dimensions stay at those of the initial MPS (or shrink) */
+  int truncation;     /* 0 = warm-started subspace split (default): on a sweep that repeats
+                         the previous sweep's bond cap, real data, cap <= 512, the kept space
+                         comes from three CholeskyQR-orthonormalised power steps on theta from
+                         the MPS factor next to it, exact for that space; any other bond, or one
+                         where CholeskyQR gives up, takes the exact split of svd_method.
+                         1 = the exact split on every bond */
 } dmrg2_config;
 
 /* One row per sweep (left-to-right + right-to-left half sweep). */
@@ -97,6 +103,8 @@ typedef struct dmrg2_sweep_report {
   int jacobi_sweeps_max;
   double device_s;         /* device time of the whole sweep (CUDA events on the solver stream) */
   long long lowprec_matvecs; /* precision form: matvecs on the split-BF16 operator */
+  int warm_splits;           /* bonds split by the warm-started subspace truncation */
+  int warm_fallbacks;        /* bonds where it gave up and the exact split ran */
 } dmrg2_sweep_report;
 
 /* ---------------------------------------------------------------- solver */
