@@ -345,6 +345,8 @@ def run_ours(args):
     heff_s = sum(r["heff_s"] for r in timed)
     heff_fl = sum(r["heff_flops"] for r in timed)
     svd_s = sum(r["svd_s"] for r in timed)
+    warm_splits = sum(r["warm_splits"] for r in timed)
+    warm_fallbacks = sum(r["warm_fallbacks"] for r in timed)
     mv = sum(r["matvecs"] for r in timed)
     n_sw = len(timed)
 
@@ -388,6 +390,9 @@ def run_ours(args):
                      "peak_source": "cuBLAS DGEMM 8192^3 (torch.matmul float64) measured in this run; "
                                     "MEASURED_PEAKS.json has no FP64 figure"},
         "time_share": {"heff": heff_s / dev, "svd": svd_s / dev, "other": max(0.0, 1 - (heff_s + svd_s) / dev)},
+        "truncation": {"warm_splits": warm_splits, "warm_fallbacks": warm_fallbacks,
+                       "exact_splits": n_sw * 2 * (L_SITES - 1) - warm_splits,
+                       "ms_per_bond": 1e3 * svd_s / max(1, n_sw * 2 * (L_SITES - 1))},
         "dominant_kernel": {"name": "density-matrix truncation (Gram GEMM, cluster tridiagonalisation, bisection, "
                                     "inverse iteration, back-transform)",
                             "share": svd_s / dev, "bound": "latency",

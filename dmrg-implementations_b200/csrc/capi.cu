@@ -183,6 +183,39 @@ void do_op_svd_eig(int m, int n, const void* M, int max_bond, double cutoff, cha
   W.release();
 }
 
+// warm-started split of M (m x n) at rank k from the orthonormal factor `warm`
+// (dir 'R': k x n rows, dir 'L': m x k columns); false when CholeskyQR gave up
+bool do_op_warm_split(int m, int n, const void* M, const void* warm, int k, char dir, void* left, void* right,
+                      double* te_out) {
+  const size_t sb = sizeof(double);
+  const bool R = (dir == 'R');
+  DBuf dM(M, sb * (size_t)m * n), dw(warm, sb * (size_t)(R ? (size_t)k * n : (size_t)m * k));
+  DBuf dl(sb * (size_t)m * k), dr(sb * (size_t)k * n);
+  RedScratch red;
+  DBuf part(sizeof(double) * 2400), cnt(sizeof(unsigned) * 4);
+  red.part = part.as<double>();
+  red.counter = cnt.as<unsigned>();
+  red.nblk = 1184;
+  DMRG2_CUDA(cudaMemset(cnt.p, 0, sizeof(unsigned) * 4));
+  WstWork W;
+  bool ok = false;
+  double te = 0.0;
+  try {
+    W.init(std::max(m, n), k);
+    ok = wst_split(W, red, dM.as<double>(), m, n, dir, k, dw.as<double>(), dl.as<double>(), dr.as<double>(), te, 0);
+    if (ok) {
+      if (left) DMRG2_CUDA(cudaMemcpy(left, dl.p, sb * (size_t)m * k, cudaMemcpyDeviceToHost));
+      if (right) DMRG2_CUDA(cudaMemcpy(right, dr.p, sb * (size_t)k * n, cudaMemcpyDeviceToHost));
+      if (te_out) *te_out = te;
+    }
+  } catch (...) {
+    W.release();
+    throw;
+  }
+  W.release();
+  return ok;
+}
+
 template <typename T>
 void do_op_svd(int m, int n, const void* M, int max_bond, double cutoff, char dir, double* S,
                void* left, void* right, int* k_out, double* te_out) {
@@ -622,6 +655,20 @@ int dmrg2_op_svd(int dtype, int m, int n, const void* M, int max_bond, double cu
       if (jac) do_op_svd<double>(m, n, M, max_bond, cutoff, direction, S, left, right, k, trunc_err);
       else do_op_svd_eig<double>(m, n, M, max_bond, cutoff, direction, S, left, right, k, trunc_err);
     }
+  });
+}
+
+int dmrg2_op_warm_split(int dtype, int m, int n, const void* M, const void* warm, int k, char direction,
+                        void* left, void* right, double* trunc_err) {
+  return guarded(nullptr, [&] {
+    check_dtype(dtype);
+    check_pos({m, n, k});
+    if (dtype != DMRG2_F64) throw std::invalid_argument("op_warm_split: real (f64) data only");
+    if (direction != 'R' && direction != 'L') throw std::invalid_argument("op_warm_split: direction must be 'R' or 'L'");
+    if (!M || !warm) throw std::invalid_argument("op_warm_split: null input");
+    if (k > CHOL_MAX || k >= std::min(m, n)) throw std::invalid_argument("op_warm_split: need k < min(m, n) and k <= 512");
+    if (!do_op_warm_split(m, n, M, warm, k, direction, left, right, trunc_err))
+      throw NumericError("op_warm_split: CholeskyQR gave up (a kept singular value below ~1e-6 of the largest)");
   });
 }
 

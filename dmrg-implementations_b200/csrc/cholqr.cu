@@ -12,6 +12,12 @@
 //   T  one warp per trailing tile subtracts L_ip L_jp^T.
 // Pivots below rel_tol times the largest diagonal entry mark the matrix as not
 // numerically positive definite (the caller falls back to the exact split).
+// With shift_rel > 0 the matrix factorised is A + shift_rel trace(A) 1: shifted
+// CholeskyQR (Fukaya, Kannan, Nakatsukasa, Yamamoto and Yanagisawa, SIAM J. Sci.
+// Comput. 42 (2020)) takes shift 11 (m k + k (k+1)) u |Y|_F^2 for the Gram matrix
+// A = Y^T Y of an m x k block, which keeps the factorisation stable for any
+// condition number of Y below ~1/u and leaves Y R^{-1} with a condition number
+// of at most ~1/sqrt(shift_rel), so plain CholeskyQR can finish it.
 //
 // chol_solve_rows_kernel: Y <- Y L^{-T}, 8 rows of Y per CTA, tile column by tile
 // column: the update by the finished columns, then the forward substitution
@@ -63,7 +69,7 @@ __device__ __forceinline__ void chol_tile_col(double (&a)[NB], int lane, double 
 
 __global__ void __launch_bounds__(CT, 1)
     chol_cluster_kernel(double* __restrict__ A, int k, int np, ll lda, double* __restrict__ rdiag,
-                        int* __restrict__ status, double rel_tol) {
+                        int* __restrict__ status, double rel_tol, double shift_rel) {
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = (int)cluster.block_rank();
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -72,18 +78,32 @@ __global__ void __launch_bounds__(CT, 1)
   double* Lp = csm;                         // L_pp [NB][TP]
   double* Rp = Lp + NB * TP;                // 1 / diag of L_pp [NB]
   double* Wt = Rp + NB;                     // per warp: an L_jp tile [NW][NB][TP]
-  __shared__ double dmax_s;
+  __shared__ double dmax_s, shift_s;
 
   // padding rows r >= k become identity rows (lower triangle only)
   for (int r = k + rank; r < np; r += CC)
     for (int c = tid; c <= r; c += CT) stg_l2(A + (ll)r * lda + c, c == r ? 1.0 : 0.0);
   if (warp == 0) {
-    double m = 0.0;
-    for (int i = lane; i < k; i += 32) m = fmax(m, ldg_l2(A + (ll)i * lda + i));
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (lane == 0) dmax_s = m;
+    double m = 0.0, tr = 0.0;
+    for (int i = lane; i < k; i += 32) {
+      const double a = ldg_l2(A + (ll)i * lda + i);
+      m = fmax(m, a);
+      tr += a;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+      tr += __shfl_xor_sync(0xffffffffu, tr, o);
+    }
+    if (lane == 0) {
+      shift_s = shift_rel * tr;
+      dmax_s = m + shift_s;
+    }
   }
-  cluster.sync();
+  cluster.sync();  // padding written, every CTA has read the unshifted diagonal
+  if (shift_rel > 0.0) {
+    for (int i = rank * CT + tid; i < k; i += CC * CT) stg_l2(A + (ll)i * lda + i, ldg_l2(A + (ll)i * lda + i) + shift_s);
+    cluster.sync();
+  }
   const double piv_min = rel_tol * dmax_s;
   const double piv_sub = dmax_s > 0.0 ? dmax_s : 1.0;
 
@@ -231,7 +251,8 @@ __global__ void __launch_bounds__(ST_THREADS)
 
 }  // namespace
 
-void chol_factor(double* A, int k, ll lda, double* rdiag, int* status, double rel_tol, cudaStream_t s) {
+void chol_factor(double* A, int k, ll lda, double* rdiag, int* status, double rel_tol, cudaStream_t s,
+                 double shift_rel) {
   const int np = chol_padded(k);
   if (k < 1 || np > CHOL_MAX) throw std::invalid_argument("chol_factor: order outside 1..512");
   if (lda < np) throw std::invalid_argument("chol_factor: lda below the padded order");
@@ -250,7 +271,7 @@ void chol_factor(double* A, int k, ll lda, double* rdiag, int* status, double re
   at[0].val.clusterDim.z = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  DMRG2_CUDA(cudaLaunchKernelEx(&cfg, chol_cluster_kernel, A, k, np, lda, rdiag, status, rel_tol));
+  DMRG2_CUDA(cudaLaunchKernelEx(&cfg, chol_cluster_kernel, A, k, np, lda, rdiag, status, rel_tol, shift_rel));
   DMRG2_CHECK_LAUNCH();
 }
 
@@ -260,7 +281,8 @@ void chol_solve_rows(double* Y, ll m, int k, ll ldy, const double* L, ll lda, co
   if (m < 1) return;
   static std::atomic<unsigned long long> attr{0};
   const int smem = (int)sizeof(double) * (SR * (np + 1) + NB * TP + SR * TP);
-  set_smem_attr_once(attr, (const void*)chol_solve_rows_kernel, smem);
+  constexpr int smem_max = (int)sizeof(double) * (SR * (CHOL_MAX + 1) + NB * TP + SR * TP);
+  set_smem_attr_once(attr, (const void*)chol_solve_rows_kernel, smem_max);  // covers every order
   const ll grid = (m + SR - 1) / SR;
   if (grid > 2147483647LL) throw std::invalid_argument("chol_solve_rows: too many rows");
   chol_solve_rows_kernel<<<(unsigned)grid, ST_THREADS, smem, s>>>(Y, m, k, np, ldy, L, lda, rdiag, status);

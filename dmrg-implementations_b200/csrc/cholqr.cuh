@@ -17,8 +17,10 @@ inline int chol_padded(int k) { return (k + CHOL_NB - 1) / CHOL_NB * CHOL_NB; }
 // identity), rdiag[j] = 1 / L_jj. *status becomes 1 (and stays so until the caller
 // clears it) when a pivot falls below rel_tol times the largest diagonal entry of A: the
 // matrix is then not numerically positive definite at that tolerance and L is not valid.
+// shift_rel > 0 factorises A + shift_rel trace(A) 1 instead (shifted CholeskyQR).
 // One 8-CTA cluster; enqueued on s.
-void chol_factor(double* A, int k, ll lda, double* rdiag, int* status, double rel_tol, cudaStream_t s);
+void chol_factor(double* A, int k, ll lda, double* rdiag, int* status, double rel_tol, cudaStream_t s,
+                 double shift_rel = 0.0);
 
 // Y <- Y L^{-T} in place for the m x k row-major Y (ldy): the orthonormal factor of
 // CholeskyQR when L L^T = Y^T Y. L and rdiag as chol_factor left them.

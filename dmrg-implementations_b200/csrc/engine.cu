@@ -95,7 +95,6 @@ class Engine final : public EngineBase {
       wst_.init((int)qmax_, cfg_.chi_max);
       bytes_ += wst_.bytes;
     }
-    last_chi_.assign(L_ + 1, 0);
     sigma_ = (double*)dalloc_bytes(sizeof(double) * qmax_);
     perm_ = (int*)dalloc_bytes(sizeof(int) * qmax_);
     svdout_ = (SvdOut*)dalloc_bytes(sizeof(SvdOut));
@@ -247,7 +246,7 @@ class Engine final : public EngineBase {
     mps_set_ = true;
     canonical_ = false;
     envs_valid_ = false;
-    std::fill(last_chi_.begin(), last_chi_.end(), 0);
+    prev_sweep_chi_ = 0;
   }
 
   void get_mps(std::vector<void*>& out) override {
@@ -266,7 +265,7 @@ class Engine final : public EngineBase {
       if (c < 1 || c > cfg_.chi_max) throw std::runtime_error("run: schedule chi outside [1, chi_max]");
     auto t0 = std::chrono::steady_clock::now();
     right_canonicalize();
-    std::fill(last_chi_.begin(), last_chi_.end(), 0);
+    prev_sweep_chi_ = 0;
     build_right_envs();
     DMRG2_CUDA(cudaStreamSynchronize(st_));
     env_build_s_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -307,6 +306,7 @@ class Engine final : public EngineBase {
       ss.energy = e;
       ss.max_bond = *std::max_element(dims_.begin(), dims_.end());
       energy_ = e;
+      prev_sweep_chi_ = schedule[sw];
       out.push_back(ss);
       if (stop_rule && (int)sw + 1 >= cfg_.min_sweeps && std::fabs(e - e_prev) < cfg_.tol) break;
       e_prev = e;
@@ -600,11 +600,12 @@ class Engine final : public EngineBase {
     ss.trunc_err_sum += o.trunc_err;
   }
 
-  // the warm-started split applies when this sweep repeats the bond cap the last split of
-  // this bond used and that split kept the full cap (its factor next to theta is then an
-  // orthonormal basis of a chi-dimensional kept space)
+  // the warm-started split applies on a sweep that repeats the previous sweep's bond cap
+  // (not in the first sweep at a new cap, where the state still moves far) to a bond that
+  // kept the full cap (its factor next to theta is then an orthonormal basis of a
+  // chi-dimensional kept space)
   bool warm_split_applies(int i, int chi, ll m, ll nc) const {
-    return wst_.kmax >= chi && last_chi_[i + 1] == chi && dims_[i + 1] == chi && std::min(m, nc) > chi;
+    return wst_.kmax >= chi && prev_sweep_chi_ == chi && dims_[i + 1] == chi && std::min(m, nc) > chi;
   }
 
   void svd_split(int i, char dir, int chi, SweepStats& ss) {
@@ -658,7 +659,6 @@ class Engine final : public EngineBase {
     ss.svd_s += ms * 1e-3;
     ss.jacobi_sweeps_max = std::max(ss.jacobi_sweeps_max, o.jacobi_sweeps);
     dims_[i + 1] = o.k;
-    last_chi_[i + 1] = chi;
     ss.trunc_err_max = std::max(ss.trunc_err_max, o.trunc_err);
     ss.trunc_err_sum += o.trunc_err;
   }
@@ -675,7 +675,7 @@ class Engine final : public EngineBase {
   LanczosWork<T> lw_;
   EigWork<T> ew_;
   WstWork wst_;                 // warm-started subspace split (real data)
-  std::vector<int> last_chi_;   // bond cap of the last split of each bond (0: none since the last set-up)
+  int prev_sweep_chi_ = 0;      // bond cap of the last completed sweep (0: none since the last set-up)
   double* sigma_ = nullptr;
   int* perm_ = nullptr;
   SvdOut* svdout_ = nullptr;

@@ -234,17 +234,18 @@ SvdOut eig_split(EigWork<T>& W, const T* theta, int m, int nt, char dir, int chi
 // orthonormal basis of last sweep's kept space next to the optimised theta: for
 // a left-to-right step the right-canonical site B (k x nt, B B^T = 1), for a
 // right-to-left step the left-canonical site A (m x k, A^T A = 1). Three
-// half-steps of block power iteration on theta from that basis, each
-// orthonormalised by CholeskyQR (the last one twice), give the kept left (or
-// right) isometry; the other factor is its projection of theta, so the split is
-// exact for the kept subspace and its discarded weight is |theta|^2 - |kept|^2:
+// half-steps of block power iteration on theta from that basis, each made
+// orthonormal by one shifted CholeskyQR pass and one plain pass (the last one by
+// two plain passes), give the kept left (or right) isometry; the other factor
+// is its projection of theta, so the split is exact for the kept subspace and its
+// discarded weight is |theta|^2 - |kept|^2:
 //   'R': U1 = qr(theta B^T), V1 = qr(theta^T U1), U = qr2(theta V1),
 //        left = U, right = U^T theta
 //   'L': V1 = qr(theta^T A), U1 = qr(theta V1), V = qr2(theta^T U1),
 //        right = V^T, left = theta V
-// A Cholesky pivot below 1e-12 of the largest diagonal entry (a kept singular
-// value below ~1e-6 of the largest) makes it give up; the caller then runs the
-// exact split of the bond.
+// The shifted pass handles kept singular values down to ~1e-12 of the largest; a
+// pivot of a plain pass below 1e-14 of the largest diagonal entry (an input that
+// is not of full rank k) makes it give up, and the caller runs the exact split.
 // ============================================================================
 struct WstWork {
   double* Ya = nullptr;  // qmax x kmax
@@ -293,9 +294,14 @@ inline size_t wst_bytes(ll qmax, ll kmax) {
   return sizeof(double) * (size_t)(2 * qmax * kmax + np * np + np + 4) + sizeof(int) * 4;
 }
 
-// Y (rows x k) <- an orthonormal basis of its columns (CholeskyQR, `passes` times)
-inline void wst_qr(WstWork& W, double* Y, ll rows, int k, int passes, cudaStream_t s) {
-  for (int it = 0; it < passes; ++it) {
+// Y (rows x k) <- Y R^{-1} with R^T R = Y^T Y (+ shift): one shifted CholeskyQR pass,
+// which leaves a basis of the same span with condition number ~1/sqrt(shift) (a
+// well-conditioned start for the next power step), and `plain` CholeskyQR passes after
+// it, which make the basis orthonormal to rounding.
+inline void wst_qr(WstWork& W, double* Y, ll rows, int k, int plain, cudaStream_t s) {
+  const double u = 1.1102230246251565e-16;
+  const double shift_rel = 11.0 * ((double)rows * k + (double)k * (k + 1)) * u;
+  for (int it = 0; it <= plain; ++it) {
     Gemm<double> g;  // G = Y^T Y
     g.ta = true;
     g.M = k; g.N = k; g.K = (int)rows;
@@ -303,7 +309,7 @@ inline void wst_qr(WstWork& W, double* Y, ll rows, int k, int passes, cudaStream
     g.B = Y; g.ldb = k;
     g.C = W.G; g.ldc = W.np;
     launch_gemm(g, s);
-    chol_factor(W.G, k, W.np, W.rd, W.status, 1e-12, s);
+    chol_factor(W.G, k, W.np, W.rd, W.status, it == 0 ? 1e-300 : 1e-14, s, it == 0 ? shift_rel : 0.0);
     chol_solve_rows(Y, rows, k, k, W.G, W.np, W.rd, W.status, s);
   }
 }

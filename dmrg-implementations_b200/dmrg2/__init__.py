@@ -36,7 +36,7 @@ EXPORTED = [
     "dmrg2_abi_version", "dmrg2_op_heff", "dmrg2_op_env_left", "dmrg2_op_env_right",
     "dmrg2_op_svd", "dmrg2_op_lanczos", "dmrg2_op_gemm", "dmrg2_resume", "dmrg2_get_launch_count",
     "dmrg2_op_heff_noalloc", "dmrg2_server_create", "dmrg2_server_submit", "dmrg2_server_poll",
-    "dmrg2_server_destroy", "dmrg2_op_gemm_bf16x3",
+    "dmrg2_server_destroy", "dmrg2_op_gemm_bf16x3", "dmrg2_op_warm_split",
 ]
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
 
@@ -128,6 +128,7 @@ def load_library(path: str | os.PathLike | None = None):
         "dmrg2_get_device_bytes": (c_int, [vp, ctypes.POINTER(ctypes.c_size_t)]),
         "dmrg2_last_error": (ctypes.c_char_p, [vp]),
         "dmrg2_abi_version": (c_int, []),
+        "dmrg2_op_warm_split": (c_int, [c_int, c_int, c_int, vp, vp, c_int, ctypes.c_char, vp, vp, dp]),
         "dmrg2_op_heff": (c_int, [c_int] * 7 + [vp] * 6),
         "dmrg2_op_heff_noalloc": (c_int, [c_int] * 7 + [vp] * 7),
         "dmrg2_op_env_left": (c_int, [c_int] * 6 + [vp] * 4),
@@ -428,6 +429,21 @@ def truncated_svd(M, max_bond, cutoff=0.0, direction="R", method="eig"):
            None, "op_svd")
     k = k.value
     return left[: m * k].reshape(m, k), S, right[: k * n].reshape(k, n), te.value
+
+
+def warm_split(M, warm, k, direction="R"):
+    """Warm-started subspace split of the real M at rank k from the orthonormal factor
+    `warm` of a previous split (k x n rows for 'R', m x k columns for 'L'); returns
+    (left, right, trunc_err)."""
+    M = _prep(M, F64)
+    warm = _prep(warm, F64)
+    m, n = M.shape
+    left = np.zeros((m, k))
+    right = np.zeros((k, n))
+    te = ctypes.c_double()
+    _check(load_library().dmrg2_op_warm_split(F64, m, n, _ptr(M), _ptr(warm), int(k), direction.encode()[:1],
+                                              _ptr(left), _ptr(right), ctypes.byref(te)), None, "op_warm_split")
+    return left, right, te.value
 
 
 def optimize_two_site(L_env, R_env, W_left, W_right, theta_init, max_iter=100, tol=1e-12,

@@ -198,6 +198,18 @@ int dmrg2_op_svd(int dtype, int m, int n, const void* M, int max_bond, double cu
 /* optimize_two_site(L, R, W_left, W_right, theta0)  (cpu/pdmrg/pdmrg/numerics/eigensolver.py:13-63;
  * GPU: lanczos_eigensolver, impl:971-1160). theta is the start vector on entry
  * and the normalised ground state on exit. */
+/* The warm-started subspace split of the engine (dmrg2_config.truncation = 0) on one
+ * matrix, real data: M (m x n, row-major) split at rank k (k < min(m, n), k <= 512)
+ * from an orthonormal factor `warm` of a previous split, k x n rows (dir 'R') or m x k
+ * columns (dir 'L'). Three CholeskyQR-orthonormalised power steps; 'R': left (m x k)
+ * isometric columns, right = left^T M; 'L': right (k x n) isometric rows, left =
+ * M right^T; trunc_err = |M|^2 - |kept factor|^2. DMRG2_ERR_NUMERIC when CholeskyQR
+ * gives up (then the engine takes the exact split). Replaces, with svd_split's
+ * truncation, the reference's gesvd step (gpu-rocm/dmrg2-gpu/src/dmrg2_gpu_impl.h:1167-1343)
+ * on sweeps that repeat the bond cap. */
+int dmrg2_op_warm_split(int dtype, int m, int n, const void* M, const void* warm, int k, char direction,
+                        void* left, void* right, double* trunc_err);
+
 int dmrg2_op_lanczos(int dtype, int cL, int cR, int d, int Dl, int Dm, int Dr, const void* L,
                      const void* R, const void* WL, const void* WR, void* theta, int krylov_max,
                      double tol, int max_restarts, double* energy, int* iters);

@@ -164,7 +164,7 @@ def right_canonicalize(mps):
 def mps_norm2(mps):
     E = np.ones((1, 1), dtype=mps[0].dtype)
     for A in mps:
-        E = np.einsum("ab,asc,bsd->cd", E, A.conj(), A)
+        E = np.einsum("ab,asc,bsd->cd", E, A.conj(), A, optimize=True)
     return float(E[0, 0].real)
 
 
@@ -174,15 +174,15 @@ def expect_local(mps, op):
     out = np.zeros(L, dtype=np.result_type(mps[0].dtype, np.asarray(op).dtype))
     left = [np.ones((1, 1), dtype=mps[0].dtype)]
     for A in mps:
-        left.append(np.einsum("ab,asc,bsd->cd", left[-1], A.conj(), A))
+        left.append(np.einsum("ab,asc,bsd->cd", left[-1], A.conj(), A, optimize=True))
     right = [None] * (L + 1)
     right[L] = np.ones((1, 1), dtype=mps[0].dtype)
     for i in range(L - 1, -1, -1):
         A = mps[i]
-        right[i] = np.einsum("cd,asc,bsd->ab", right[i + 1], A.conj(), A)
+        right[i] = np.einsum("cd,asc,bsd->ab", right[i + 1], A.conj(), A, optimize=True)
     nrm = left[L][0, 0]
     for i, A in enumerate(mps):
-        out[i] = np.einsum("ab,atc,ts,bsd,cd->", left[i], A.conj(), op, A, right[i + 1]) / nrm
+        out[i] = np.einsum("ab,atc,ts,bsd,cd->", left[i], A.conj(), op, A, right[i + 1], optimize=True) / nrm
     return out
 
 

@@ -302,3 +302,80 @@ def test_lanczos_vs_dense(cplx):
     ov = abs(np.vdot(V[:, 0], th.ravel()))
     assert abs(ov - 1.0) < 1e-8
     assert abs(np.linalg.norm(th) - 1.0) < 1e-12
+
+
+def _orth_rows(X):
+    q, _ = np.linalg.qr(X.T)
+    return q.T
+
+
+@pytest.mark.parametrize("m,n,k,direction", [(64, 64, 20, "R"), (96, 64, 32, "L"), (128, 160, 48, "R"),
+                                             (256, 200, 100, "L"), (512, 512, 256, "R"), (512, 512, 256, "L"),
+                                             (40, 64, 8, "R")])
+def test_warm_split_vs_numpy(m, n, k, direction):
+    """The warm-started subspace split (three CholeskyQR power steps) against numpy's SVD:
+    M has singular values 1 .. 1e-2 on the kept k and a gap of 100 below them; the warm
+    factor is last split's subspace perturbed by 1e-3. The kept factor is orthonormal to
+    1e-13, its projector equals the top-k singular projector to 1e-9, the other factor is
+    its projection of M, and the discarded weight matches to 1e-12 relative to |M|^2."""
+    rng = np.random.default_rng(m * 7 + n + k)
+    r = min(m, n)
+    U, _ = np.linalg.qr(rng.standard_normal((m, r)))
+    V, _ = np.linalg.qr(rng.standard_normal((n, r)))
+    s = np.concatenate([np.logspace(0, -2, k), 1e-4 * np.logspace(0, -3, r - k)])
+    M = (U * s) @ V.T
+    if direction == "R":
+        warm = _orth_rows(V[:, :k].T + 1e-3 * rng.standard_normal((k, n)))
+    else:
+        warm = _orth_rows(U[:, :k].T + 1e-3 * rng.standard_normal((k, m))).T
+    left, right, te = dmrg2.warm_split(M, warm, k, direction)
+    Pk = U[:, :k] @ U[:, :k].T
+    Qk = V[:, :k] @ V[:, :k].T
+    if direction == "R":
+        np.testing.assert_allclose(left.T @ left, np.eye(k), atol=1e-13)
+        assert np.abs(left @ left.T - Pk).max() < 1e-9
+        np.testing.assert_allclose(right, left.T @ M, atol=1e-13)
+    else:
+        np.testing.assert_allclose(right @ right.T, np.eye(k), atol=1e-13)
+        assert np.abs(right.T @ right - Qk).max() < 1e-9
+        np.testing.assert_allclose(left, M @ right.T, atol=1e-13)
+    assert abs(te - np.sum(s[k:] ** 2)) <= 1e-12 * np.sum(s ** 2)
+
+
+@pytest.mark.parametrize("direction", ["R", "L"])
+def test_warm_split_wide_kept_spectrum(direction):
+    """Kept singular values spanning 1 .. 1e-9 (a DMRG bond at a large bond cap keeps
+    Schmidt values far below 1e-6 of the largest): the shifted CholeskyQR pass keeps the
+    split on the warm path (no fallback) and the kept factor still spans the top-k
+    singular space to 1e-9 and is orthonormal to 1e-13."""
+    rng = np.random.default_rng(11)
+    m = n = 512
+    k = 256
+    U, _ = np.linalg.qr(rng.standard_normal((m, m)))
+    V, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    s = np.concatenate([np.logspace(0, -9, k), 1e-11 * np.logspace(0, -3, m - k)])
+    M = (U * s) @ V.T
+    if direction == "R":
+        warm = _orth_rows(V[:, :k].T + 1e-6 * rng.standard_normal((k, n)))
+    else:
+        warm = _orth_rows(U[:, :k].T + 1e-6 * rng.standard_normal((k, m))).T
+    left, right, te = dmrg2.warm_split(M, warm, k, direction)
+    if direction == "R":
+        np.testing.assert_allclose(left.T @ left, np.eye(k), atol=1e-13)
+        assert np.abs(left @ left.T - U[:, :k] @ U[:, :k].T).max() < 1e-9
+    else:
+        np.testing.assert_allclose(right @ right.T, np.eye(k), atol=1e-13)
+        assert np.abs(right.T @ right - V[:, :k] @ V[:, :k].T).max() < 1e-9
+    assert abs(te - np.sum(s[k:] ** 2)) <= 1e-12 * np.sum(s ** 2)
+
+
+def test_warm_split_gives_up_on_a_rank_deficient_factor():
+    """A warm factor with directions outside the range of M makes CholeskyQR's Gram
+    matrix singular: the split reports DMRG2_ERR_NUMERIC (the engine then runs the exact
+    split) instead of returning a non-orthonormal factor."""
+    rng = np.random.default_rng(3)
+    m, n, k = 64, 64, 16
+    M = rng.standard_normal((m, 8)) @ rng.standard_normal((8, n))  # rank 8 < k
+    warm = _orth_rows(rng.standard_normal((k, n)))
+    with pytest.raises(dmrg2.Dmrg2Error, match=f"status {dmrg2.ERR_NUMERIC}"):
+        dmrg2.warm_split(M, warm, k, "R")
