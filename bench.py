@@ -347,6 +347,7 @@ def run_ours(args):
     svd_s = sum(r["svd_s"] for r in timed)
     warm_splits = sum(r["warm_splits"] for r in timed)
     warm_fallbacks = sum(r["warm_fallbacks"] for r in timed)
+    eig_fallbacks = sum(r["eig_fallbacks"] for r in timed)
     mv = sum(r["matvecs"] for r in timed)
     n_sw = len(timed)
 
@@ -390,7 +391,7 @@ def run_ours(args):
                      "peak_source": "cuBLAS DGEMM 8192^3 (torch.matmul float64) measured in this run; "
                                     "MEASURED_PEAKS.json has no FP64 figure"},
         "time_share": {"heff": heff_s / dev, "svd": svd_s / dev, "other": max(0.0, 1 - (heff_s + svd_s) / dev)},
-        "truncation": {"warm_splits": warm_splits, "warm_fallbacks": warm_fallbacks,
+        "truncation": {"warm_splits": warm_splits, "warm_fallbacks": warm_fallbacks, "eig_fallbacks": eig_fallbacks,
                        "exact_splits": n_sw * 2 * (L_SITES - 1) - warm_splits,
                        "ms_per_bond": 1e3 * svd_s / max(1, n_sw * 2 * (L_SITES - 1))},
         "dominant_kernel": {"name": "density-matrix truncation (Gram GEMM, cluster tridiagonalisation, bisection, "

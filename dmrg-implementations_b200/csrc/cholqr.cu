@@ -181,6 +181,240 @@ __global__ void __launch_bounds__(CT, 1)
   }
 }
 
+// ---------------------------------------------------------------------------
+// cholinv_cluster_kernel: X = L^{-1}, L L^T = G (+ shift), for orders k <= 256, in one
+// cluster of 8 CTAs with every tile in shared memory: CTA r holds block row r of G
+// (turned into L in place) and block row r of X, and stages the tiles it needs from
+// its peers (distributed shared memory) in a third area. Per tile column p:
+//   D  CTA p, warp 0: in-register Cholesky of the diagonal tile (rsqrt, one shuffle
+//      broadcast per column); warp 1 then inverts it into X_pp off the critical path
+//      (after the CTA has arrived at the cluster barrier);
+//   P  CTAs r > p: L_rp = A_rp L_pp^{-T} by forward substitution (lane = row);
+//   T  CTAs r > p: A_rj -= L_rp L_jp^T for p < j <= r (one warp per tile). CTA p+1
+//      owns only tile (p+1, p+1) and factors it right after (look-ahead: no barrier
+//      between its update and the next diagonal factorisation).
+// Then X by tile diagonals s = 1 .. nblk-1: X_{r,r-s} = -X_rr sum_j L_rj X_{j,r-s}
+// (CTA r, its peers' X tiles staged), and each CTA writes its block row of X (zeros
+// above the diagonal) to global memory. Two cluster barriers per tile column and one
+// per tile diagonal; nothing leaves shared memory until the end.
+// ---------------------------------------------------------------------------
+constexpr int CI_MAXB = 8;
+constexpr int CI_THREADS = 256;
+constexpr int CI_TILE = NB * TP;  // doubles per padded tile
+constexpr size_t CI_SMEM = sizeof(double) * (3 * CI_MAXB * CI_TILE + 2 * NB);
+
+__device__ inline void cl_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
+__device__ inline void cl_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
+
+// column J of the in-register Cholesky of one diagonal tile (lane i holds row i) with a
+// reciprocal square root per pivot, then the columns after it
+template <int J>
+__device__ __forceinline__ void ci_tile_col(double (&a)[NB], int lane, double piv_min, double piv_sub,
+                                            bool& bad, double* rd) {
+  double piv = __shfl_sync(0xffffffffu, a[J], J);
+  if (!(piv > piv_min)) {  // also catches NaN
+    bad = true;
+    piv = piv_sub;
+  }
+  const double r = rsqrt(piv);
+  if (lane == J) {
+    a[J] = piv * r;
+    rd[J] = r;
+  } else if (lane > J) {
+    a[J] *= r;
+  }
+#pragma unroll
+  for (int c = J + 1; c < NB; ++c) {
+    const double lc = __shfl_sync(0xffffffffu, a[J], c);
+    if (lane >= c) a[c] -= a[J] * lc;
+  }
+  if constexpr (J + 1 < NB) ci_tile_col<J + 1>(a, lane, piv_min, piv_sub, bad, rd);
+}
+
+__global__ void __launch_bounds__(CI_THREADS, 1)
+    cholinv_cluster_kernel(const double* __restrict__ G, int k, int np, ll ldg, double* __restrict__ X, ll ldx,
+                           int* __restrict__ status, double rel_tol, double shift_rel) {
+  cg::cluster_group cluster = cg::this_cluster();
+  const int r = (int)cluster.block_rank();
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nblk = np / NB;
+  extern __shared__ __align__(16) double cism[];
+  double* Lt = cism;                           // [CI_MAXB] tiles: block row r of G -> L
+  double* Xt = Lt + CI_MAXB * CI_TILE;         // [CI_MAXB] tiles: block row r of X
+  double* St = Xt + CI_MAXB * CI_TILE;         // [CI_MAXB] staged tiles of peers
+  double* Rd = St + CI_MAXB * CI_TILE;         // 1 / diag of this CTA's L_rr
+  double* Rs = Rd + NB;                        // staged 1 / diag of L_pp
+  __shared__ double tr_s, dmax_s;
+  auto T_ = [](double* base, int t) { return base + t * CI_TILE; };
+
+  // trace and largest diagonal entry of G (every CTA reads them from global memory)
+  if (warp == 0) {
+    double m = 0.0, tr = 0.0;
+    for (int i = lane; i < k; i += 32) {
+      const double a = G[(ll)i * ldg + i];
+      m = fmax(m, a);
+      tr += a;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+      tr += __shfl_xor_sync(0xffffffffu, tr, o);
+    }
+    if (lane == 0) {
+      tr_s = tr;
+      dmax_s = m + shift_rel * tr;
+    }
+  }
+  __syncthreads();
+  const double shift = shift_rel * tr_s;
+  const double piv_min = rel_tol * dmax_s;
+  const double piv_sub = dmax_s > 0.0 ? dmax_s : 1.0;
+  // block row r of G (+ shift on the diagonal; identity beyond k; lower part of the diagonal tile)
+  if (r < nblk)
+    for (int j = 0; j <= r; ++j)
+      for (int e = tid; e < NB * NB; e += CI_THREADS) {
+        const int row = e >> 5, col = e & 31;
+        const int gi = r * NB + row, gj = j * NB + col;
+        double v;
+        if (gi < k && gj < k) v = (j < r || col <= row) ? G[(ll)gi * ldg + gj] + (gi == gj ? shift : 0.0) : 0.0;
+        else v = (gi == gj) ? 1.0 : 0.0;
+        T_(Lt, j)[row * TP + col] = v;
+      }
+  cluster.sync();
+
+  for (int p = 0; p < nblk; ++p) {
+    // ---- D: diagonal tile of CTA p (its tile p, already updated by every earlier column)
+    if (r == p && warp == 0) {
+      double a[NB];
+      double* Lpp = T_(Lt, p);
+#pragma unroll
+      for (int j = 0; j < NB; ++j) a[j] = (j <= lane) ? Lpp[lane * TP + j] : 0.0;
+      bool bad = false;
+      ci_tile_col<0>(a, lane, piv_min, piv_sub, bad, Rd);
+#pragma unroll
+      for (int j = 0; j < NB; ++j) Lpp[lane * TP + j] = (j <= lane) ? a[j] : 0.0;
+      if (bad && lane == 0) atomicExch(status, 1);
+    }
+    __syncthreads();  // L_pp and Rd written before the barrier and before warp 1 reads them
+    cl_arrive();
+    if (r == p && warp == 1) {
+      // X_pp = L_pp^{-1}: lane c forms column c by forward substitution
+      const double* Lpp = T_(Lt, p);
+      double x[NB];
+#pragma unroll
+      for (int i = 0; i < NB; ++i) {
+        double s = (i == lane) ? 1.0 : 0.0;
+#pragma unroll
+        for (int j = 0; j < i; ++j) s -= Lpp[i * TP + j] * x[j];
+        x[i] = s * Rd[i];
+      }
+#pragma unroll
+      for (int i = 0; i < NB; ++i) T_(Xt, p)[i * TP + lane] = x[i];
+    }
+    cl_wait();
+    // ---- P: L_rp = A_rp L_pp^{-T}
+    if (r > p && r < nblk) {
+      const double* Rpp = cluster.map_shared_rank(T_(Lt, p), p);
+      const double* Rrd = cluster.map_shared_rank(Rd, p);
+      for (int e = tid; e < NB * NB; e += CI_THREADS) St[(e >> 5) * TP + (e & 31)] = Rpp[(e >> 5) * TP + (e & 31)];
+      if (tid < NB) Rs[tid] = Rrd[tid];
+      __syncthreads();
+      if (warp == 0) {
+        double* Arp = T_(Lt, p);
+        double x[NB];
+#pragma unroll
+        for (int c = 0; c < NB; ++c) x[c] = Arp[lane * TP + c];
+#pragma unroll
+        for (int c = 0; c < NB; ++c) {
+          x[c] *= Rs[c];
+#pragma unroll
+          for (int c2 = c + 1; c2 < NB; ++c2) x[c2] -= x[c] * St[c2 * TP + c];
+        }
+#pragma unroll
+        for (int c = 0; c < NB; ++c) Arp[lane * TP + c] = x[c];
+      }
+    }
+    cluster.sync();  // every L_rp of this column is final
+    // ---- T: A_rj -= L_rp L_jp^T, p < j <= r
+    if (r > p && r < nblk) {
+      for (int j = p + 1; j < r; ++j) {  // peers' L_jp into staging slot j
+        const double* src = cluster.map_shared_rank(T_(Lt, p), j);
+        for (int e = tid; e < NB * NB; e += CI_THREADS) T_(St, j)[(e >> 5) * TP + (e & 31)] = src[(e >> 5) * TP + (e & 31)];
+      }
+      __syncthreads();
+      const int j = p + 1 + warp;
+      if (j <= r) {
+        const double* Ljp = (j == r) ? T_(Lt, p) : T_(St, j);
+        const double* Lrp = T_(Lt, p);
+        double x[NB], acc[NB];
+#pragma unroll
+        for (int t = 0; t < NB; ++t) {
+          x[t] = Lrp[lane * TP + t];
+          acc[t] = 0.0;
+        }
+#pragma unroll
+        for (int t = 0; t < NB; ++t)
+#pragma unroll
+          for (int c = 0; c < NB; ++c) acc[c] += x[t] * Ljp[c * TP + t];
+        double* Arj = T_(Lt, j);
+        const int cmax = (j == r) ? lane : NB - 1;
+#pragma unroll
+        for (int c = 0; c < NB; ++c)
+          if (c <= cmax) Arj[lane * TP + c] -= acc[c];
+      }
+      __syncthreads();  // staging reused by the next column; tile (r, p+1) final before D / P
+    }
+  }
+  cluster.sync();  // every X_pp is written
+  // ---- X below the diagonal, one tile diagonal at a time
+  for (int s = 1; s < nblk; ++s) {
+    if (r >= s && r < nblk) {
+      const int q = r - s;
+      for (int j = q; j < r; ++j) {  // X_{j,q} of CTA j into staging slot j - q
+        const double* src = cluster.map_shared_rank(T_(Xt, q), j);
+        for (int e = tid; e < NB * NB; e += CI_THREADS) T_(St, j - q)[(e >> 5) * TP + (e & 31)] = src[(e >> 5) * TP + (e & 31)];
+      }
+      __syncthreads();
+      // W = sum_j L_rj X_jq: warp w rows 4w..4w+3, lane = column
+      double w4[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int j = q; j < r; ++j) {
+        const double* Lrj = T_(Lt, j);
+        const double* Xjq = T_(St, j - q);
+#pragma unroll 8
+        for (int t = 0; t < NB; ++t) {
+          const double xv = Xjq[t * TP + lane];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) w4[u] += Lrj[(4 * warp + u) * TP + t] * xv;
+        }
+      }
+      double* Wt = T_(St, CI_MAXB - 1);  // free: at most 7 tiles are staged
+#pragma unroll
+      for (int u = 0; u < 4; ++u) Wt[(4 * warp + u) * TP + lane] = w4[u];
+      __syncthreads();
+      // X_rq = -X_rr W
+      const double* Xrr = T_(Xt, r);
+      double o4[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 8
+      for (int t = 0; t < NB; ++t) {
+        const double wv = Wt[t * TP + lane];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) o4[u] -= Xrr[(4 * warp + u) * TP + t] * wv;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) T_(Xt, q)[(4 * warp + u) * TP + lane] = o4[u];
+    }
+    cluster.sync();  // X tiles of this diagonal visible to the peers
+  }
+  // ---- block row r of X to global memory (lower triangle, zeros above)
+  if (r < nblk)
+    for (int j = 0; j < nblk; ++j)
+      for (int e = tid; e < NB * NB; e += CI_THREADS) {
+        const int row = e >> 5, col = e & 31;
+        const int gi = r * NB + row, gj = j * NB + col;
+        if (gi < k && gj < k) X[(ll)gi * ldx + gj] = (j < r || (j == r && col <= row)) ? T_(Xt, j)[row * TP + col] : 0.0;
+      }
+  cluster.sync();  // no CTA leaves while a peer may still read its shared memory
+}
+
 constexpr int SR = 8;        // rows of Y per CTA in the solve
 constexpr int ST_THREADS = 64;
 
@@ -249,7 +483,76 @@ __global__ void __launch_bounds__(ST_THREADS)
   }
 }
 
+// every column of Y (rows x k, ld k) scaled to unit norm; a zero or non-finite column
+// sets *status. One CTA per 32 columns (lane = column, warps stride the rows).
+__global__ void __launch_bounds__(256) col_normalize_kernel(double* __restrict__ Y, ll rows, int k,
+                                                            int* __restrict__ status) {
+  __shared__ double part[8][33];
+  __shared__ double inv[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int c = blockIdx.x * 32 + lane;
+  double sq = 0.0;
+  if (c < k)
+    for (ll r = warp; r < rows; r += 8) {
+      const double v = Y[r * k + c];
+      sq += v * v;
+    }
+  part[warp][lane] = sq;
+  __syncthreads();
+  if (warp == 0) {
+    double t = 0.0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) t += part[w][lane];
+    double sc = 0.0;
+    if (c < k) {
+      if (t > 0.0 && isfinite(t)) sc = rsqrt(t);
+      else atomicExch(status, 1);
+    }
+    inv[lane] = sc;
+  }
+  __syncthreads();
+  if (c < k)
+    for (ll r = warp; r < rows; r += 8) Y[r * k + c] *= inv[lane];
+}
+
+__global__ void mark_unconverged_kernel(const SvdOut* out, int* status) {
+  if (!out->ns_done) *status = 1;
+}
+
 }  // namespace
+
+void mark_unconverged(const SvdOut* out, int* status, cudaStream_t s) {
+  mark_unconverged_kernel<<<1, 1, 0, s>>>(out, status);
+  DMRG2_CHECK_LAUNCH();
+}
+
+void col_normalize(double* Y, ll rows, int k, int* status, cudaStream_t s) {
+  if (rows < 1 || k < 1) return;
+  col_normalize_kernel<<<(unsigned)((k + 31) / 32), 256, 0, s>>>(Y, rows, k, status);
+  DMRG2_CHECK_LAUNCH();
+}
+
+void chol_inverse(const double* G, int k, ll ldg, double* X, ll ldx, int* status, double rel_tol, double shift_rel,
+                  cudaStream_t s) {
+  const int np = chol_padded(k);
+  if (k < 1 || np > CI_MAXB * NB) throw std::invalid_argument("chol_inverse: order outside 1..256");
+  static std::atomic<unsigned long long> attr{0};
+  set_smem_attr_once(attr, (const void*)cholinv_cluster_kernel, (int)CI_SMEM);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(CI_MAXB);
+  cfg.blockDim = dim3(CI_THREADS);
+  cfg.dynamicSmemBytes = CI_SMEM;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = CI_MAXB;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  DMRG2_CUDA(cudaLaunchKernelEx(&cfg, cholinv_cluster_kernel, G, k, np, ldg, X, ldx, status, rel_tol, shift_rel));
+  DMRG2_CHECK_LAUNCH();
+}
 
 void chol_factor(double* A, int k, ll lda, double* rdiag, int* status, double rel_tol, cudaStream_t s,
                  double shift_rel) {

@@ -3,6 +3,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "kernels.cuh"
 
 namespace dmrg2 {
 
@@ -21,6 +22,22 @@ inline int chol_padded(int k) { return (k + CHOL_NB - 1) / CHOL_NB * CHOL_NB; }
 // One 8-CTA cluster; enqueued on s.
 void chol_factor(double* A, int k, ll lda, double* rdiag, int* status, double rel_tol, cudaStream_t s,
                  double shift_rel = 0.0);
+
+// X = L^{-1} (k x k row-major, ldx; zeros above the diagonal) where L L^T = G +
+// shift_rel trace(G) 1 for the symmetric positive definite k x k G (row-major, ldg; only
+// its lower triangle is read), k <= 256. Everything stays in the shared memory of one
+// 8-CTA cluster until X is written. *status becomes 1 when a pivot falls below rel_tol
+// times the largest (shifted) diagonal entry; X is then not valid.
+constexpr int CHOL_INV_MAX = 256;
+void chol_inverse(const double* G, int k, ll ldg, double* X, ll ldx, int* status, double rel_tol, double shift_rel,
+                  cudaStream_t s);
+
+// *status = 1 unless out->ns_done (a Newton-Schulz run that did not converge)
+void mark_unconverged(const SvdOut* out, int* status, cudaStream_t s);
+
+// every column of the rows x k row-major Y scaled to unit norm (*status = 1 on a zero
+// or non-finite column)
+void col_normalize(double* Y, ll rows, int k, int* status, cudaStream_t s);
 
 // Y <- Y L^{-T} in place for the m x k row-major Y (ldy): the orthonormal factor of
 // CholeskyQR when L L^T = Y^T Y. L and rdiag as chol_factor left them.

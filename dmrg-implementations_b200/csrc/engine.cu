@@ -417,8 +417,18 @@ class Engine final : public EngineBase {
       const int cl = dims_[i], cr = dims_[i + 1];
       const int nc = d_ * cr;
       const int chi = std::min(cfg_.chi_max, cap_[i]);
-      int k;
-      if (cfg_.svd_method == 1) {
+      int k = 0;
+      bool jacobi = (cfg_.svd_method == 1);
+      if (!jacobi) {
+        try {
+          SvdOut o = eig_split(ew_, mps_[i], cl, nc, 'L', chi, 1e-14, true, tmp_, mps_[i], st_);
+          k = o.k;
+          scale_inplace(tmp_, (ll)cl * k, &ew_.out->sigma_max2, st_);
+        } catch (const NumericError&) {
+          jacobi = true;  // eigenvectors not orthonormal: the Jacobi SVD splits this site
+        }
+      }
+      if (jacobi) {
         transpose(mps_[i], svdX_, cl, nc, st_);
         norm2(svdX_, (ll)cl * nc, dscal_, red_, st_);
         set_identity(svdQ_, nc, st_);
@@ -427,10 +437,6 @@ class Engine final : public EngineBase {
         k = read_svd().k;
         svd_gather(svdX_, svdQ_, perm_, nc, (ll)cl, k, 1, tmp_, mps_[i], st_);
         scale_inplace(tmp_, (ll)cl * k, &svdout_->sigma_max2, st_);
-      } else {
-        SvdOut o = eig_split(ew_, mps_[i], cl, nc, 'L', chi, 1e-14, true, tmp_, mps_[i], st_);
-        k = o.k;
-        scale_inplace(tmp_, (ll)cl * k, &ew_.out->sigma_max2, st_);
       }
       {  // A[i-1] <- A[i-1] . (U S / sigma_max)
         Gemm<T> g;
@@ -601,11 +607,23 @@ class Engine final : public EngineBase {
   }
 
   // the warm-started split applies on a sweep that repeats the previous sweep's bond cap
-  // (not in the first sweep at a new cap, where the state still moves far) to a bond that
-  // kept the full cap (its factor next to theta is then an orthonormal basis of a
-  // chi-dimensional kept space)
+  // (not in the first sweep at a new cap, where the state still moves far); it keeps the
+  // bond's dimension k (the factor next to theta is an orthonormal basis of a
+  // k-dimensional kept space)
   bool warm_split_applies(int i, int chi, ll m, ll nc) const {
-    return wst_.kmax >= chi && prev_sweep_chi_ == chi && dims_[i + 1] == chi && std::min(m, nc) > chi;
+    const int k = dims_[i + 1];
+    return prev_sweep_chi_ == chi && k <= chi && k <= wst_.kmax && std::min(m, nc) > k;
+  }
+
+  // A bond below the cap keeps its dimension only while the weight the warm split
+  // discards could all lie below the exact split's threshold (cutoff^2, or the density
+  // matrix's rounding floor 16 eps |theta|^2): otherwise some discarded Schmidt value
+  // may be above it, the exact split would keep more states, and it runs instead (this
+  // is how a bond dimension grows back).
+  bool warm_split_keeps_rank(int k, int chi, ll m, ll nc, double te, double fro2) const {
+    if (k >= chi) return true;
+    const double thr = std::max(cfg_.cutoff * cfg_.cutoff, EIG_NOISE_FLOOR * fro2);
+    return te <= (double)(std::min(m, nc) - k) * thr;
   }
 
   void svd_split(int i, char dir, int chi, SweepStats& ss) {
@@ -616,7 +634,9 @@ class Engine final : public EngineBase {
       if (warm_split_applies(i, chi, m, nc)) {
         double te = 0.0;
         const double* warm = (dir == 'R') ? mps_[i + 1] : mps_[i];
-        if (wst_split(wst_, red_, theta_, (int)m, (int)nc, dir, chi, warm, mps_[i], mps_[i + 1], te, st_)) {
+        const int k = dims_[i + 1];
+        if (wst_split(wst_, red_, theta_, (int)m, (int)nc, dir, k, warm, mps_[i], mps_[i + 1], te, st_) &&
+            warm_split_keeps_rank(k, chi, m, nc, te, wst_.h_buf[1])) {
           DMRG2_CUDA(cudaEventRecord(ev_d_, st_));
           DMRG2_CUDA(cudaEventSynchronize(ev_d_));
           float ms = 0.f;
@@ -625,13 +645,26 @@ class Engine final : public EngineBase {
           ss.warm_splits += 1;
           ss.trunc_err_max = std::max(ss.trunc_err_max, te);
           ss.trunc_err_sum += te;
-          return;  // dims_[i + 1] stays chi
+          return;  // dims_[i + 1] unchanged
         }
         ss.warm_fallbacks += 1;
       }
     }
     SvdOut o;
-    if (cfg_.svd_method == 1) {
+    bool jacobi = (cfg_.svd_method == 1);
+    if (!jacobi) {
+      try {
+        o = eig_split(ew_, theta_, (int)m, (int)nc, dir, chi, cfg_.cutoff, false, mps_[i], mps_[i + 1], st_);
+        DMRG2_CUDA(cudaEventRecord(ev_d_, st_));
+        DMRG2_CUDA(cudaEventSynchronize(ev_d_));
+      } catch (const NumericError&) {
+        // the eigenvectors of this density matrix could not be made orthonormal: split the
+        // bond with the one-sided Jacobi SVD of theta instead (theta is unchanged)
+        jacobi = true;
+        ss.eig_fallbacks += 1;
+      }
+    }
+    if (jacobi) {
       int nvec;
       ll len;
       if (dir == 'R') {
@@ -649,10 +682,6 @@ class Engine final : public EngineBase {
       DMRG2_CUDA(cudaEventRecord(ev_d_, st_));
       o = read_svd();
       svd_gather(svdX_, svdQ_, perm_, nvec, len, o.k, dir == 'R' ? 0 : 1, mps_[i], mps_[i + 1], st_);
-    } else {
-      o = eig_split(ew_, theta_, (int)m, (int)nc, dir, chi, cfg_.cutoff, false, mps_[i], mps_[i + 1], st_);
-      DMRG2_CUDA(cudaEventRecord(ev_d_, st_));
-      DMRG2_CUDA(cudaEventSynchronize(ev_d_));
     }
     float ms = 0.f;
     DMRG2_CUDA(cudaEventElapsedTime(&ms, ev_c_, ev_d_));

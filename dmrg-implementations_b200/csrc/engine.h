@@ -52,6 +52,8 @@ struct SweepStats {
   long long lowprec_matvecs = 0;  // precision form: matvecs on the split-BF16 operator
   int warm_splits = 0;       // bonds split by the warm-started subspace truncation
   int warm_fallbacks = 0;    // bonds where it gave up and the exact split ran
+  int eig_fallbacks = 0;     // bonds where the density-matrix eigenvectors could not be made
+                             // orthonormal and the Jacobi SVD split the bond
 };
 
 class EngineBase {

@@ -4,6 +4,8 @@
 #pragma once
 
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <stdexcept>
 #include <vector>
@@ -234,28 +236,50 @@ SvdOut eig_split(EigWork<T>& W, const T* theta, int m, int nt, char dir, int chi
 // orthonormal basis of last sweep's kept space next to the optimised theta: for
 // a left-to-right step the right-canonical site B (k x nt, B B^T = 1), for a
 // right-to-left step the left-canonical site A (m x k, A^T A = 1). Three
-// half-steps of block power iteration on theta from that basis, each made
-// orthonormal by one shifted CholeskyQR pass and one plain pass (the last one by
-// two plain passes), give the kept left (or right) isometry; the other factor
-// is its projection of theta, so the split is exact for the kept subspace and its
-// discarded weight is |theta|^2 - |kept|^2:
-//   'R': U1 = qr(theta B^T), V1 = qr(theta^T U1), U = qr2(theta V1),
+// half-steps of block power iteration on theta from that basis give the kept
+// left (or right) isometry; the other factor is its projection of theta, so the
+// split is exact for the kept subspace and its discarded weight is
+// |theta|^2 - |kept|^2:
+//   'R': U1 = tri(theta B^T), V1 = tri(theta^T U1), U = tri(theta V1),
 //        left = U, right = U^T theta
-//   'L': V1 = qr(theta^T A), U1 = qr(theta V1), V = qr2(theta^T U1),
+//   'L': V1 = tri(theta^T A), U1 = tri(theta V1), V = tri(theta^T U1),
 //        right = V^T, left = theta V
-// The shifted pass handles kept singular values down to ~1e-12 of the largest; a
-// pivot of a plain pass below 1e-14 of the largest diagonal entry (an input that
-// is not of full rank k) makes it give up, and the caller runs the exact split.
+// tri = unit columns, then one CholeskyQR pass (Gram matrix, its Cholesky factor
+// inverted in one cluster kernel, then Z L^{-T} on the tensor cores). Why that is
+// enough: the basis a step starts from is orthonormal, ordered by decreasing
+// singular value and close to the Schmidt basis of the bond (the exact split
+// returns Schmidt vectors, and each later warm split keeps that), so each product
+// has nearly orthogonal columns whose norms are the singular values; their spread
+// (up to ~1e9 at chi = 256) is all of its condition number, and unit columns leave a
+// condition number near 1 (measured 1.0-4.6 on Heisenberg, J1-J2 and Josephson
+// chains), for which one CholeskyQR pass is orthonormal to ~25 u. The orthonormal
+// factor must be triangular in the columns: it removes from each column the
+// larger-singular-value directions that leaked into it and nothing else, which
+// keeps the basis aligned with the Schmidt vectors. (A polar factor, e.g. from
+// Newton-Schulz, rotates columns into each other by the leak, and the next power
+// step amplifies that rotation by the singular-value ratios.) The final basis then
+// gets Newton-Schulz steps to rounding (a rotation of order 1e-14 at most). A pivot
+// below 1e-10 of the largest (a product that is not of full rank k, or a state that
+// moved too far for a warm start) makes the split give up, and the caller runs the
+// exact split of the bond.
 // ============================================================================
 struct WstWork {
   double* Ya = nullptr;  // qmax x kmax
   double* Yb = nullptr;
-  double* G = nullptr;   // np x np, np = chol_padded(kmax)
-  double* rd = nullptr;  // np
+  double* Yc = nullptr;  // qmax x kmax, the other half of each Newton-Schulz step
+  double* S = nullptr;   // kmax x kmax Gram matrix (padded to chol_padded(kmax) rows)
+  double* Xi = nullptr;  // kmax x kmax inverse Cholesky factor
+  double* rd = nullptr;  // reciprocal pivots (orders above 256)
+  double* ws = nullptr;  // split-K partial products: 8 x qmax x kmax
   double* nrm = nullptr; // |theta|^2, |kept factor|^2
+  double* part = nullptr;
+  unsigned* counter = nullptr;
   int* status = nullptr;
-  double* h_buf = nullptr;  // pinned: status (as double), |theta|^2, |kept|^2
-  int qmax = 0, kmax = 0, np = 0;
+  SvdOut* out = nullptr;    // k and the Newton-Schulz convergence flag
+  double* h_buf = nullptr;  // pinned: |theta|^2, |kept|^2
+  SvdOut* h_out = nullptr;  // pinned
+  int* h_status = nullptr;  // pinned
+  int qmax = 0, kmax = 0;
   size_t bytes = 0;
   std::vector<void*> owned;
 
@@ -269,20 +293,34 @@ struct WstWork {
   void init(int qmax_, int kmax_) {
     qmax = std::max(qmax_, 1);
     kmax = std::max(std::min(kmax_, CHOL_MAX), 1);
-    np = chol_padded(kmax);
-    Ya = (double*)alloc(sizeof(double) * (size_t)qmax * kmax);
-    Yb = (double*)alloc(sizeof(double) * (size_t)qmax * kmax);
-    G = (double*)alloc(sizeof(double) * (size_t)np * np);
-    rd = (double*)alloc(sizeof(double) * (size_t)np);
+    const size_t qk = (size_t)qmax * kmax;
+    Ya = (double*)alloc(sizeof(double) * qk);
+    Yb = (double*)alloc(sizeof(double) * qk);
+    Yc = (double*)alloc(sizeof(double) * qk);
+    const size_t np = (size_t)chol_padded(kmax);
+    S = (double*)alloc(sizeof(double) * np * np);
+    Xi = (double*)alloc(sizeof(double) * (size_t)kmax * kmax);
+    rd = (double*)alloc(sizeof(double) * np);
+    ws = (double*)alloc(sizeof(double) * 8 * qk);
     nrm = (double*)alloc(sizeof(double) * 4);
+    part = (double*)alloc(sizeof(double) * 64);
+    counter = (unsigned*)alloc(sizeof(unsigned) * 4);
     status = (int*)alloc(sizeof(int) * 4);
+    out = (SvdOut*)alloc(sizeof(SvdOut));
+    DMRG2_CUDA(cudaMemset(counter, 0, sizeof(unsigned) * 4));
     DMRG2_CUDA(cudaMallocHost(&h_buf, sizeof(double) * 4));
+    DMRG2_CUDA(cudaMallocHost(&h_out, sizeof(SvdOut)));
+    DMRG2_CUDA(cudaMallocHost(&h_status, sizeof(int)));
   }
   void release() {
     for (void* p : owned) cudaFree(p);
     owned.clear();
     if (h_buf) cudaFreeHost(h_buf);
+    if (h_out) cudaFreeHost(h_out);
+    if (h_status) cudaFreeHost(h_status);
     h_buf = nullptr;
+    h_out = nullptr;
+    h_status = nullptr;
   }
 };
 
@@ -291,80 +329,131 @@ inline size_t wst_bytes(ll qmax, ll kmax) {
   qmax = std::max<ll>(qmax, 1);
   kmax = std::max<ll>(std::min<ll>(kmax, CHOL_MAX), 1);
   const ll np = chol_padded((int)kmax);
-  return sizeof(double) * (size_t)(2 * qmax * kmax + np * np + np + 4) + sizeof(int) * 4;
+  return sizeof(double) * (size_t)(11 * qmax * kmax + np * np + kmax * kmax + np + 4 + 64) +
+         sizeof(unsigned) * 4 + sizeof(int) * 4 + sizeof(SvdOut);
 }
 
-// Y (rows x k) <- Y R^{-1} with R^T R = Y^T Y (+ shift): one shifted CholeskyQR pass,
-// which leaves a basis of the same span with condition number ~1/sqrt(shift) (a
-// well-conditioned start for the next power step), and `plain` CholeskyQR passes after
-// it, which make the basis orthonormal to rounding.
-inline void wst_qr(WstWork& W, double* Y, ll rows, int k, int plain, cudaStream_t s) {
-  const double u = 1.1102230246251565e-16;
-  const double shift_rel = 11.0 * ((double)rows * k + (double)k * (k + 1)) * u;
-  for (int it = 0; it <= plain; ++it) {
-    Gemm<double> g;  // G = Y^T Y
-    g.ta = true;
-    g.M = k; g.N = k; g.K = (int)rows;
-    g.A = Y; g.lda = k;
-    g.B = Y; g.ldb = k;
-    g.C = W.G; g.ldc = W.np;
-    launch_gemm(g, s);
-    chol_factor(W.G, k, W.np, W.rd, W.status, it == 0 ? 1e-300 : 1e-14, s, it == 0 ? shift_rel : 0.0);
-    chol_solve_rows(Y, rows, k, k, W.G, W.np, W.rd, W.status, s);
-  }
+// DMRG2_DEBUG_WARM=1: the warm split prints each orthonormalisation's outcome to stderr
+inline bool wst_debug() {
+  static const bool on = [] {
+    const char* e = std::getenv("DMRG2_DEBUG_WARM");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+
+// K split so that a GEMM with few output tiles still spreads over the GPU
+inline int wst_splitk(int M, int N, int K) {
+  const int tiles = ceil_div(M, GemmTile<double>::BM) * ceil_div(N, GemmTile<double>::BN);
+  int sk = 1;
+  while (sk < 8 && tiles * sk < 148 && K / (2 * sk) >= 64) sk *= 2;
+  return sk;
 }
 
 // Warm-started split of theta (m x nt) at kept rank k; `warm` is B (k x nt) for 'R',
 // A (m x k) for 'L'. Writes left (m x k) and right (k x nt) and returns true, or returns
-// false (left / right undefined) when CholeskyQR gave up. The host waits once.
+// false (left / right undefined) when the warm start was not good enough. The host
+// waits once.
 inline bool wst_split(WstWork& W, RedScratch& red, const double* theta, int m, int nt, char dir, int k,
                       const double* warm, double* left, double* right, double& trunc_err, cudaStream_t s) {
   if (k > W.kmax || m > W.qmax || nt > W.qmax) throw std::runtime_error("wst_split: workspace too small");
   DMRG2_CUDA(cudaMemsetAsync(W.status, 0, sizeof(int), s));
-  auto mul = [&](bool ta, const double* A, ll lda, int M, int Kd, const double* B, ll ldb, bool tb, double* C) {
-    Gemm<double> g;  // C (M x k) = op(A) op(B)
+  {
+    SvdOut o0{};
+    o0.k = k;
+    *W.h_out = o0;
+    DMRG2_CUDA(cudaMemcpyAsync(W.out, W.h_out, sizeof(SvdOut), cudaMemcpyHostToDevice, s));
+  }
+  // C (M x N) = alpha op(A) op(B) + beta C, K split over CTAs when the output is small
+  auto mul = [&](bool ta, const double* A, ll lda, int M, int N, int Kd, const double* B, ll ldb, bool tb,
+                 double* C, ll ldc, double alpha, double beta, const int* skip) {
+    Gemm<double> g;
     g.ta = ta; g.tb = tb;
-    g.M = M; g.N = k; g.K = Kd;
+    g.M = M; g.N = N; g.K = Kd;
     g.A = A; g.lda = lda;
     g.B = B; g.ldb = ldb;
-    g.C = C; g.ldc = k;
+    g.C = C; g.ldc = ldc;
+    g.alpha = alpha; g.beta = beta;
+    g.skip = skip;
+    g.splitk = wst_splitk(M, N, Kd);
+    g.ws = W.ws;
     launch_gemm(g, s);
   };
+  const int* done = &W.out->ns_done;
+  // Newton-Schulz polish of the nearly orthonormal Z (rows x k): S = Z^T Z, stop once
+  // |S - 1| < tol, Z <- 1.5 Z - 0.5 Z S (iterations after convergence only launch
+  // kernels that return); a run that ends unconverged marks the split as failed. The
+  // result is left in dst.
+  auto orth = [&](double* Z, ll rows, double tol, int iters, double* dst) {
+    DMRG2_CUDA(cudaMemsetAsync(&W.out->ns_done, 0, sizeof(int), s));
+    double* a = Z;
+    double* b = (Z == W.Yc) ? dst : W.Yc;
+    for (int it = 0; it < iters; ++it) {
+      mul(true, a, k, k, k, (int)rows, a, k, false, W.S, k, 1.0, 0.0, done);
+      ns_check(W.S, k, W.out, tol, W.part, W.counter, s);
+      DMRG2_CUDA(cudaMemcpyAsync(b, a, sizeof(double) * (size_t)rows * k, cudaMemcpyDeviceToDevice, s));
+      mul(false, a, k, (int)rows, k, k, W.S, k, false, b, k, -0.5, 1.5, done);
+      std::swap(a, b);
+    }
+    mark_unconverged(W.out, W.status, s);
+    if (a != dst) DMRG2_CUDA(cudaMemcpyAsync(dst, a, sizeof(double) * (size_t)rows * k, cudaMemcpyDeviceToDevice, s));
+    if (wst_debug()) {
+      DMRG2_CUDA(cudaMemcpyAsync(W.h_out, W.out, sizeof(SvdOut), cudaMemcpyDeviceToHost, s));
+      DMRG2_CUDA(cudaMemcpyAsync(W.h_status, W.status, sizeof(int), cudaMemcpyDeviceToHost, s));
+      std::vector<double> hs((size_t)k * k);
+      DMRG2_CUDA(cudaMemcpyAsync(hs.data(), W.S, sizeof(double) * hs.size(), cudaMemcpyDeviceToHost, s));
+      DMRG2_CUDA(cudaStreamSynchronize(s));
+      double e = 0.0;
+      for (int i = 0; i < k; ++i)
+        for (int j = 0; j < k; ++j) e = std::max(e, std::fabs(hs[(size_t)i * k + j] - (i == j ? 1.0 : 0.0)));
+      std::fprintf(stderr, "[warm split] orth rows=%lld k=%d tol=%.1e done=%d status=%d last |S-1|=%.3e\n",
+                   (long long)rows, k, tol, W.h_out->ns_done, *W.h_status, e);
+    }
+  };
+  // Z (rows x k) <- tri(Z) into dst (dst != Z): unit columns, Gram matrix, L^{-1}, Z L^{-T}
+  const int ldS = chol_padded(k);
+  auto tri = [&](double* Z, ll rows, double* dst) {
+    col_normalize(Z, rows, k, W.status, s);
+    mul(true, Z, k, k, k, (int)rows, Z, k, false, W.S, ldS, 1.0, 0.0, nullptr);
+    if (k <= CHOL_INV_MAX) {
+      chol_inverse(W.S, k, ldS, W.Xi, k, W.status, 1e-10, 0.0, s);
+      mul(false, Z, k, (int)rows, k, k, W.Xi, k, true, dst, k, 1.0, 0.0, nullptr);
+    } else {
+      chol_factor(W.S, k, ldS, W.rd, W.status, 1e-10, s);
+      chol_solve_rows(Z, rows, k, k, W.S, ldS, W.rd, W.status, s);
+      DMRG2_CUDA(cudaMemcpyAsync(dst, Z, sizeof(double) * (size_t)rows * k, cudaMemcpyDeviceToDevice, s));
+    }
+  };
   if (dir == 'R') {
-    mul(false, theta, nt, m, nt, warm, nt, true, W.Ya);  // theta B^T
-    wst_qr(W, W.Ya, m, k, 1, s);
-    mul(true, theta, nt, nt, m, W.Ya, k, false, W.Yb);   // theta^T U1
-    wst_qr(W, W.Yb, nt, k, 1, s);
-    mul(false, theta, nt, m, nt, W.Yb, k, false, left);  // theta V1
-    wst_qr(W, left, m, k, 2, s);
-    Gemm<double> g;  // right = U^T theta
-    g.ta = true;
-    g.M = k; g.N = nt; g.K = m;
-    g.A = left; g.lda = k;
-    g.B = theta; g.ldb = nt;
-    g.C = right; g.ldc = nt;
-    launch_gemm(g, s);
+    mul(false, theta, nt, m, k, nt, warm, nt, true, W.Ya, k, 1.0, 0.0, nullptr);  // theta B^T
+    tri(W.Ya, m, W.Yb);
+    mul(true, theta, nt, nt, k, m, W.Yb, k, false, W.Ya, k, 1.0, 0.0, nullptr);   // theta^T U1
+    tri(W.Ya, nt, W.Yb);
+    mul(false, theta, nt, m, k, nt, W.Yb, k, false, W.Ya, k, 1.0, 0.0, nullptr);  // theta V1
+    tri(W.Ya, m, W.Yb);
+    orth(W.Yb, m, 4e-16 * (double)m, 3, left);                                     // polish
+    mul(true, left, k, k, nt, m, theta, nt, false, right, nt, 1.0, 0.0, nullptr);  // right = U^T theta
     norm2(right, (ll)k * nt, W.nrm + 1, red, s);
   } else {
-    mul(true, theta, nt, nt, m, warm, k, false, W.Ya);   // theta^T A
-    wst_qr(W, W.Ya, nt, k, 1, s);
-    mul(false, theta, nt, m, nt, W.Ya, k, false, W.Yb);  // theta V1
-    wst_qr(W, W.Yb, m, k, 1, s);
-    mul(true, theta, nt, nt, m, W.Yb, k, false, W.Ya);   // theta^T U1
-    wst_qr(W, W.Ya, nt, k, 2, s);
-    transpose(W.Ya, right, (ll)nt, (ll)k, s);            // right = V^T
-    mul(false, theta, nt, m, nt, W.Ya, k, false, left);  // left = theta V
+    mul(true, theta, nt, nt, k, m, warm, k, false, W.Ya, k, 1.0, 0.0, nullptr);   // theta^T A
+    tri(W.Ya, nt, W.Yb);
+    mul(false, theta, nt, m, k, nt, W.Yb, k, false, W.Ya, k, 1.0, 0.0, nullptr);  // theta V1
+    tri(W.Ya, m, W.Yb);
+    mul(true, theta, nt, nt, k, m, W.Yb, k, false, W.Ya, k, 1.0, 0.0, nullptr);   // theta^T U1
+    tri(W.Ya, nt, W.Yb);
+    orth(W.Yb, nt, 4e-16 * (double)nt, 3, W.Ya);                                   // polish; V in Ya
+    transpose(W.Ya, right, (ll)nt, (ll)k, s);                                      // right = V^T
+    mul(false, theta, nt, m, k, nt, W.Ya, k, false, left, k, 1.0, 0.0, nullptr);   // left = theta V
     norm2(left, (ll)m * k, W.nrm + 1, red, s);
   }
   norm2(theta, (ll)m * nt, W.nrm, red, s);
   DMRG2_CUDA(cudaMemcpyAsync(W.h_buf + 1, W.nrm, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
-  int st = 0;
-  DMRG2_CUDA(cudaMemcpyAsync(W.h_buf, W.status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  DMRG2_CUDA(cudaMemcpyAsync(W.h_out, W.out, sizeof(SvdOut), cudaMemcpyDeviceToHost, s));
+  DMRG2_CUDA(cudaMemcpyAsync(W.h_status, W.status, sizeof(int), cudaMemcpyDeviceToHost, s));
   DMRG2_CUDA(cudaStreamSynchronize(s));
-  std::memcpy(&st, W.h_buf, sizeof(int));
-  if (st) return false;
-  trunc_err = std::max(W.h_buf[1] - W.h_buf[2], 0.0);
+  if (*W.h_status) return false;
   if (!std::isfinite(W.h_buf[1]) || !std::isfinite(W.h_buf[2])) return false;
+  trunc_err = std::max(W.h_buf[1] - W.h_buf[2], 0.0);
   return true;
 }
 

@@ -78,10 +78,13 @@ typedef struct dmrg2_config {
                          dmrg-gpu driver (gpu-rocm/dmrg-gpu/src/dmrg_gpu_impl.h:1119-1450):
                          bond dimensions stay at those of the initial MPS (or shrink) */
   int truncation;     /* 0 = warm-started subspace split (default): on a sweep that repeats
-                         the previous sweep's bond cap, real data, cap <= 512, the kept space
-                         comes from three CholeskyQR-orthonormalised power steps on theta from
-                         the MPS factor next to it, exact for that space; any other bond, or one
-                         where CholeskyQR gives up, takes the exact split of svd_method.
+                         the previous sweep's bond cap, real data, cap <= 512, a bond keeps
+                         its dimension and the kept space comes from three power steps on theta
+                         from the MPS factor next to it (column-scaled, orthonormalised by
+                         CholeskyQR), exact for that space; the first sweep at a cap, a bond
+                         below the cap whose discarded weight exceeds the exact split's
+                         threshold, or one where CholeskyQR gives up, takes the exact split of
+                         svd_method.
                          1 = the exact split on every bond */
 } dmrg2_config;
 
@@ -105,6 +108,8 @@ typedef struct dmrg2_sweep_report {
   long long lowprec_matvecs; /* precision form: matvecs on the split-BF16 operator */
   int warm_splits;           /* bonds split by the warm-started subspace truncation */
   int warm_fallbacks;        /* bonds where it gave up and the exact split ran */
+  int eig_fallbacks;         /* bonds whose density-matrix eigenvectors could not be made
+                                orthonormal, split by the one-sided Jacobi SVD instead */
 } dmrg2_sweep_report;
 
 /* ---------------------------------------------------------------- solver */

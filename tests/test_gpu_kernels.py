@@ -346,8 +346,10 @@ def test_warm_split_vs_numpy(m, n, k, direction):
 def test_warm_split_wide_kept_spectrum(direction):
     """Kept singular values spanning 1 .. 1e-9 (a DMRG bond at a large bond cap keeps
     Schmidt values far below 1e-6 of the largest): the shifted CholeskyQR pass keeps the
-    split on the warm path (no fallback) and the kept factor still spans the top-k
-    singular space to 1e-9 and is orthonormal to 1e-13."""
+    split on the warm path (no fallback), the kept factor is orthonormal to 1e-13 and
+    spans the top-k singular space to 1e-6 (rounding fixes the directions of singular
+    values near 1e-9 only to ~u/1e-9 ~ 1e-7, for an exact SVD as well), and the
+    discarded weight matches to 1e-12 of |M|^2."""
     rng = np.random.default_rng(11)
     m = n = 512
     k = 256
@@ -362,10 +364,10 @@ def test_warm_split_wide_kept_spectrum(direction):
     left, right, te = dmrg2.warm_split(M, warm, k, direction)
     if direction == "R":
         np.testing.assert_allclose(left.T @ left, np.eye(k), atol=1e-13)
-        assert np.abs(left @ left.T - U[:, :k] @ U[:, :k].T).max() < 1e-9
+        assert np.abs(left @ left.T - U[:, :k] @ U[:, :k].T).max() < 1e-6
     else:
         np.testing.assert_allclose(right @ right.T, np.eye(k), atol=1e-13)
-        assert np.abs(right.T @ right - V[:, :k] @ V[:, :k].T).max() < 1e-9
+        assert np.abs(right.T @ right - V[:, :k] @ V[:, :k].T).max() < 1e-6
     assert abs(te - np.sum(s[k:] ** 2)) <= 1e-12 * np.sum(s ** 2)
 
 
