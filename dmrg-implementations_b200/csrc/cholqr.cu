@@ -484,35 +484,52 @@ __global__ void __launch_bounds__(ST_THREADS)
 }
 
 // every column of Y (rows x k, ld k) scaled to unit norm; a zero or non-finite column
-// sets *status. One CTA per 32 columns (lane = column, warps stride the rows).
-__global__ void __launch_bounds__(256) col_normalize_kernel(double* __restrict__ Y, ll rows, int k,
-                                                            int* __restrict__ status) {
-  __shared__ double part[8][33];
-  __shared__ double inv[32];
+// sets *status. Two passes over a grid of 32-column x CN_ROWS-row blocks: partial
+// sums of squares per block (lane = column, warps stride the rows), then every block
+// adds the partials of its columns and scales its rows.
+constexpr int CN_ROWS = 32;
+__global__ void __launch_bounds__(256) col_sumsq_kernel(const double* __restrict__ Y, ll rows, int k,
+                                                        double* __restrict__ part) {
+  __shared__ double ps[8][33];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int c = blockIdx.x * 32 + lane;
+  const ll r0 = (ll)blockIdx.y * CN_ROWS, r1 = min(rows, r0 + CN_ROWS);
   double sq = 0.0;
   if (c < k)
-    for (ll r = warp; r < rows; r += 8) {
+    for (ll r = r0 + warp; r < r1; r += 8) {
       const double v = Y[r * k + c];
       sq += v * v;
     }
-  part[warp][lane] = sq;
+  ps[warp][lane] = sq;
   __syncthreads();
-  if (warp == 0) {
+  if (warp == 0 && c < k) {
     double t = 0.0;
 #pragma unroll
-    for (int w = 0; w < 8; ++w) t += part[w][lane];
+    for (int w = 0; w < 8; ++w) t += ps[w][lane];
+    part[(ll)blockIdx.y * k + c] = t;
+  }
+}
+
+__global__ void __launch_bounds__(256) col_scale_kernel(double* __restrict__ Y, ll rows, int k,
+                                                        const double* __restrict__ part, int nchunks,
+                                                        int* __restrict__ status) {
+  __shared__ double inv[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int c = blockIdx.x * 32 + lane;
+  if (warp == 0) {
     double sc = 0.0;
     if (c < k) {
+      double t = 0.0;
+      for (int q = 0; q < nchunks; ++q) t += part[(ll)q * k + c];  // the same order in every block
       if (t > 0.0 && isfinite(t)) sc = rsqrt(t);
-      else atomicExch(status, 1);
+      else if (blockIdx.y == 0) atomicExch(status, 1);
     }
     inv[lane] = sc;
   }
   __syncthreads();
+  const ll r0 = (ll)blockIdx.y * CN_ROWS, r1 = min(rows, r0 + CN_ROWS);
   if (c < k)
-    for (ll r = warp; r < rows; r += 8) Y[r * k + c] *= inv[lane];
+    for (ll r = r0 + warp; r < r1; r += 8) Y[r * k + c] *= inv[lane];
 }
 
 __global__ void mark_unconverged_kernel(const SvdOut* out, int* status) {
@@ -526,9 +543,14 @@ void mark_unconverged(const SvdOut* out, int* status, cudaStream_t s) {
   DMRG2_CHECK_LAUNCH();
 }
 
-void col_normalize(double* Y, ll rows, int k, int* status, cudaStream_t s) {
+void col_normalize(double* Y, ll rows, int k, double* part, int* status, cudaStream_t s) {
   if (rows < 1 || k < 1) return;
-  col_normalize_kernel<<<(unsigned)((k + 31) / 32), 256, 0, s>>>(Y, rows, k, status);
+  const ll nch = (rows + CN_ROWS - 1) / CN_ROWS;
+  if (nch > COLNORM_MAX_CHUNKS) throw std::invalid_argument("col_normalize: too many rows");
+  dim3 g((unsigned)((k + 31) / 32), (unsigned)nch);
+  col_sumsq_kernel<<<g, 256, 0, s>>>(Y, rows, k, part);
+  DMRG2_CHECK_LAUNCH();
+  col_scale_kernel<<<g, 256, 0, s>>>(Y, rows, k, part, (int)nch, status);
   DMRG2_CHECK_LAUNCH();
 }
 

@@ -36,8 +36,10 @@ void chol_inverse(const double* G, int k, ll ldg, double* X, ll ldx, int* status
 void mark_unconverged(const SvdOut* out, int* status, cudaStream_t s);
 
 // every column of the rows x k row-major Y scaled to unit norm (*status = 1 on a zero
-// or non-finite column)
-void col_normalize(double* Y, ll rows, int k, int* status, cudaStream_t s);
+// or non-finite column); part holds COLNORM_MAX_CHUNKS x k doubles of partial sums
+// (rows <= 32 COLNORM_MAX_CHUNKS)
+constexpr int COLNORM_MAX_CHUNKS = 64;
+void col_normalize(double* Y, ll rows, int k, double* part, int* status, cudaStream_t s);
 
 // Y <- Y L^{-T} in place for the m x k row-major Y (ldy): the orthonormal factor of
 // CholeskyQR when L L^T = Y^T Y. L and rdiag as chol_factor left them.

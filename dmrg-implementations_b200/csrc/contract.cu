@@ -155,6 +155,21 @@ double env_flops(int ci, int co, int d, int Dl, int Dr, bool cplx) {
   return cplx ? 4.0 * f : f;
 }
 
+// split the K range of an environment GEMM over CTAs when its output tiles do not fill
+// the GPU, with ws (room for ws_elems elements) as the partial-product workspace
+template <typename T>
+static void env_splitk(Gemm<T>& g, ll ws_elems, T* ws) {
+  const int tiles = ceil_div(g.M, GemmTile<T>::BM) * ceil_div(g.N, GemmTile<T>::BN);
+  int sk = 1;
+  while (sk < 8 && tiles * sk < 148 && (ll)g.K / (2 * sk) >= 4 * GemmTile<T>::BK &&
+         (ll)(2 * sk) * g.M * g.N <= ws_elems)
+    sk *= 2;
+  if (sk > 1) {
+    g.splitk = sk;
+    g.ws = ws;
+  }
+}
+
 template <typename T>
 void env_left(const T* Lenv, const T* A, const T* WmixL, T* Lnew, T* X, T* Y, int cL, int cO, int d,
               int Dl, int Dr, cudaStream_t s) {
@@ -182,6 +197,9 @@ void env_left(const T* Lenv, const T* A, const T* WmixL, T* Lnew, T* X, T* Y, in
     g.A = A; g.lda = cO;
     g.B = Y; g.ldb = (ll)Dr * cO;
     g.C = Lnew; g.ldc = (ll)Dr * cO;
+    // K split when the output tiles cannot fill the GPU; X (free again) holds the
+    // cL Dl d cO products of step 1
+    env_splitk(g, (ll)cL * Dl * d * cO, X);
     launch_gemm(g, s);
   }
 }
@@ -215,17 +233,20 @@ void env_right(const T* Renv, const T* B, const T* WmixR, T* Rnew, T* X, T* Y, i
     g.A = B; g.lda = (ll)d * cI;
     g.B = Y; g.ldb = (ll)Dl * cO;
     g.C = Rnew; g.ldc = (ll)Dl * cO;
+    env_splitk(g, (ll)cI * Dr * d * cO, X);  // X holds the cI Dr d cO products of step 1
     launch_gemm(g, s);
   }
 }
 
 template <typename T>
-void theta_form(const T* A, const T* B, T* theta, int cL, int cM, int cR, int d, cudaStream_t s) {
+void theta_form(const T* A, const T* B, T* theta, int cL, int cM, int cR, int d, cudaStream_t s, T* ws,
+                ll ws_elems) {
   Gemm<T> g;
   g.M = cL * d; g.N = d * cR; g.K = cM;
   g.A = A; g.lda = cM;
   g.B = B; g.ldb = (ll)d * cR;
   g.C = theta; g.ldc = (ll)d * cR;
+  if (ws) env_splitk(g, ws_elems, ws);
   launch_gemm(g, s);
 }
 
@@ -287,7 +308,7 @@ void build_wmix_right(const T* W, int Dl, int Dr, int d, std::vector<T>& out) {
                             cudaStream_t);                                                       \
   template void env_right<T>(const T*, const T*, const T*, T*, T*, T*, int, int, int, int, int, \
                              cudaStream_t);                                                      \
-  template void theta_form<T>(const T*, const T*, T*, int, int, int, int, cudaStream_t);         \
+  template void theta_form<T>(const T*, const T*, T*, int, int, int, int, cudaStream_t, T*, ll); \
   template void build_wwt<T>(const T*, const T*, int, int, int, int, std::vector<T>&);          \
   template void build_wmix_left<T>(const T*, int, int, int, std::vector<T>&);                   \
   template void build_wmix_right<T>(const T*, int, int, int, std::vector<T>&);

@@ -57,7 +57,9 @@ void env_right(const T* Renv, const T* B, const T* WmixR, T* Rnew, T* X, T* Y, i
 
 // theta = A_i . A_{i+1} (reference: form_theta_two_site, dmrg2_gpu_impl.h:583-600)
 template <typename T>
-void theta_form(const T* A, const T* B, T* theta, int cL, int cM, int cR, int d, cudaStream_t s);
+// theta = A B; ws (ws_elems elements, optional) lets a GEMM with few output tiles split K
+void theta_form(const T* A, const T* B, T* theta, int cL, int cM, int cR, int d, cudaStream_t s, T* ws = nullptr,
+                ll ws_elems = 0);
 
 // host-side MPO preprocessing (reference: set_mpo / precompute_fused_mpo, dmrg2_gpu_impl.h:436-576)
 template <typename T>

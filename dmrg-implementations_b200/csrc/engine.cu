@@ -224,6 +224,7 @@ class Engine final : public EngineBase {
     }
     X_ = carve(xs);
     Y_ = carve(xs);
+    xs_ = xs;
     mpo_set_ = true;
     envs_valid_ = false;
   }
@@ -477,7 +478,7 @@ class Engine final : public EngineBase {
   double optimize_bond(int i, char dir, int chi, SweepStats& ss) {
     const int cL = dims_[i], cM = dims_[i + 1], cR = dims_[i + 2];
     const ll n = (ll)cL * d_ * d_ * cR;
-    theta_form(mps_[i], mps_[i + 1], theta_, cL, cM, cR, d_, st_);
+    theta_form(mps_[i], mps_[i + 1], theta_, cL, cM, cR, d_, st_, X_, xs_);
     double e = lanczos(i, n, ss);
     svd_split(i, dir, chi, ss);
     if (dir == 'R')
@@ -721,6 +722,7 @@ class Engine final : public EngineBase {
   void* mpo_slab_ = nullptr;  // every MPO-dependent buffer (mixing matrices, environments, scratch)
   size_t bytes_ = 0, bytes_mpo_ = 0;
   ll nmax_ = 0, qmax_ = 0;
+  ll xs_ = 0;  // elements of each contraction scratch buffer X_, Y_
   bool mpo_set_ = false, mps_set_ = false, canonical_ = false;
   double energy_ = 0.0, env_build_s_ = 0.0;
 };

@@ -270,6 +270,7 @@ struct WstWork {
   double* S = nullptr;   // kmax x kmax Gram matrix (padded to chol_padded(kmax) rows)
   double* Xi = nullptr;  // kmax x kmax inverse Cholesky factor
   double* rd = nullptr;  // reciprocal pivots (orders above 256)
+  double* cpart = nullptr;  // column sums of squares per row chunk
   double* ws = nullptr;  // split-K partial products: 8 x qmax x kmax
   double* nrm = nullptr; // |theta|^2, |kept factor|^2
   double* part = nullptr;
@@ -301,6 +302,7 @@ struct WstWork {
     S = (double*)alloc(sizeof(double) * np * np);
     Xi = (double*)alloc(sizeof(double) * (size_t)kmax * kmax);
     rd = (double*)alloc(sizeof(double) * np);
+    cpart = (double*)alloc(sizeof(double) * (size_t)COLNORM_MAX_CHUNKS * kmax);
     ws = (double*)alloc(sizeof(double) * 8 * qk);
     nrm = (double*)alloc(sizeof(double) * 4);
     part = (double*)alloc(sizeof(double) * 64);
@@ -329,7 +331,7 @@ inline size_t wst_bytes(ll qmax, ll kmax) {
   qmax = std::max<ll>(qmax, 1);
   kmax = std::max<ll>(std::min<ll>(kmax, CHOL_MAX), 1);
   const ll np = chol_padded((int)kmax);
-  return sizeof(double) * (size_t)(11 * qmax * kmax + np * np + kmax * kmax + np + 4 + 64) +
+  return sizeof(double) * (size_t)(11 * qmax * kmax + np * np + kmax * kmax + np + COLNORM_MAX_CHUNKS * kmax + 4 + 64) +
          sizeof(unsigned) * 4 + sizeof(int) * 4 + sizeof(SvdOut);
 }
 
@@ -357,6 +359,7 @@ inline int wst_splitk(int M, int N, int K) {
 inline bool wst_split(WstWork& W, RedScratch& red, const double* theta, int m, int nt, char dir, int k,
                       const double* warm, double* left, double* right, double& trunc_err, cudaStream_t s) {
   if (k > W.kmax || m > W.qmax || nt > W.qmax) throw std::runtime_error("wst_split: workspace too small");
+  if (std::max(m, nt) > 32 * COLNORM_MAX_CHUNKS) return false;  // beyond the column-scaling kernel
   DMRG2_CUDA(cudaMemsetAsync(W.status, 0, sizeof(int), s));
   {
     SvdOut o0{};
@@ -413,7 +416,7 @@ inline bool wst_split(WstWork& W, RedScratch& red, const double* theta, int m, i
   // Z (rows x k) <- tri(Z) into dst (dst != Z): unit columns, Gram matrix, L^{-1}, Z L^{-T}
   const int ldS = chol_padded(k);
   auto tri = [&](double* Z, ll rows, double* dst) {
-    col_normalize(Z, rows, k, W.status, s);
+    col_normalize(Z, rows, k, W.cpart, W.status, s);
     mul(true, Z, k, k, k, (int)rows, Z, k, false, W.S, ldS, 1.0, 0.0, nullptr);
     if (k <= CHOL_INV_MAX) {
       chol_inverse(W.S, k, ldS, W.Xi, k, W.status, 1e-10, 0.0, s);

@@ -3,14 +3,22 @@
     python -m dmrg2.microbench heff --chi 256 [--d 2 --D 5 --complex --reps 50]
     python -m dmrg2.microbench svd  --n 512   [--keep 256 --complex --reps 5]
     python -m dmrg2.microbench gemm --m 1024 --n 4096 --k 1024 [--complex --reps 5]
+    python -m dmrg2.microbench lanczos --chi 256 [--reps 3]
+    python -m dmrg2.microbench env  --chi 256 [--reps 10]
+    python -m dmrg2.microbench warm --n 512 [--keep 256 --reps 3]
 
 heff runs dmrg2_op_heff_noalloc on device-resident operands (torch tensors)
 and reports the device time per matvec (CUDA events) and its algorithmic
 TFLOP/s; svd runs the truncated split through dmrg2_op_svd (host buffers,
 so the time includes the copies); gemm runs the FP64 DMMA GEMM and the
 split-BF16 tcgen05 GEMM of the precision form on the same operands (host
-buffers) and reports their difference. They are the fixed small workloads the
-kernel profiles are taken on.
+buffers) and reports their difference. lanczos runs the
+device Lanczos solver (dmrg2_op_lanczos: H_eff matvecs and the fused Krylov
+vector passes) on a Heisenberg two-site problem with seeded Hermitian
+environments; env runs one left environment update; warm runs the
+warm-started subspace split (dmrg2_op_warm_split) of a matrix with a decaying
+spectrum from a perturbed copy of its kept right singular vectors. They are the
+fixed small workloads the kernel profiles are taken on.
 """
 from __future__ import annotations
 
@@ -98,9 +106,62 @@ def bench_gemm(m, n, k, cplx, reps, seed=0):
             "max_abs_diff": float(err), "flops": (8.0 if cplx else 2.0) * m * n * k}
 
 
+def _heis_w(D=5):
+    W = np.zeros((D, D, 2, 2))
+    sz = np.diag([0.5, -0.5])
+    sp = np.array([[0.0, 1.0], [0.0, 0.0]])
+    I = np.eye(2)
+    W[0, 0], W[0, 1], W[0, 2], W[0, 3] = I, 0.5 * sp, 0.5 * sp.T, sz
+    W[1, 4], W[2, 4], W[3, 4], W[4, 4] = sp.T, sp, sz, I
+    return W
+
+
+def _herm_env(rng, chi, D):
+    E = rng.standard_normal((chi, D, chi))
+    return 0.5 * (E + np.transpose(E, (2, 1, 0)))
+
+
+def bench_lanczos(chi, reps, seed=0):
+    rng = np.random.default_rng(seed)
+    W = _heis_w()
+    L, R = _herm_env(rng, chi, 5), _herm_env(rng, chi, 5)
+    th = rng.standard_normal((chi, 2, 2, chi))
+    times = []
+    for _ in range(reps + 1):
+        t = time.perf_counter()
+        e, _ = dmrg2.optimize_two_site(L, R, W, W, th, max_iter=30, tol=1e-12, max_restarts=0)
+        times.append(time.perf_counter() - t)
+    return {"op": "lanczos", "chi": chi, "energy": e, "ms_per_call_host": 1e3 * float(np.median(times[1:]))}
+
+
+def bench_env(chi, reps, seed=0):
+    rng = np.random.default_rng(seed)
+    L = _herm_env(rng, chi, 5)
+    A = rng.standard_normal((chi, 2, chi))
+    t = time.perf_counter()
+    for _ in range(reps):
+        dmrg2.update_left_env(L, A, _heis_w())
+    return {"op": "env", "chi": chi, "ms_per_call_host": 1e3 * (time.perf_counter() - t) / reps}
+
+
+def bench_warm(n, keep, reps, seed=1):
+    rng = np.random.default_rng(seed)
+    U, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    V, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    s = np.concatenate([np.logspace(0, -7, keep), 1e-8 * np.logspace(0, -3, n - keep)])
+    M = (U * s) @ V.T
+    warm = np.linalg.qr(V[:, :keep] + 1e-4 * rng.standard_normal((n, keep)))[0].T.copy()
+    times = []
+    for _ in range(reps + 1):
+        t = time.perf_counter()
+        _, _, te = dmrg2.warm_split(M, warm, keep, "R")
+        times.append(time.perf_counter() - t)
+    return {"op": "warm", "n": n, "keep": keep, "trunc_err": te, "ms_per_call_host": 1e3 * float(np.median(times[1:]))}
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("op", choices=["heff", "svd", "gemm"])
+    ap.add_argument("op", choices=["heff", "svd", "gemm", "lanczos", "env", "warm"])
     ap.add_argument("--m", type=int, default=1024)
     ap.add_argument("--k", type=int, default=1024)
     ap.add_argument("--chi", type=int, default=256)
@@ -116,6 +177,13 @@ def main():
     elif a.op == "svd":
         n = a.n or 512
         r = bench_svd(n, a.keep or n // 2, a.complex, a.reps or 5)
+    elif a.op == "lanczos":
+        r = bench_lanczos(a.chi, a.reps or 3)
+    elif a.op == "env":
+        r = bench_env(a.chi, a.reps or 10)
+    elif a.op == "warm":
+        n = a.n or 512
+        r = bench_warm(n, a.keep or n // 2, a.reps or 3)
     else:
         r = bench_gemm(a.m, a.n or 4096, a.k, a.complex, a.reps or 5)
     print(json.dumps(r))
