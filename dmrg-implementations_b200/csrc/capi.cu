@@ -521,6 +521,7 @@ static void fill_reports(const std::vector<SweepStats>& st, dmrg2_sweep_report* 
     r.lowprec_matvecs = st[s].lowprec_matvecs;
     r.warm_splits = st[s].warm_splits;
     r.warm_fallbacks = st[s].warm_fallbacks;
+    r.warm_short = st[s].warm_short;
     r.eig_fallbacks = st[s].eig_fallbacks;
   }
 }

@@ -55,6 +55,7 @@ class Engine final : public EngineBase {
       throw std::invalid_argument("single-site sweeps use the density-matrix truncation and FP64 matvecs");
     L_ = cfg_.L;
     d_ = cfg_.d;
+    reset_split_history();
     DMRG2_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
     cap_.resize(L_ + 1);
     for (int i = 0; i <= L_; ++i) cap_[i] = (int)ipow_cap(d_, std::min(i, L_ - i), cfg_.chi_max);
@@ -247,7 +248,7 @@ class Engine final : public EngineBase {
     mps_set_ = true;
     canonical_ = false;
     envs_valid_ = false;
-    prev_sweep_chi_ = 0;
+    reset_split_history();
   }
 
   void get_mps(std::vector<void*>& out) override {
@@ -266,7 +267,7 @@ class Engine final : public EngineBase {
       if (c < 1 || c > cfg_.chi_max) throw std::runtime_error("run: schedule chi outside [1, chi_max]");
     auto t0 = std::chrono::steady_clock::now();
     right_canonicalize();
-    prev_sweep_chi_ = 0;
+    reset_split_history();
     build_right_envs();
     DMRG2_CUDA(cudaStreamSynchronize(st_));
     env_build_s_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -607,6 +608,12 @@ class Engine final : public EngineBase {
     ss.trunc_err_sum += o.trunc_err;
   }
 
+  void reset_split_history() {
+    prev_sweep_chi_ = 0;
+    te_ref_.assign((size_t)std::max(L_ - 1, 0), -1.0);
+    short_age_.assign((size_t)std::max(L_ - 1, 0), 0);
+  }
+
   // the warm-started split applies on a sweep that repeats the previous sweep's bond cap
   // (not in the first sweep at a new cap, where the state still moves far); it keeps the
   // bond's dimension k (the factor next to theta is an orthonormal basis of a
@@ -627,6 +634,17 @@ class Engine final : public EngineBase {
     return te <= (double)(std::min(m, nc) - k) * thr;
   }
 
+  // One power half-step from the warm factor is kept when its discarded weight is within
+  // WARM_SHORT_SLACK of the weight the last full split of this bond (three half-steps,
+  // or the exact split) discarded, plus the rounding floor of |theta|^2 - |kept|^2; a
+  // short split can therefore never discard more than that reference, which only full
+  // splits set. At most WARM_SHORT_RUN short splits of a bond follow one full split.
+  static constexpr double WARM_SHORT_SLACK = 1e-3;
+  static constexpr int WARM_SHORT_RUN = 3;
+  bool warm_short_accepts(int i, double te, double fro2) const {
+    return te <= te_ref_[i] * (1.0 + WARM_SHORT_SLACK) + 64.0 * 2.220446049250313e-16 * fro2;
+  }
+
   void svd_split(int i, char dir, int chi, SweepStats& ss) {
     const int cL = dims_[i], cR = dims_[i + 2];
     const ll m = (ll)cL * d_, nc = (ll)d_ * cR;
@@ -636,14 +654,41 @@ class Engine final : public EngineBase {
         double te = 0.0;
         const double* warm = (dir == 'R') ? mps_[i + 1] : mps_[i];
         const int k = dims_[i + 1];
-        if (wst_split(wst_, red_, theta_, (int)m, (int)nc, dir, k, warm, mps_[i], mps_[i + 1], te, st_) &&
-            warm_split_keeps_rank(k, chi, m, nc, te, wst_.h_buf[1])) {
+        auto split = [&](WstMode mode) {
+          return wst_split(wst_, red_, theta_, (int)m, (int)nc, dir, k, warm, mps_[i], mps_[i + 1], te, st_, mode) &&
+                 warm_split_keeps_rank(k, chi, m, nc, te, wst_.h_buf[1]);
+        };
+        bool ok = false, short_kept = false;
+        if (te_ref_[i] >= 0.0 && short_age_[i] < WARM_SHORT_RUN) {
+          if (split(WST_SHORT)) {
+            const double te_short = te;
+            short_kept = warm_short_accepts(i, te, wst_.h_buf[1]);
+            ok = short_kept;
+            if (!short_kept || wst_debug()) {
+              ok = split(WST_RESUME);  // the two remaining half-steps on the same theta
+              if (wst_debug())
+                std::fprintf(stderr, "[warm short] bond %d %c k=%d te_short=%.6e te_full=%.6e te_ref=%.6e kept=%d\n",
+                             i, dir, k, te_short, te, te_ref_[i], (int)short_kept);
+              short_kept = short_kept && !wst_debug();
+            }
+          }
+        } else {
+          ok = split(WST_FULL);
+        }
+        if (ok) {
           DMRG2_CUDA(cudaEventRecord(ev_d_, st_));
           DMRG2_CUDA(cudaEventSynchronize(ev_d_));
           float ms = 0.f;
           DMRG2_CUDA(cudaEventElapsedTime(&ms, ev_c_, ev_d_));
           ss.svd_s += ms * 1e-3;
           ss.warm_splits += 1;
+          if (short_kept) {
+            ss.warm_short += 1;
+            short_age_[i] += 1;
+          } else {
+            te_ref_[i] = te;
+            short_age_[i] = 0;
+          }
           ss.trunc_err_max = std::max(ss.trunc_err_max, te);
           ss.trunc_err_sum += te;
           return;  // dims_[i + 1] unchanged
@@ -691,6 +736,8 @@ class Engine final : public EngineBase {
     dims_[i + 1] = o.k;
     ss.trunc_err_max = std::max(ss.trunc_err_max, o.trunc_err);
     ss.trunc_err_sum += o.trunc_err;
+    te_ref_[i] = o.trunc_err;
+    short_age_[i] = 0;
   }
 
   // ---------------------------------------------------------------- state
@@ -706,6 +753,8 @@ class Engine final : public EngineBase {
   EigWork<T> ew_;
   WstWork wst_;                 // warm-started subspace split (real data)
   int prev_sweep_chi_ = 0;      // bond cap of the last completed sweep (0: none since the last set-up)
+  std::vector<double> te_ref_;  // per bond: weight discarded by its last full split (< 0: none yet)
+  std::vector<int> short_age_;  // per bond: short warm splits since that full split
   double* sigma_ = nullptr;
   int* perm_ = nullptr;
   SvdOut* svdout_ = nullptr;

@@ -52,6 +52,7 @@ struct SweepStats {
   long long lowprec_matvecs = 0;  // precision form: matvecs on the split-BF16 operator
   int warm_splits = 0;       // bonds split by the warm-started subspace truncation
   int warm_fallbacks = 0;    // bonds where it gave up and the exact split ran
+  int warm_short = 0;        // warm splits kept after one power half-step
   int eig_fallbacks = 0;     // bonds where the density-matrix eigenvectors could not be made
                              // orthonormal and the Jacobi SVD split the bond
 };

@@ -352,12 +352,22 @@ inline int wst_splitk(int M, int N, int K) {
   return sk;
 }
 
+// How many power half-steps a warm split runs:
+//   WST_FULL   three, from the warm factor (the scheme above);
+//   WST_SHORT  one, from the warm factor: left = tri(theta B^T) ('R'), right^T =
+//              tri(theta^T A) ('L'), each polished and the other factor projected;
+//   WST_RESUME the two after a WST_SHORT call on the same theta, starting from the
+//              basis that call left (in `left` for 'R', in W.Ya for 'L'); together they
+//              are WST_FULL.
+enum WstMode { WST_FULL = 0, WST_SHORT = 1, WST_RESUME = 2 };
+
 // Warm-started split of theta (m x nt) at kept rank k; `warm` is B (k x nt) for 'R',
 // A (m x k) for 'L'. Writes left (m x k) and right (k x nt) and returns true, or returns
 // false (left / right undefined) when the warm start was not good enough. The host
 // waits once.
 inline bool wst_split(WstWork& W, RedScratch& red, const double* theta, int m, int nt, char dir, int k,
-                      const double* warm, double* left, double* right, double& trunc_err, cudaStream_t s) {
+                      const double* warm, double* left, double* right, double& trunc_err, cudaStream_t s,
+                      WstMode mode = WST_FULL) {
   if (k > W.kmax || m > W.qmax || nt > W.qmax) throw std::runtime_error("wst_split: workspace too small");
   if (std::max(m, nt) > 32 * COLNORM_MAX_CHUNKS) return false;  // beyond the column-scaling kernel
   DMRG2_CUDA(cudaMemsetAsync(W.status, 0, sizeof(int), s));
@@ -428,22 +438,34 @@ inline bool wst_split(WstWork& W, RedScratch& red, const double* theta, int m, i
     }
   };
   if (dir == 'R') {
-    mul(false, theta, nt, m, k, nt, warm, nt, true, W.Ya, k, 1.0, 0.0, nullptr);  // theta B^T
-    tri(W.Ya, m, W.Yb);
-    mul(true, theta, nt, nt, k, m, W.Yb, k, false, W.Ya, k, 1.0, 0.0, nullptr);   // theta^T U1
-    tri(W.Ya, nt, W.Yb);
-    mul(false, theta, nt, m, k, nt, W.Yb, k, false, W.Ya, k, 1.0, 0.0, nullptr);  // theta V1
-    tri(W.Ya, m, W.Yb);
+    if (mode != WST_RESUME) {
+      mul(false, theta, nt, m, k, nt, warm, nt, true, W.Ya, k, 1.0, 0.0, nullptr);  // theta B^T
+      tri(W.Ya, m, W.Yb);
+    } else {
+      DMRG2_CUDA(cudaMemcpyAsync(W.Yb, left, sizeof(double) * (size_t)m * k, cudaMemcpyDeviceToDevice, s));  // U1
+    }
+    if (mode != WST_SHORT) {
+      mul(true, theta, nt, nt, k, m, W.Yb, k, false, W.Ya, k, 1.0, 0.0, nullptr);  // theta^T U1
+      tri(W.Ya, nt, W.Yb);
+      mul(false, theta, nt, m, k, nt, W.Yb, k, false, W.Ya, k, 1.0, 0.0, nullptr); // theta V1
+      tri(W.Ya, m, W.Yb);
+    }
     orth(W.Yb, m, 4e-16 * (double)m, 3, left);                                     // polish
     mul(true, left, k, k, nt, m, theta, nt, false, right, nt, 1.0, 0.0, nullptr);  // right = U^T theta
     norm2(right, (ll)k * nt, W.nrm + 1, red, s);
   } else {
-    mul(true, theta, nt, nt, k, m, warm, k, false, W.Ya, k, 1.0, 0.0, nullptr);   // theta^T A
-    tri(W.Ya, nt, W.Yb);
-    mul(false, theta, nt, m, k, nt, W.Yb, k, false, W.Ya, k, 1.0, 0.0, nullptr);  // theta V1
-    tri(W.Ya, m, W.Yb);
-    mul(true, theta, nt, nt, k, m, W.Yb, k, false, W.Ya, k, 1.0, 0.0, nullptr);   // theta^T U1
-    tri(W.Ya, nt, W.Yb);
+    if (mode != WST_RESUME) {
+      mul(true, theta, nt, nt, k, m, warm, k, false, W.Ya, k, 1.0, 0.0, nullptr);  // theta^T A
+      tri(W.Ya, nt, W.Yb);
+    } else {
+      DMRG2_CUDA(cudaMemcpyAsync(W.Yb, W.Ya, sizeof(double) * (size_t)nt * k, cudaMemcpyDeviceToDevice, s));  // V1
+    }
+    if (mode != WST_SHORT) {
+      mul(false, theta, nt, m, k, nt, W.Yb, k, false, W.Ya, k, 1.0, 0.0, nullptr); // theta V1
+      tri(W.Ya, m, W.Yb);
+      mul(true, theta, nt, nt, k, m, W.Yb, k, false, W.Ya, k, 1.0, 0.0, nullptr);  // theta^T U1
+      tri(W.Ya, nt, W.Yb);
+    }
     orth(W.Yb, nt, 4e-16 * (double)nt, 3, W.Ya);                                   // polish; V in Ya
     transpose(W.Ya, right, (ll)nt, (ll)k, s);                                      // right = V^T
     mul(false, theta, nt, m, k, nt, W.Ya, k, false, left, k, 1.0, 0.0, nullptr);   // left = theta V

@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define DMRG2_ABI_VERSION 3
+#define DMRG2_ABI_VERSION 4
 
 enum dmrg2_status {
   DMRG2_OK = 0,
@@ -110,6 +110,7 @@ typedef struct dmrg2_sweep_report {
   int warm_fallbacks;        /* bonds where it gave up and the exact split ran */
   int eig_fallbacks;         /* bonds whose density-matrix eigenvectors could not be made
                                 orthonormal, split by the one-sided Jacobi SVD instead */
+  int warm_short;            /* warm splits kept after one power half-step (of warm_splits) */
 } dmrg2_sweep_report;
 
 /* ---------------------------------------------------------------- solver */

@@ -289,3 +289,23 @@ def test_warm_split_matches_exact_split_and_oracle():
         a = A[k].reshape(A[k].shape[0], -1)
         np.testing.assert_allclose(a @ a.T, np.eye(a.shape[0]), atol=1e-12)
     assert abs(O.mpo_expectation(A, mpo).real - rw[-1]["energy"]) < 1e-9
+
+
+def test_warm_short_split_on_converged_sweeps():
+    """Converged sweeps at a fixed cap keep most warm splits after one power half-step
+    (warm_short), never discarding more than 1e-3 above the last full split of the bond;
+    the run matches the exact split on every bond (truncation=1) to 1e-10 in energy and
+    1e-8 in the largest discarded weight, sweep by sweep once the cap is reached."""
+    L = 32
+    mpo, mps = M.heisenberg_mpo(L), O.random_mps(L, 2, 16, seed=3)
+    sched = [32, 32, 64, 64] + [64] * 8
+    kw = dict(krylov_max=30, max_restarts=2, cutoff=1e-12, tol=1e-300, min_sweeps=100)
+    ew, rw = gpu_run(mpo, mps, sched, **kw)
+    ex, rx = gpu_run(mpo, mps, sched, truncation=1, **kw)
+    short = [r["warm_short"] for r in rw]
+    print("warm_short per sweep", short, "warm splits", [r["warm_splits"] for r in rw])
+    assert all(r["warm_short"] <= r["warm_splits"] for r in rw)
+    assert sum(short[4:]) >= 2 * (L - 1)
+    for a, b in zip(rw[4:], rx[4:]):
+        assert abs(a["energy"] - b["energy"]) <= 1e-10 * abs(b["energy"])
+        assert abs(a["trunc_err_max"] - b["trunc_err_max"]) <= 1e-8
