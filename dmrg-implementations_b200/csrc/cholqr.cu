@@ -1,30 +1,36 @@
 // CholeskyQR building blocks (real FP64) for the warm-started subspace truncation.
 //
-// chol_cluster_kernel: right-looking blocked Cholesky of a symmetric positive
-// definite matrix of order <= 512 in 32 x 32 tiles, one cluster of 8 CTAs. The
-// matrix stays in global memory (it is L2-resident: 2 MB at most) and is read and
-// written with L2-only accesses, so the cluster barriers (release / acquire at
-// cluster scope) are the only synchronisation. Per tile column p:
-//   D  one warp factors the diagonal tile with register shuffles (the sqrt chain
-//      of the 32 columns is the critical path of the whole factorisation);
-//   P  one warp per sub-diagonal tile solves L_ip L_pp^T = A_ip row by row
-//      (forward substitution, one lane per row);
-//   T  one warp per trailing tile subtracts L_ip L_jp^T.
-// Pivots below rel_tol times the largest diagonal entry mark the matrix as not
-// numerically positive definite (the caller falls back to the exact split).
-// With shift_rel > 0 the matrix factorised is A + shift_rel trace(A) 1: shifted
-// CholeskyQR (Fukaya, Kannan, Nakatsukasa, Yamamoto and Yanagisawa, SIAM J. Sci.
-// Comput. 42 (2020)) takes shift 11 (m k + k (k+1)) u |Y|_F^2 for the Gram matrix
-// A = Y^T Y of an m x k block, which keeps the factorisation stable for any
-// condition number of Y below ~1/u and leaves Y R^{-1} with a condition number
-// of at most ~1/sqrt(shift_rel), so plain CholeskyQR can finish it.
+// chol_tiles_kernel: blocked Cholesky factorisation of an order <= 512 symmetric
+// positive definite matrix in 32 x 32 tiles, in one cluster of C = 8 or 16 CTAs.
+// CTA r owns block row r in its shared memory and turns it into L's block row
+// (right-looking: at tile column t it forms L_rt, then subtracts L_rt L_jt^T from
+// its tiles t < j <= r). There is no cluster barrier inside the factorisation: each
+// CTA publishes how many tiles of its row are final (a counter in its shared memory,
+// written with release semantics after the tiles), and a CTA that needs a peer's
+// tile polls that counter (acquire, bounded) and then reads the tile straight from
+// the peer's shared memory. A published tile is never written again, and nothing is
+// copied asynchronously, so the only exit condition is the final cluster barrier
+// (no CTA leaves while a peer may still read it). Per tile column t:
+//   P  CTA r > t: L_rt = A_rt X_tt^T with X_tt = L_tt^{-1} from CTA t (rows split
+//      over the 8 warps);
+//   T  CTA r > t: A_rj -= L_rt L_jt^T for the peers' tiles t < j < r (one warp per
+//      tile, the peer tile staged in that warp's buffer) and the lower part of the
+//      diagonal tile j = r (rows split over the warps);
+//   D  CTA t, once its row is updated: in-register Cholesky of the diagonal tile
+//      (one warp, lane = row; the chain of pivots is the critical path), then X_tt by
+//      forward substitution (lane = column), then the counter says "row complete".
+// The critical path is one P, one diagonal update and one D per tile column; the
+// wider updates of the rows further down overlap with it. A poll that runs out marks
+// the result invalid (status) and the CTA carries on with what it has, so every CTA
+// reaches the final barrier.
 //
-// chol_solve_rows_kernel: Y <- Y L^{-T}, 8 rows of Y per CTA, tile column by tile
-// column: the update by the finished columns, then the forward substitution
-// with the diagonal tile (one lane per row).
+// trsm_rows_kernel: Y = Z L^{-T}, 16 rows of Z per CTA, column block by column block:
+// Y_b = (Z_b - sum_{j<b} Y_j L_bj^T) X_bb^T on the FP64 tensor cores (DMMA), the tiles
+// of L streamed through shared memory with cp.async double buffering.
 #include <cooperative_groups.h>
 
 #include "cholqr.cuh"
+#include "gemm.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -33,184 +39,33 @@ namespace dmrg2 {
 namespace {
 
 constexpr int NB = CHOL_NB;
-constexpr int CC = 8;    // CTAs in the factorisation cluster
-constexpr int CT = 256;  // threads per CTA (8 warps)
-constexpr int NW = CT / 32;
-constexpr int TP = NB + 1;  // padded tile row in shared memory
+constexpr int TP = NB + 1;           // padded tile row in shared memory (conflict-free columns)
+constexpr int TT = NB * TP;          // doubles per padded tile
+constexpr int CT_THREADS = 256;      // 8 warps
+constexpr int CT_WARPS = CT_THREADS / 32;
+constexpr long long CT_SPIN = 1ll << 22;  // polls of a peer's counter before giving up
 
-__device__ inline double ldg_l2(const double* p) { return __ldcg(p); }
-__device__ inline void stg_l2(double* p, double v) { __stcg(p, v); }
-
-// column J of the in-register Cholesky of one diagonal tile (lane i holds row i), then
-// the columns after it; compile-time J keeps every index of a[] static
-template <int J>
-__device__ __forceinline__ void chol_tile_col(double (&a)[NB], int lane, double piv_min, double piv_sub,
-                                              bool& bad, double* rd) {
-  double piv = __shfl_sync(0xffffffffu, a[J], J);
-  if (!(piv > piv_min)) {  // also catches NaN
-    bad = true;
-    piv = piv_sub;
-  }
-  const double l = sqrt(piv);
-  const double r = 1.0 / l;
-  if (lane == J) {
-    a[J] = l;
-    rd[J] = r;
-  } else if (lane > J) {
-    a[J] *= r;
-  }
-#pragma unroll
-  for (int c = J + 1; c < NB; ++c) {
-    const double lc = __shfl_sync(0xffffffffu, a[J], c);
-    if (lane >= c) a[c] -= a[J] * lc;
-  }
-  if constexpr (J + 1 < NB) chol_tile_col<J + 1>(a, lane, piv_min, piv_sub, bad, rd);
+__device__ inline int ld_acquire_cluster(const int* p) {
+  int v;
+  asm volatile("ld.acquire.cluster.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
 }
-
-__global__ void __launch_bounds__(CT, 1)
-    chol_cluster_kernel(double* __restrict__ A, int k, int np, ll lda, double* __restrict__ rdiag,
-                        int* __restrict__ status, double rel_tol, double shift_rel) {
-  cg::cluster_group cluster = cg::this_cluster();
-  const int rank = (int)cluster.block_rank();
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int nblk = np / NB;
-  extern __shared__ __align__(16) double csm[];
-  double* Lp = csm;                         // L_pp [NB][TP]
-  double* Rp = Lp + NB * TP;                // 1 / diag of L_pp [NB]
-  double* Wt = Rp + NB;                     // per warp: an L_jp tile [NW][NB][TP]
-  __shared__ double dmax_s, shift_s;
-
-  // padding rows r >= k become identity rows (lower triangle only)
-  for (int r = k + rank; r < np; r += CC)
-    for (int c = tid; c <= r; c += CT) stg_l2(A + (ll)r * lda + c, c == r ? 1.0 : 0.0);
-  if (warp == 0) {
-    double m = 0.0, tr = 0.0;
-    for (int i = lane; i < k; i += 32) {
-      const double a = ldg_l2(A + (ll)i * lda + i);
-      m = fmax(m, a);
-      tr += a;
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-      tr += __shfl_xor_sync(0xffffffffu, tr, o);
-    }
-    if (lane == 0) {
-      shift_s = shift_rel * tr;
-      dmax_s = m + shift_s;
-    }
-  }
-  cluster.sync();  // padding written, every CTA has read the unshifted diagonal
-  if (shift_rel > 0.0) {
-    for (int i = rank * CT + tid; i < k; i += CC * CT) stg_l2(A + (ll)i * lda + i, ldg_l2(A + (ll)i * lda + i) + shift_s);
-    cluster.sync();
-  }
-  const double piv_min = rel_tol * dmax_s;
-  const double piv_sub = dmax_s > 0.0 ? dmax_s : 1.0;
-
-  for (int p = 0; p < nblk; ++p) {
-    double* App = A + (ll)(p * NB) * lda + p * NB;
-    // ---- D: diagonal tile, one warp (lane i holds row i)
-    if (rank == p % CC && warp == 0) {
-      double a[NB];
-#pragma unroll
-      for (int j = 0; j < NB; ++j) a[j] = (j <= lane) ? ldg_l2(App + (ll)lane * lda + j) : 0.0;
-      bool bad = false;
-      chol_tile_col<0>(a, lane, piv_min, piv_sub, bad, rdiag + p * NB);
-#pragma unroll
-      for (int j = 0; j < NB; ++j) stg_l2(App + (ll)lane * lda + j, j <= lane ? a[j] : 0.0);
-      if (bad && lane == 0) atomicExch(status, 1);
-    }
-    cluster.sync();
-    if (p + 1 == nblk) break;
-    // ---- P: sub-diagonal tiles of column p
-    const int np_tiles = nblk - p - 1;
-    if (rank < np_tiles) {  // CTAs with a panel tile load L_pp and 1 / diag
-      for (int e = tid; e < NB * NB; e += CT) Lp[(e / NB) * TP + (e % NB)] = ldg_l2(App + (ll)(e / NB) * lda + e % NB);
-      if (tid < NB) Rp[tid] = ldg_l2(rdiag + p * NB + tid);
-    }
-    __syncthreads();
-    for (int g = rank + CC * warp; g < np_tiles; g += CC * NW) {
-      const int i = p + 1 + g;
-      double* Aip = A + (ll)(i * NB) * lda + p * NB;
-      double x[NB];
-#pragma unroll
-      for (int c = 0; c < NB; ++c) x[c] = ldg_l2(Aip + (ll)lane * lda + c);
-#pragma unroll
-      for (int c = 0; c < NB; ++c) {
-        x[c] *= Rp[c];
-#pragma unroll
-        for (int c2 = c + 1; c2 < NB; ++c2) x[c2] -= x[c] * Lp[c2 * TP + c];
-      }
-#pragma unroll
-      for (int c = 0; c < NB; ++c) stg_l2(Aip + (ll)lane * lda + c, x[c]);
-    }
-    cluster.sync();
-    // ---- T: trailing tiles (i, j), p < j <= i, in row order
-    const int nt = np_tiles * (np_tiles + 1) / 2;
-    double* Ww = Wt + warp * NB * TP;
-    for (int g = rank + CC * warp; g < nt; g += CC * NW) {
-      int i = p + 1, rem = g;
-      while (rem >= i - p) {
-        rem -= i - p;
-        ++i;
-      }
-      const int j = p + 1 + rem;
-      const double* Ljp = A + (ll)(j * NB) * lda + p * NB;
-      const double* Lip = A + (ll)(i * NB) * lda + p * NB;
-      double* Aij = A + (ll)(i * NB) * lda + j * NB;
-#pragma unroll 4
-      for (int r = 0; r < NB; ++r) Ww[r * TP + lane] = ldg_l2(Ljp + (ll)r * lda + lane);
-      __syncwarp();
-      double x[NB], acc[NB];
-#pragma unroll
-      for (int t = 0; t < NB; ++t) {
-        x[t] = ldg_l2(Lip + (ll)lane * lda + t);
-        acc[t] = 0.0;
-      }
-#pragma unroll
-      for (int t = 0; t < NB; ++t)
-#pragma unroll
-        for (int c = 0; c < NB; ++c) acc[c] += x[t] * Ww[c * TP + t];
-      const int cmax = (i == j) ? lane : NB - 1;  // the diagonal tile keeps its lower part only
-#pragma unroll
-      for (int c = 0; c < NB; ++c)
-        if (c <= cmax) stg_l2(Aij + (ll)lane * lda + c, ldg_l2(Aij + (ll)lane * lda + c) - acc[c]);
-      __syncwarp();
-    }
-    cluster.sync();
-  }
+__device__ inline void st_release_cluster(int* p, int v) {
+  asm volatile("st.release.cluster.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
-
-// ---------------------------------------------------------------------------
-// cholinv_cluster_kernel: X = L^{-1}, L L^T = G (+ shift), for orders k <= 256, in one
-// cluster of 8 CTAs with every tile in shared memory: CTA r holds block row r of G
-// (turned into L in place) and block row r of X, and stages the tiles it needs from
-// its peers (distributed shared memory) in a third area. Per tile column p:
-//   D  CTA p, warp 0: in-register Cholesky of the diagonal tile (rsqrt, one shuffle
-//      broadcast per column); warp 1 then inverts it into X_pp off the critical path
-//      (after the CTA has arrived at the cluster barrier);
-//   P  CTAs r > p: L_rp = A_rp L_pp^{-T} by forward substitution (lane = row);
-//   T  CTAs r > p: A_rj -= L_rp L_jp^T for p < j <= r (one warp per tile). CTA p+1
-//      owns only tile (p+1, p+1) and factors it right after (look-ahead: no barrier
-//      between its update and the next diagonal factorisation).
-// Then X by tile diagonals s = 1 .. nblk-1: X_{r,r-s} = -X_rr sum_j L_rj X_{j,r-s}
-// (CTA r, its peers' X tiles staged), and each CTA writes its block row of X (zeros
-// above the diagonal) to global memory. Two cluster barriers per tile column and one
-// per tile diagonal; nothing leaves shared memory until the end.
-// ---------------------------------------------------------------------------
-constexpr int CI_MAXB = 8;
-constexpr int CI_THREADS = 256;
-constexpr int CI_TILE = NB * TP;  // doubles per padded tile
-constexpr size_t CI_SMEM = sizeof(double) * (3 * CI_MAXB * CI_TILE + 2 * NB);
-
-__device__ inline void cl_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
-__device__ inline void cl_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
+// true once *peer_done >= need (every calling thread acquires), false after CT_SPIN polls
+__device__ inline bool wait_tiles(const int* peer_done, int need) {
+  for (long long it = 0; it < CT_SPIN; ++it)
+    if (ld_acquire_cluster(peer_done) >= need) return true;
+  return false;
+}
 
 // column J of the in-register Cholesky of one diagonal tile (lane i holds row i) with a
-// reciprocal square root per pivot, then the columns after it
+// reciprocal square root per pivot, then the columns after it; compile-time J keeps
+// every index of a[] static
 template <int J>
-__device__ __forceinline__ void ci_tile_col(double (&a)[NB], int lane, double piv_min, double piv_sub,
-                                            bool& bad, double* rd) {
+__device__ __forceinline__ void tile_chol_col(double (&a)[NB], int lane, double piv_min, double piv_sub, bool& bad,
+                                              double* rd) {
   double piv = __shfl_sync(0xffffffffu, a[J], J);
   if (!(piv > piv_min)) {  // also catches NaN
     bad = true;
@@ -228,25 +83,31 @@ __device__ __forceinline__ void ci_tile_col(double (&a)[NB], int lane, double pi
     const double lc = __shfl_sync(0xffffffffu, a[J], c);
     if (lane >= c) a[c] -= a[J] * lc;
   }
-  if constexpr (J + 1 < NB) ci_tile_col<J + 1>(a, lane, piv_min, piv_sub, bad, rd);
+  if constexpr (J + 1 < NB) tile_chol_col<J + 1>(a, lane, piv_min, piv_sub, bad, rd);
 }
 
-__global__ void __launch_bounds__(CI_THREADS, 1)
-    cholinv_cluster_kernel(const double* __restrict__ G, int k, int np, ll ldg, double* __restrict__ X, ll ldx,
-                           int* __restrict__ status, double rel_tol, double shift_rel) {
+template <int C>
+__global__ void __launch_bounds__(CT_THREADS, 1)
+    chol_tiles_kernel(const double* __restrict__ G, int k, int nb, ll ldg, double* __restrict__ LX, ll ldx,
+                      int* __restrict__ status, double rel_tol, double shift_rel) {
   cg::cluster_group cluster = cg::this_cluster();
   const int r = (int)cluster.block_rank();
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int nblk = np / NB;
-  extern __shared__ __align__(16) double cism[];
-  double* Lt = cism;                           // [CI_MAXB] tiles: block row r of G -> L
-  double* Xt = Lt + CI_MAXB * CI_TILE;         // [CI_MAXB] tiles: block row r of X
-  double* St = Xt + CI_MAXB * CI_TILE;         // [CI_MAXB] staged tiles of peers
-  double* Rd = St + CI_MAXB * CI_TILE;         // 1 / diag of this CTA's L_rr
-  double* Rs = Rd + NB;                        // staged 1 / diag of L_pp
+  extern __shared__ __align__(16) double ctsm[];
+  double* Lt = ctsm;                 // [C] tiles of block row r: A_rj, turned into L_rj
+  double* Xr = Lt + C * TT;          // X_rr = L_rr^{-1} (zeros above the diagonal)
+  double* Xs = Xr + TT;              // X_tt of the tile column being solved, staged
+  double* Ws = Xs + TT;              // [CT_WARPS] a peer's L_jt, staged per warp
+  double* Rd = Ws + CT_WARPS * TT;   // 1 / diag of L_rr
+  __shared__ int done_s;             // tiles of this block row that are final (read by peers)
+  __shared__ int fail_s;
   __shared__ double tr_s, dmax_s;
-  auto T_ = [](double* base, int t) { return base + t * CI_TILE; };
+  auto T_ = [](double* base, int t) { return base + t * TT; };
 
+  if (tid == 0) {
+    done_s = 0;
+    fail_s = 0;
+  }
   // trace and largest diagonal entry of G (every CTA reads them from global memory)
   if (warp == 0) {
     double m = 0.0, tr = 0.0;
@@ -269,9 +130,9 @@ __global__ void __launch_bounds__(CI_THREADS, 1)
   const double piv_min = rel_tol * dmax_s;
   const double piv_sub = dmax_s > 0.0 ? dmax_s : 1.0;
   // block row r of G (+ shift on the diagonal; identity beyond k; lower part of the diagonal tile)
-  if (r < nblk)
+  if (r < nb)
     for (int j = 0; j <= r; ++j)
-      for (int e = tid; e < NB * NB; e += CI_THREADS) {
+      for (int e = tid; e < NB * NB; e += CT_THREADS) {
         const int row = e >> 5, col = e & 31;
         const int gi = r * NB + row, gj = j * NB + col;
         double v;
@@ -279,208 +140,227 @@ __global__ void __launch_bounds__(CI_THREADS, 1)
         else v = (gi == gj) ? 1.0 : 0.0;
         T_(Lt, j)[row * TP + col] = v;
       }
+  // every counter is initialised and every block row read before any CTA polls a peer
+  // or writes LX (which may be the buffer G is in)
   cluster.sync();
 
-  for (int p = 0; p < nblk; ++p) {
-    // ---- D: diagonal tile of CTA p (its tile p, already updated by every earlier column)
-    if (r == p && warp == 0) {
-      double a[NB];
-      double* Lpp = T_(Lt, p);
+  bool bad = false;
+  if (r < nb) {
+    for (int t = 0; t < r; ++t) {
+      // ---- P: L_rt = A_rt X_tt^T once CTA t has published X_tt (its row complete)
+      if (!wait_tiles(cluster.map_shared_rank(&done_s, t), t + 1)) fail_s = 1;
+      {
+        const double* Xp = cluster.map_shared_rank(Xr, t);
+        for (int e = tid; e < NB * NB; e += CT_THREADS) Xs[(e >> 5) * TP + (e & 31)] = Xp[(e >> 5) * TP + (e & 31)];
+      }
+      __syncthreads();
+      {
+        double* Art = T_(Lt, t);
+        double o[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 8
+        for (int s = 0; s < NB; ++s) {
+          const double xv = Xs[lane * TP + s];  // X_tt[c = lane][s]
 #pragma unroll
-      for (int j = 0; j < NB; ++j) a[j] = (j <= lane) ? Lpp[lane * TP + j] : 0.0;
-      bool bad = false;
-      ci_tile_col<0>(a, lane, piv_min, piv_sub, bad, Rd);
+          for (int u = 0; u < 4; ++u) o[u] += Art[(4 * warp + u) * TP + s] * xv;
+        }
+        __syncwarp();  // the warp's rows are read before they are overwritten
 #pragma unroll
-      for (int j = 0; j < NB; ++j) Lpp[lane * TP + j] = (j <= lane) ? a[j] : 0.0;
-      if (bad && lane == 0) atomicExch(status, 1);
+        for (int u = 0; u < 4; ++u) Art[(4 * warp + u) * TP + lane] = o[u];
+      }
+      __syncthreads();
+      if (tid == 0) st_release_cluster(&done_s, t + 1);  // L_rt is final
+      // ---- T: A_rj -= L_rt L_jt^T for t < j <= r
+      const double* Lrt = T_(Lt, t);
+      for (int q = warp; q < r - t - 1; q += CT_WARPS) {  // the peers' tiles j = t+1 .. r-1
+        const int j = t + 1 + q;
+        if (!wait_tiles(cluster.map_shared_rank(&done_s, j), t + 1)) fail_s = 1;
+        const double* src = cluster.map_shared_rank(T_(Lt, t), j);  // L_jt in CTA j
+        double* W = T_(Ws, warp);
+        {
+          double v[NB];
+#pragma unroll
+          for (int c = 0; c < NB; ++c) v[c] = src[c * TP + lane];
+#pragma unroll
+          for (int c = 0; c < NB; ++c) W[c * TP + lane] = v[c];
+        }
+        __syncwarp();
+        double x[NB], acc[NB];  // lane = row i of A_rj: acc[c] = sum_s L_rt[i][s] L_jt[c][s]
+#pragma unroll
+        for (int s = 0; s < NB; ++s) {
+          x[s] = Lrt[lane * TP + s];
+          acc[s] = 0.0;
+        }
+#pragma unroll
+        for (int s = 0; s < NB; ++s)
+#pragma unroll
+          for (int c = 0; c < NB; ++c) acc[c] += x[s] * W[c * TP + s];
+        double* Arj = T_(Lt, j);
+#pragma unroll
+        for (int c = 0; c < NB; ++c) Arj[lane * TP + c] -= acc[c];
+        __syncwarp();  // W is staged again by this warp's next tile
+      }
+      {  // the diagonal tile: rows 4w .. 4w+3, lane = column, lower part only
+        double* Arr = T_(Lt, r);
+        double o[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 8
+        for (int s = 0; s < NB; ++s) {
+          const double lv = Lrt[lane * TP + s];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) o[u] += Lrt[(4 * warp + u) * TP + s] * lv;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (lane <= 4 * warp + u) Arr[(4 * warp + u) * TP + lane] -= o[u];
+      }
+      __syncthreads();  // tile (r, t+1) and the diagonal tile are final for this column
     }
-    __syncthreads();  // L_pp and Rd written before the barrier and before warp 1 reads them
-    cl_arrive();
-    if (r == p && warp == 1) {
-      // X_pp = L_pp^{-1}: lane c forms column c by forward substitution
-      const double* Lpp = T_(Lt, p);
+    // ---- D: L_rr (registers, lane = row), then X_rr = L_rr^{-1} (lane = column)
+    if (warp == 0) {
+      double* Lrr = T_(Lt, r);
+      double a[NB];
+#pragma unroll
+      for (int j = 0; j < NB; ++j) a[j] = (j <= lane) ? Lrr[lane * TP + j] : 0.0;
+      tile_chol_col<0>(a, lane, piv_min, piv_sub, bad, Rd);
+#pragma unroll
+      for (int j = 0; j < NB; ++j) Lrr[lane * TP + j] = (j <= lane) ? a[j] : 0.0;
+      __syncwarp();
       double x[NB];
 #pragma unroll
       for (int i = 0; i < NB; ++i) {
-        double s = (i == lane) ? 1.0 : 0.0;
+        // four partial sums break the dependent chain of the row's dot product
+        double s0 = (i == lane) ? 1.0 : 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
 #pragma unroll
-        for (int j = 0; j < i; ++j) s -= Lpp[i * TP + j] * x[j];
-        x[i] = s * Rd[i];
-      }
-#pragma unroll
-      for (int i = 0; i < NB; ++i) T_(Xt, p)[i * TP + lane] = x[i];
-    }
-    cl_wait();
-    // ---- P: L_rp = A_rp L_pp^{-T}
-    if (r > p && r < nblk) {
-      const double* Rpp = cluster.map_shared_rank(T_(Lt, p), p);
-      const double* Rrd = cluster.map_shared_rank(Rd, p);
-      for (int e = tid; e < NB * NB; e += CI_THREADS) St[(e >> 5) * TP + (e & 31)] = Rpp[(e >> 5) * TP + (e & 31)];
-      if (tid < NB) Rs[tid] = Rrd[tid];
-      __syncthreads();
-      if (warp == 0) {
-        double* Arp = T_(Lt, p);
-        double x[NB];
-#pragma unroll
-        for (int c = 0; c < NB; ++c) x[c] = Arp[lane * TP + c];
-#pragma unroll
-        for (int c = 0; c < NB; ++c) {
-          x[c] *= Rs[c];
-#pragma unroll
-          for (int c2 = c + 1; c2 < NB; ++c2) x[c2] -= x[c] * St[c2 * TP + c];
+        for (int j = 0; j + 3 < i; j += 4) {
+          s0 -= Lrr[i * TP + j] * x[j];
+          s1 -= Lrr[i * TP + j + 1] * x[j + 1];
+          s2 -= Lrr[i * TP + j + 2] * x[j + 2];
+          s3 -= Lrr[i * TP + j + 3] * x[j + 3];
         }
 #pragma unroll
-        for (int c = 0; c < NB; ++c) Arp[lane * TP + c] = x[c];
+        for (int j = i & ~3; j < i; ++j) s0 -= Lrr[i * TP + j] * x[j];
+        x[i] = ((s0 + s1) + (s2 + s3)) * Rd[i];
       }
+#pragma unroll
+      for (int i = 0; i < NB; ++i) Xr[i * TP + lane] = x[i];
     }
-    cluster.sync();  // every L_rp of this column is final
-    // ---- T: A_rj -= L_rp L_jp^T, p < j <= r
-    if (r > p && r < nblk) {
-      for (int j = p + 1; j < r; ++j) {  // peers' L_jp into staging slot j
-        const double* src = cluster.map_shared_rank(T_(Lt, p), j);
-        for (int e = tid; e < NB * NB; e += CI_THREADS) T_(St, j)[(e >> 5) * TP + (e & 31)] = src[(e >> 5) * TP + (e & 31)];
-      }
-      __syncthreads();
-      const int j = p + 1 + warp;
-      if (j <= r) {
-        const double* Ljp = (j == r) ? T_(Lt, p) : T_(St, j);
-        const double* Lrp = T_(Lt, p);
-        double x[NB], acc[NB];
-#pragma unroll
-        for (int t = 0; t < NB; ++t) {
-          x[t] = Lrp[lane * TP + t];
-          acc[t] = 0.0;
-        }
-#pragma unroll
-        for (int t = 0; t < NB; ++t)
-#pragma unroll
-          for (int c = 0; c < NB; ++c) acc[c] += x[t] * Ljp[c * TP + t];
-        double* Arj = T_(Lt, j);
-        const int cmax = (j == r) ? lane : NB - 1;
-#pragma unroll
-        for (int c = 0; c < NB; ++c)
-          if (c <= cmax) Arj[lane * TP + c] -= acc[c];
-      }
-      __syncthreads();  // staging reused by the next column; tile (r, p+1) final before D / P
+    __syncthreads();
+    if (tid == 0) st_release_cluster(&done_s, r + 1);  // the whole row, X_rr included
+    // ---- block row r of LX: L_rj below the diagonal, X_rr on it
+    for (int j = 0; j <= r; ++j) {
+      const double* src = (j < r) ? T_(Lt, j) : Xr;
+      for (int e = tid; e < NB * NB; e += CT_THREADS)
+        LX[(ll)(r * NB + (e >> 5)) * ldx + j * NB + (e & 31)] = src[(e >> 5) * TP + (e & 31)];
     }
   }
-  cluster.sync();  // every X_pp is written
-  // ---- X below the diagonal, one tile diagonal at a time
-  for (int s = 1; s < nblk; ++s) {
-    if (r >= s && r < nblk) {
-      const int q = r - s;
-      for (int j = q; j < r; ++j) {  // X_{j,q} of CTA j into staging slot j - q
-        const double* src = cluster.map_shared_rank(T_(Xt, q), j);
-        for (int e = tid; e < NB * NB; e += CI_THREADS) T_(St, j - q)[(e >> 5) * TP + (e & 31)] = src[(e >> 5) * TP + (e & 31)];
-      }
-      __syncthreads();
-      // W = sum_j L_rj X_jq: warp w rows 4w..4w+3, lane = column
-      double w4[4] = {0.0, 0.0, 0.0, 0.0};
-      for (int j = q; j < r; ++j) {
-        const double* Lrj = T_(Lt, j);
-        const double* Xjq = T_(St, j - q);
-#pragma unroll 8
-        for (int t = 0; t < NB; ++t) {
-          const double xv = Xjq[t * TP + lane];
-#pragma unroll
-          for (int u = 0; u < 4; ++u) w4[u] += Lrj[(4 * warp + u) * TP + t] * xv;
-        }
-      }
-      double* Wt = T_(St, CI_MAXB - 1);  // free: at most 7 tiles are staged
-#pragma unroll
-      for (int u = 0; u < 4; ++u) Wt[(4 * warp + u) * TP + lane] = w4[u];
-      __syncthreads();
-      // X_rq = -X_rr W
-      const double* Xrr = T_(Xt, r);
-      double o4[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll 8
-      for (int t = 0; t < NB; ++t) {
-        const double wv = Wt[t * TP + lane];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) o4[u] -= Xrr[(4 * warp + u) * TP + t] * wv;
-      }
-#pragma unroll
-      for (int u = 0; u < 4; ++u) T_(Xt, q)[(4 * warp + u) * TP + lane] = o4[u];
-    }
-    cluster.sync();  // X tiles of this diagonal visible to the peers
-  }
-  // ---- block row r of X to global memory (lower triangle, zeros above)
-  if (r < nblk)
-    for (int j = 0; j < nblk; ++j)
-      for (int e = tid; e < NB * NB; e += CI_THREADS) {
-        const int row = e >> 5, col = e & 31;
-        const int gi = r * NB + row, gj = j * NB + col;
-        if (gi < k && gj < k) X[(ll)gi * ldx + gj] = (j < r || (j == r && col <= row)) ? T_(Xt, j)[row * TP + col] : 0.0;
-      }
+  if (bad) atomicExch(status, 1);
   cluster.sync();  // no CTA leaves while a peer may still read its shared memory
+  if (tid == 0 && fail_s) atomicExch(status, 1);
 }
 
-constexpr int SR = 8;        // rows of Y per CTA in the solve
-constexpr int ST_THREADS = 64;
+// ---------------------------------------------------------------------------
+// trsm_rows_kernel
+// ---------------------------------------------------------------------------
+constexpr int TR_R = 16;                     // rows of Z per CTA (one DMMA row block)
+constexpr int TR_THREADS = 128;              // warp w: output columns 8w .. 8w+7 of a block
+constexpr int TR_LP = NB + 4;                // staged tile row: 288 bytes (16-byte aligned rows)
+constexpr int TR_TILE = NB * TR_LP;
 
-__global__ void __launch_bounds__(ST_THREADS)
-    chol_solve_rows_kernel(double* __restrict__ Y, ll m, int k, int np, ll ldy, const double* __restrict__ L,
-                           ll lda, const double* __restrict__ rdiag, const int* __restrict__ status) {
+__device__ inline void tr_stage(double* dst, const double* LX, ll ldx, int b, int j, int tid) {
+  // tile (b, j) of LX: 32 rows x 32 doubles = 512 chunks of 16 bytes, four per thread
+#pragma unroll
+  for (int h = 0; h < 4; ++h) {
+    const int e = tid + h * TR_THREADS;
+    const int row = e >> 4, c2 = (e & 15) * 2;
+    cp_async_16(dst + row * TR_LP + c2, LX + (ll)(b * NB + row) * ldx + j * NB + c2, true);
+  }
+}
+
+__global__ void __launch_bounds__(TR_THREADS)
+    trsm_rows_kernel(const double* __restrict__ Z, ll rows, int k, int nb, const double* __restrict__ LX, ll ldx,
+                     double* __restrict__ Y, const int* __restrict__ status) {
   if (*((volatile const int*)status)) return;  // the factor is not valid: the caller falls back
-  extern __shared__ __align__(16) double ssm[];
-  double* Qs = ssm;                // [SR][np + 1]: finished columns of these rows
-  double* Lt = Qs + SR * (np + 1);  // one L tile [NB][TP]
-  double* Us = Lt + NB * TP;       // updated block [SR][TP]
+  extern __shared__ __align__(16) double tsm[];
+  const int YP = nb * NB + 4;     // row of the finished blocks
+  double* Yf = tsm;               // [TR_R][YP]: Y of this CTA's rows, block by block
+  double* Lb = Yf + TR_R * YP;    // [2][TR_TILE]: staged tiles
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const ll r0 = (ll)blockIdx.x * SR;
-  const int nrows = (int)min((ll)SR, m - r0);
-  const int nblk = np / NB;
-  const int QP = np + 1;
-  for (int p = 0; p < nblk; ++p) {
-    // this block of Y (columns >= k are zero)
-    double acc[SR / 2];
-#pragma unroll
-    for (int q = 0; q < SR / 2; ++q) {
-      const int r = warp * (SR / 2) + q;
-      const int c = p * NB + lane;
-      acc[q] = (r < nrows && c < k) ? Y[(r0 + r) * ldy + c] : 0.0;
+  const int gq = lane >> 2, tq = lane & 3;
+  const ll r0 = (ll)blockIdx.x * TR_R;
+  const int ntiles = nb * (nb + 1) / 2;  // (b, j) for j <= b, in that order
+  // tile s of the sequence -> (b, j)
+  auto tile_of = [](int s, int& b, int& j) {
+    b = 0;
+    while (s > b) {
+      s -= b + 1;
+      ++b;
     }
-    // minus the finished columns times L_pj^T
-    for (int j = 0; j < p; ++j) {
-      __syncthreads();
-      for (int e = tid; e < NB * NB; e += ST_THREADS)
-        Lt[(e / NB) * TP + (e % NB)] = __ldg(L + (ll)(p * NB + e / NB) * lda + j * NB + e % NB);
-      __syncthreads();
-#pragma unroll 8
-      for (int t = 0; t < NB; ++t) {
-        const double l = Lt[lane * TP + t];  // L[p*NB + lane][j*NB + t]
+    j = s;
+  };
+  {
+    int b, j;
+    tile_of(0, b, j);
+    tr_stage(Lb, LX, ldx, b, j, tid);
+    cp_async_commit();
+  }
+  int s = 0;
+  for (int b = 0; b < nb; ++b) {
+    const int c0 = b * NB + warp * 8 + 2 * tq;  // this lane's two output columns
+    double acc[4];
 #pragma unroll
-        for (int q = 0; q < SR / 2; ++q) acc[q] -= Qs[(warp * (SR / 2) + q) * QP + j * NB + t] * l;
+    for (int q = 0; q < 4; ++q) {
+      const ll row = r0 + gq + ((q & 2) ? 8 : 0);
+      const int col = c0 + (q & 1);
+      acc[q] = (row < rows && col < k) ? Z[row * k + col] : 0.0;
+    }
+    for (int j = 0; j <= b; ++j, ++s) {
+      if (j == b) {
+        // the update of block b is complete: store it for the X_bb product (no warp
+        // reads block b of Yf before the barrier below)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) Yf[(gq + ((q & 2) ? 8 : 0)) * YP + c0 + (q & 1)] = acc[q];
       }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < SR / 2; ++q) Us[(warp * (SR / 2) + q) * TP + lane] = acc[q];
-    for (int e = tid; e < NB * NB; e += ST_THREADS)
-      Lt[(e / NB) * TP + (e % NB)] = __ldg(L + (ll)(p * NB + e / NB) * lda + p * NB + e % NB);
-    __syncthreads();
-    // forward substitution with L_pp, one thread per row
-    if (tid < SR) {
-      double x[NB];
-#pragma unroll
-      for (int c = 0; c < NB; ++c) x[c] = Us[tid * TP + c];
-#pragma unroll
-      for (int c = 0; c < NB; ++c) {
-        x[c] *= __ldg(rdiag + p * NB + c);
-#pragma unroll
-        for (int c2 = c + 1; c2 < NB; ++c2) x[c2] -= x[c] * Lt[c2 * TP + c];
+      if (s + 1 < ntiles) {  // prefetch the next tile into the other buffer
+        int bn, jn;
+        tile_of(s + 1, bn, jn);
+        tr_stage(Lb + ((s + 1) & 1) * TR_TILE, LX, ldx, bn, jn, tid);
       }
+      cp_async_commit();
+      cp_async_wait<1>();
+      __syncthreads();  // tile s staged (and, for j == b, the updated block in Yf)
+      const double* Lt = Lb + (s & 1) * TR_TILE;
+      if (j < b) {
+        // acc -= Y_j L_bj^T: A = Y_j (16 x 32), B[kk][n] = L_bj[n][kk]
 #pragma unroll
-      for (int c = 0; c < NB; ++c) Qs[tid * QP + p * NB + c] = x[c];
-    }
-    __syncthreads();
+        for (int kk = 0; kk < NB; kk += 4) {
+          const double a0 = -Yf[gq * YP + j * NB + kk + tq];
+          const double a1 = -Yf[(gq + 8) * YP + j * NB + kk + tq];
+          const double b0 = Lt[(warp * 8 + gq) * TR_LP + kk + tq];
+          dmma16x8x4(acc, a0, a1, b0);
+        }
+      } else {
+        // Y_b = (Z_b - ...) X_bb^T: the updated block is in Yf (written before the
+        // barrier above), the product goes to registers, then back to Yf and Y
+        double out[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-    for (int q = 0; q < SR / 2; ++q) {
-      const int r = warp * (SR / 2) + q;
-      const int c = p * NB + lane;
-      if (r < nrows && c < k) Y[(r0 + r) * ldy + c] = Qs[r * QP + c];
+        for (int kk = 0; kk < NB; kk += 4) {
+          const double a0 = Yf[gq * YP + b * NB + kk + tq];
+          const double a1 = Yf[(gq + 8) * YP + b * NB + kk + tq];
+          const double b0 = Lt[(warp * 8 + gq) * TR_LP + kk + tq];
+          dmma16x8x4(out, a0, a1, b0);
+        }
+        __syncthreads();  // every warp has read the updated block
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int rr = gq + ((q & 2) ? 8 : 0);
+          const int col = c0 + (q & 1);
+          Yf[rr * YP + col] = out[q];
+          if (r0 + rr < rows && col < k) Y[(r0 + rr) * k + col] = out[q];
+        }
+      }
+      __syncthreads();  // buffer s & 1 is free for the prefetch of tile s + 2
     }
   }
+  cp_async_wait<0>();
 }
 
 // every column of Y (rows x k, ld k) scaled to unit norm; a zero or non-finite column
@@ -536,6 +416,32 @@ __global__ void mark_unconverged_kernel(const SvdOut* out, int* status) {
   if (!out->ns_done) *status = 1;
 }
 
+template <int C>
+void chol_tiles_launch(const double* G, int k, int nb, ll ldg, double* LX, ll ldx, int* status, double rel_tol,
+                       double shift_rel, cudaStream_t s) {
+  constexpr size_t smem = sizeof(double) * ((size_t)(C + 2 + CT_WARPS) * TT + NB);
+  static std::atomic<unsigned long long> attr{0};
+  set_smem_attr_once(attr, (const void*)chol_tiles_kernel<C>, (int)smem);
+  if constexpr (C > 8) {
+    static std::atomic<unsigned long long> attr_c{0};
+    func_attr_once(attr_c, (const void*)chol_tiles_kernel<C>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(C);
+  cfg.blockDim = dim3(CT_THREADS);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = C;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  DMRG2_CUDA(cudaLaunchKernelEx(&cfg, chol_tiles_kernel<C>, G, k, nb, ldg, LX, ldx, status, rel_tol, shift_rel));
+  DMRG2_CHECK_LAUNCH();
+}
+
 }  // namespace
 
 void mark_unconverged(const SvdOut* out, int* status, cudaStream_t s) {
@@ -554,63 +460,30 @@ void col_normalize(double* Y, ll rows, int k, double* part, int* status, cudaStr
   DMRG2_CHECK_LAUNCH();
 }
 
-void chol_inverse(const double* G, int k, ll ldg, double* X, ll ldx, int* status, double rel_tol, double shift_rel,
-                  cudaStream_t s) {
+void chol_tiles(const double* G, int k, ll ldg, double* LX, ll ldx, int* status, double rel_tol, double shift_rel,
+                cudaStream_t s) {
   const int np = chol_padded(k);
-  if (k < 1 || np > CI_MAXB * NB) throw std::invalid_argument("chol_inverse: order outside 1..256");
-  static std::atomic<unsigned long long> attr{0};
-  set_smem_attr_once(attr, (const void*)cholinv_cluster_kernel, (int)CI_SMEM);
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(CI_MAXB);
-  cfg.blockDim = dim3(CI_THREADS);
-  cfg.dynamicSmemBytes = CI_SMEM;
-  cfg.stream = s;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeClusterDimension;
-  at[0].val.clusterDim.x = CI_MAXB;
-  at[0].val.clusterDim.y = 1;
-  at[0].val.clusterDim.z = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = 1;
-  DMRG2_CUDA(cudaLaunchKernelEx(&cfg, cholinv_cluster_kernel, G, k, np, ldg, X, ldx, status, rel_tol, shift_rel));
-  DMRG2_CHECK_LAUNCH();
+  if (k < 1 || np > CHOL_MAX) throw std::invalid_argument("chol_tiles: order outside 1..512");
+  if (ldg < k || ldx < np) throw std::invalid_argument("chol_tiles: leading dimension too small");
+  const int nb = np / NB;
+  if (nb <= 8) chol_tiles_launch<8>(G, k, nb, ldg, LX, ldx, status, rel_tol, shift_rel, s);
+  else chol_tiles_launch<16>(G, k, nb, ldg, LX, ldx, status, rel_tol, shift_rel, s);
 }
 
-void chol_factor(double* A, int k, ll lda, double* rdiag, int* status, double rel_tol, cudaStream_t s,
-                 double shift_rel) {
+void trsm_rows(const double* Z, ll rows, int k, const double* LX, ll ldx, double* Y, const int* status,
+               cudaStream_t s) {
+  if (rows < 1) return;
   const int np = chol_padded(k);
-  if (k < 1 || np > CHOL_MAX) throw std::invalid_argument("chol_factor: order outside 1..512");
-  if (lda < np) throw std::invalid_argument("chol_factor: lda below the padded order");
+  if (k < 1 || np > CHOL_MAX) throw std::invalid_argument("trsm_rows: order outside 1..512");
+  if (ldx < np || (ldx & 1)) throw std::invalid_argument("trsm_rows: LX leading dimension");
+  const int nb = np / NB;
+  const size_t smem = sizeof(double) * ((size_t)TR_R * (nb * NB + 4) + 2 * TR_TILE);
+  constexpr size_t smem_max = sizeof(double) * ((size_t)TR_R * (CHOL_MAX + 4) + 2 * TR_TILE);
   static std::atomic<unsigned long long> attr{0};
-  const int smem = (int)sizeof(double) * (NB * TP + NB + NW * NB * TP);
-  set_smem_attr_once(attr, (const void*)chol_cluster_kernel, smem);
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(CC);
-  cfg.blockDim = dim3(CT);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = s;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeClusterDimension;
-  at[0].val.clusterDim.x = CC;
-  at[0].val.clusterDim.y = 1;
-  at[0].val.clusterDim.z = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = 1;
-  DMRG2_CUDA(cudaLaunchKernelEx(&cfg, chol_cluster_kernel, A, k, np, lda, rdiag, status, rel_tol, shift_rel));
-  DMRG2_CHECK_LAUNCH();
-}
-
-void chol_solve_rows(double* Y, ll m, int k, ll ldy, const double* L, ll lda, const double* rdiag,
-                     const int* status, cudaStream_t s) {
-  const int np = chol_padded(k);
-  if (m < 1) return;
-  static std::atomic<unsigned long long> attr{0};
-  const int smem = (int)sizeof(double) * (SR * (np + 1) + NB * TP + SR * TP);
-  constexpr int smem_max = (int)sizeof(double) * (SR * (CHOL_MAX + 1) + NB * TP + SR * TP);
-  set_smem_attr_once(attr, (const void*)chol_solve_rows_kernel, smem_max);  // covers every order
-  const ll grid = (m + SR - 1) / SR;
-  if (grid > 2147483647LL) throw std::invalid_argument("chol_solve_rows: too many rows");
-  chol_solve_rows_kernel<<<(unsigned)grid, ST_THREADS, smem, s>>>(Y, m, k, np, ldy, L, lda, rdiag, status);
+  set_smem_attr_once(attr, (const void*)trsm_rows_kernel, (int)smem_max);  // covers every order
+  const ll grid = (rows + TR_R - 1) / TR_R;
+  if (grid > 2147483647LL) throw std::invalid_argument("trsm_rows: too many rows");
+  trsm_rows_kernel<<<(unsigned)grid, TR_THREADS, smem, s>>>(Z, rows, k, nb, LX, ldx, Y, status);
   DMRG2_CHECK_LAUNCH();
 }
 

@@ -244,8 +244,8 @@ SvdOut eig_split(EigWork<T>& W, const T* theta, int m, int nt, char dir, int chi
 //        left = U, right = U^T theta
 //   'L': V1 = tri(theta^T A), U1 = tri(theta V1), V = tri(theta^T U1),
 //        right = V^T, left = theta V
-// tri = unit columns, then one CholeskyQR pass (Gram matrix, its Cholesky factor
-// inverted in one cluster kernel, then Z L^{-T} on the tensor cores). Why that is
+// tri = unit columns, then one CholeskyQR pass (Gram matrix, its tiled Cholesky factor
+// in one cluster kernel, then the row solve Z L^{-T} on the tensor cores). Why that is
 // enough: the basis a step starts from is orthonormal, ordered by decreasing
 // singular value and close to the Schmidt basis of the bond (the exact split
 // returns Schmidt vectors, and each later warm split keeps that), so each product
@@ -267,9 +267,7 @@ struct WstWork {
   double* Ya = nullptr;  // qmax x kmax
   double* Yb = nullptr;
   double* Yc = nullptr;  // qmax x kmax, the other half of each Newton-Schulz step
-  double* S = nullptr;   // kmax x kmax Gram matrix (padded to chol_padded(kmax) rows)
-  double* Xi = nullptr;  // kmax x kmax inverse Cholesky factor
-  double* rd = nullptr;  // reciprocal pivots (orders above 256)
+  double* S = nullptr;   // Gram matrix, then its tiled Cholesky factor (np x np, np = chol_padded(kmax))
   double* cpart = nullptr;  // column sums of squares per row chunk
   double* ws = nullptr;  // split-K partial products: 8 x qmax x kmax
   double* nrm = nullptr; // |theta|^2, |kept factor|^2
@@ -300,8 +298,6 @@ struct WstWork {
     Yc = (double*)alloc(sizeof(double) * qk);
     const size_t np = (size_t)chol_padded(kmax);
     S = (double*)alloc(sizeof(double) * np * np);
-    Xi = (double*)alloc(sizeof(double) * (size_t)kmax * kmax);
-    rd = (double*)alloc(sizeof(double) * np);
     cpart = (double*)alloc(sizeof(double) * (size_t)COLNORM_MAX_CHUNKS * kmax);
     ws = (double*)alloc(sizeof(double) * 8 * qk);
     nrm = (double*)alloc(sizeof(double) * 4);
@@ -331,7 +327,7 @@ inline size_t wst_bytes(ll qmax, ll kmax) {
   qmax = std::max<ll>(qmax, 1);
   kmax = std::max<ll>(std::min<ll>(kmax, CHOL_MAX), 1);
   const ll np = chol_padded((int)kmax);
-  return sizeof(double) * (size_t)(11 * qmax * kmax + np * np + kmax * kmax + np + COLNORM_MAX_CHUNKS * kmax + 4 + 64) +
+  return sizeof(double) * (size_t)(11 * qmax * kmax + np * np + COLNORM_MAX_CHUNKS * kmax + 4 + 64) +
          sizeof(unsigned) * 4 + sizeof(int) * 4 + sizeof(SvdOut);
 }
 
@@ -423,19 +419,13 @@ inline bool wst_split(WstWork& W, RedScratch& red, const double* theta, int m, i
                    (long long)rows, k, tol, W.h_out->ns_done, *W.h_status, e);
     }
   };
-  // Z (rows x k) <- tri(Z) into dst (dst != Z): unit columns, Gram matrix, L^{-1}, Z L^{-T}
+  // Z (rows x k) <- tri(Z) into dst (dst != Z): unit columns, Gram matrix, its Cholesky factor, Z L^{-T}
   const int ldS = chol_padded(k);
   auto tri = [&](double* Z, ll rows, double* dst) {
     col_normalize(Z, rows, k, W.cpart, W.status, s);
     mul(true, Z, k, k, k, (int)rows, Z, k, false, W.S, ldS, 1.0, 0.0, nullptr);
-    if (k <= CHOL_INV_MAX) {
-      chol_inverse(W.S, k, ldS, W.Xi, k, W.status, 1e-10, 0.0, s);
-      mul(false, Z, k, (int)rows, k, k, W.Xi, k, true, dst, k, 1.0, 0.0, nullptr);
-    } else {
-      chol_factor(W.S, k, ldS, W.rd, W.status, 1e-10, s);
-      chol_solve_rows(Z, rows, k, k, W.S, ldS, W.rd, W.status, s);
-      DMRG2_CUDA(cudaMemcpyAsync(dst, Z, sizeof(double) * (size_t)rows * k, cudaMemcpyDeviceToDevice, s));
-    }
+    chol_tiles(W.S, k, ldS, W.S, ldS, W.status, 1e-10, 0.0, s);  // factor in place of the Gram matrix
+    trsm_rows(Z, rows, k, W.S, ldS, dst, W.status, s);
   };
   if (dir == 'R') {
     if (mode != WST_RESUME) {

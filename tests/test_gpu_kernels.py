@@ -311,7 +311,8 @@ def _orth_rows(X):
 
 @pytest.mark.parametrize("m,n,k,direction", [(64, 64, 20, "R"), (96, 64, 32, "L"), (128, 160, 48, "R"),
                                              (256, 200, 100, "L"), (512, 512, 256, "R"), (512, 512, 256, "L"),
-                                             (40, 64, 8, "R")])
+                                             (40, 64, 8, "R"), (100, 90, 37, "R"), (700, 640, 300, "R"),
+                                             (640, 700, 480, "L")])
 def test_warm_split_vs_numpy(m, n, k, direction):
     """The warm-started subspace split (three CholeskyQR power steps) against numpy's SVD:
     M has singular values 1 .. 1e-2 on the kept k and a gap of 100 below them; the warm
