@@ -24,7 +24,7 @@ CLI = PKG / "bin" / "dmrg2_gpu"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", str(REPO / "include")]
-LIB_SOURCES = ["gemm.cu", "lanczos.cu", "svd.cu", "eig.cu", "contract.cu", "engine.cu", "capi.cu", "noalloc.cu", "umma.cu", "cholqr.cu"]
+LIB_SOURCES = ["gemm.cu", "lanczos.cu", "svd.cu", "eig.cu", "contract.cu", "engine.cu", "capi.cu", "noalloc.cu", "umma.cu", "cholqr.cu", "rsvd.cu"]
 CLI_SOURCES = ["cli.cpp", "mpo_builders.cpp"]
 
 

@@ -364,7 +364,7 @@ EngineConfig engine_config(const dmrg2_config* cfg) {
   c.precision = cfg->precision;
   if (cfg->single_site != 0 && cfg->single_site != 1) throw std::invalid_argument("single_site must be 0 or 1");
   c.single_site = cfg->single_site;
-  if (cfg->truncation != 0 && cfg->truncation != 1) throw std::invalid_argument("unknown truncation");
+  if (cfg->truncation < 0 || cfg->truncation > 2) throw std::invalid_argument("unknown truncation");
   c.truncation = cfg->truncation;
   return c;
 }
@@ -522,6 +522,8 @@ static void fill_reports(const std::vector<SweepStats>& st, dmrg2_sweep_report* 
     r.warm_splits = st[s].warm_splits;
     r.warm_fallbacks = st[s].warm_fallbacks;
     r.warm_short = st[s].warm_short;
+    r.rsvd_splits = st[s].rsvd_splits;
+    r.rsvd_fallbacks = st[s].rsvd_fallbacks;
     r.eig_fallbacks = st[s].eig_fallbacks;
   }
 }

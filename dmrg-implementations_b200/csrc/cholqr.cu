@@ -53,7 +53,7 @@ __device__ inline int ld_acquire_cluster(const int* p) {
 __device__ inline void st_release_cluster(int* p, int v) {
   asm volatile("st.release.cluster.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
-// true once *peer_done >= need (every calling thread acquires), false after CT_SPIN polls
+// true once *peer_done >= need (the calling thread acquires), false after CT_SPIN polls
 __device__ inline bool wait_tiles(const int* peer_done, int need) {
   for (long long it = 0; it < CT_SPIN; ++it)
     if (ld_acquire_cluster(peer_done) >= need) return true;
@@ -147,8 +147,11 @@ __global__ void __launch_bounds__(CT_THREADS, 1)
   bool bad = false;
   if (r < nb) {
     for (int t = 0; t < r; ++t) {
-      // ---- P: L_rt = A_rt X_tt^T once CTA t has published X_tt (its row complete)
-      if (!wait_tiles(cluster.map_shared_rank(&done_s, t), t + 1)) fail_s = 1;
+      // ---- P: L_rt = A_rt X_tt^T once CTA t has published X_tt (its row complete); one
+      // thread polls (the peer's shared memory serves its critical factorisation meanwhile)
+      // and the CTA barrier passes what it acquired on to the other threads
+      if (tid == 0 && !wait_tiles(cluster.map_shared_rank(&done_s, t), t + 1)) fail_s = 1;
+      __syncthreads();
       {
         const double* Xp = cluster.map_shared_rank(Xr, t);
         for (int e = tid; e < NB * NB; e += CT_THREADS) Xs[(e >> 5) * TP + (e & 31)] = Xp[(e >> 5) * TP + (e & 31)];
@@ -173,7 +176,8 @@ __global__ void __launch_bounds__(CT_THREADS, 1)
       const double* Lrt = T_(Lt, t);
       for (int q = warp; q < r - t - 1; q += CT_WARPS) {  // the peers' tiles j = t+1 .. r-1
         const int j = t + 1 + q;
-        if (!wait_tiles(cluster.map_shared_rank(&done_s, j), t + 1)) fail_s = 1;
+        if (lane == 0 && !wait_tiles(cluster.map_shared_rank(&done_s, j), t + 1)) fail_s = 1;
+        __syncwarp();  // lane 0 acquired the tile for the warp
         const double* src = cluster.map_shared_rank(T_(Lt, t), j);  // L_jt in CTA j
         double* W = T_(Ws, warp);
         {

@@ -22,6 +22,7 @@
 #include "contract.cuh"
 #include "engine.h"
 #include "lanczos_driver.cuh"
+#include "rsvd.cuh"
 #include "truncate.cuh"
 
 namespace dmrg2 {
@@ -31,6 +32,10 @@ namespace {
 // bond caps of at most 512
 bool warm_capable(const EngineConfig& c) {
   return !c.complex && c.truncation == 0 && c.svd_method == 0 && !c.single_site && c.chi_max <= CHOL_MAX;
+}
+// the randomised split is an option of two-site sweeps with the density-matrix split
+bool rsvd_capable(const EngineConfig& c) {
+  return c.truncation == 2 && c.svd_method == 0 && !c.single_site;
 }
 
 ll ipow_cap(int d, int e, ll cap) {
@@ -96,6 +101,10 @@ class Engine final : public EngineBase {
       wst_.init((int)qmax_, cfg_.chi_max);
       bytes_ += wst_.bytes;
     }
+    if (rsvd_capable(cfg_)) {
+      rsvd_.init((int)qmax_, cfg_.chi_max + RSVD_OVERSAMPLE);
+      bytes_ += rsvd_.bytes;
+    }
     sigma_ = (double*)dalloc_bytes(sizeof(double) * qmax_);
     perm_ = (int*)dalloc_bytes(sizeof(int) * qmax_);
     svdout_ = (SvdOut*)dalloc_bytes(sizeof(SvdOut));
@@ -125,6 +134,7 @@ class Engine final : public EngineBase {
     lw_.release();
     ew_.release();
     wst_.release();
+    rsvd_.release();
     cudaEventDestroy(ev_c_);
     cudaEventDestroy(ev_d_);
     cudaEventDestroy(ev_s0_);
@@ -696,6 +706,33 @@ class Engine final : public EngineBase {
         ss.warm_fallbacks += 1;
       }
     }
+    if (rsvd_.rmax > 0 && rsvd_applies(rsvd_, (int)m, (int)nc, dir, chi)) {
+      // randomised split (truncation mode 2): a fresh test matrix per call
+      SvdOut o;
+      const unsigned long long seed = ((unsigned long long)cfg_.seed << 32) ^ (unsigned long long)(++rsvd_calls_);
+      bool ok = false;
+      try {
+        ok = rsvd_split(rsvd_, ew_, red_, theta_, (int)m, (int)nc, dir, chi, cfg_.cutoff, seed, mps_[i],
+                        mps_[i + 1], o, st_);
+      } catch (const NumericError&) {
+        ok = false;  // the small split's eigenvectors: the exact split below decides
+      }
+      if (ok) {
+        DMRG2_CUDA(cudaEventRecord(ev_d_, st_));
+        DMRG2_CUDA(cudaEventSynchronize(ev_d_));
+        float ms = 0.f;
+        DMRG2_CUDA(cudaEventElapsedTime(&ms, ev_c_, ev_d_));
+        ss.svd_s += ms * 1e-3;
+        ss.rsvd_splits += 1;
+        dims_[i + 1] = o.k;
+        ss.trunc_err_max = std::max(ss.trunc_err_max, o.trunc_err);
+        ss.trunc_err_sum += o.trunc_err;
+        te_ref_[i] = o.trunc_err;
+        short_age_[i] = 0;
+        return;
+      }
+      ss.rsvd_fallbacks += 1;
+    }
     SvdOut o;
     bool jacobi = (cfg_.svd_method == 1);
     if (!jacobi) {
@@ -752,6 +789,8 @@ class Engine final : public EngineBase {
   LanczosWork<T> lw_;
   EigWork<T> ew_;
   WstWork wst_;                 // warm-started subspace split (real data)
+  RsvdWork<T> rsvd_;            // randomised split (truncation mode 2)
+  unsigned long long rsvd_calls_ = 0;
   int prev_sweep_chi_ = 0;      // bond cap of the last completed sweep (0: none since the last set-up)
   std::vector<double> te_ref_;  // per bond: weight discarded by its last full split (< 0: none yet)
   std::vector<int> short_age_;  // per bond: short warm splits since that full split
@@ -804,6 +843,9 @@ size_t engine_footprint(const EngineConfig& c, const std::vector<int>& Dl, const
          sizeof(double) * 64 + sizeof(unsigned) * 4 + sizeof(SvdOut);
   }
   if (warm_capable(c)) b += wst_bytes(qmax, chi);
+  if (rsvd_capable(c))
+    b += c.complex ? RsvdWork<zc>::bytes_for(qmax, chi + RSVD_OVERSAMPLE)
+                   : RsvdWork<double>::bytes_for(qmax, chi + RSVD_OVERSAMPLE);
   b += sizeof(double) * (size_t)qmax + sizeof(int) * (size_t)qmax + sizeof(SvdOut) + sizeof(JacobiCtl) +
        sizeof(double) * 16 + sizeof(double) * (size_t)nblk * 2 * (KRYLOV_CAP + 2) + sizeof(unsigned) * 4 +
        sizeof(int) * (size_t)(L + 1);

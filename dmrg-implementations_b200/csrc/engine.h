@@ -29,7 +29,9 @@ struct EngineConfig {
   int precision = 0;           // 0: FP64 matvecs; 1: split-BF16 matvecs on tcgen05, then FP64 refinement
   int single_site = 0;         // 1: single-site sweeps (the reference's dmrg-gpu driver)
   int truncation = 0;          // 0: warm-started subspace split on sweeps that repeat the previous
-                               //    sweep's bond cap (real data), exact otherwise; 1: exact always
+                               //    sweep's bond cap (real data), exact otherwise; 1: exact always;
+                               //    2: randomised split where it applies (full_k > k + 10 and the
+                               //    sketched side longer than 2k), exact otherwise
   unsigned seed = 42;
 };
 
@@ -53,6 +55,8 @@ struct SweepStats {
   int warm_splits = 0;       // bonds split by the warm-started subspace truncation
   int warm_fallbacks = 0;    // bonds where it gave up and the exact split ran
   int warm_short = 0;        // warm splits kept after one power half-step
+  int rsvd_splits = 0;       // bonds split by the randomised split
+  int rsvd_fallbacks = 0;    // bonds where it gave up and the exact split ran
   int eig_fallbacks = 0;     // bonds where the density-matrix eigenvectors could not be made
                              // orthonormal and the Jacobi SVD split the bond
 };

@@ -64,7 +64,8 @@ class SweepReport(ctypes.Structure):
         ("lanczos_iters", ctypes.c_longlong), ("lanczos_unconverged", ctypes.c_int),
         ("svd_s", ctypes.c_double), ("jacobi_sweeps_max", ctypes.c_int), ("device_s", ctypes.c_double),
         ("lowprec_matvecs", ctypes.c_longlong), ("warm_splits", ctypes.c_int), ("warm_fallbacks", ctypes.c_int),
-        ("eig_fallbacks", ctypes.c_int), ("warm_short", ctypes.c_int),
+        ("eig_fallbacks", ctypes.c_int), ("warm_short", ctypes.c_int), ("rsvd_splits", ctypes.c_int),
+        ("rsvd_fallbacks", ctypes.c_int),
     ]
 
     def as_dict(self):

@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define DMRG2_ABI_VERSION 4
+#define DMRG2_ABI_VERSION 5
 
 enum dmrg2_status {
   DMRG2_OK = 0,
@@ -85,7 +85,13 @@ typedef struct dmrg2_config {
                          below the cap whose discarded weight exceeds the exact split's
                          threshold, or one where CholeskyQR gives up, takes the exact split of
                          svd_method.
-                         1 = the exact split on every bond */
+                         1 = the exact split on every bond
+                         2 = randomised split (the reference's RSVD option, dmrg2_gpu_impl.h:
+                         1178-1266): r = k + 10 random sketch columns on the side that takes
+                         the isometry, shifted CholeskyQR3, the density-matrix split of the
+                         r-row projection; where full_k > k + 10 and that side is longer than
+                         2k (and r <= 512 real / 256 complex), the exact split elsewhere.
+                         Approximate: its discarded weight is at least the exact split's */
 } dmrg2_config;
 
 /* One row per sweep (left-to-right + right-to-left half sweep). */
@@ -111,6 +117,8 @@ typedef struct dmrg2_sweep_report {
   int eig_fallbacks;         /* bonds whose density-matrix eigenvectors could not be made
                                 orthonormal, split by the one-sided Jacobi SVD instead */
   int warm_short;            /* warm splits kept after one power half-step (of warm_splits) */
+  int rsvd_splits;           /* bonds split by the randomised split (truncation 2) */
+  int rsvd_fallbacks;        /* bonds where it could not orthonormalise its sketch */
 } dmrg2_sweep_report;
 
 /* ---------------------------------------------------------------- solver */
