@@ -64,11 +64,35 @@ static void launch_impl(const Gemm<T>& d, cudaStream_t st) {
   a.beta_re = ST<T>::re(d.beta); a.beta_im = ST<T>::im(d.beta);
   a.skip = d.skip;
   a.kchunk = 0;
+  a.kcluster = 0;
   if (d.splitk > 1) {
-    // partial products per K slice into ws[z] (M x N, ld N), then one reduction
     const int chunk = ceil_div(ceil_div(d.K, d.splitk), G::BK) * G::BK;
     const int nsplit = ceil_div(d.K, chunk);
     a.kchunk = chunk;
+    a.sA1 = a.sA2 = a.sB1 = a.sB2 = a.sC1 = a.sC2 = 0;
+    a.nb2 = 1;
+    if (nsplit > 1 && nsplit <= 8) {
+      // the slices of a tile form one cluster and are summed in it: no workspace, no
+      // second launch, the same summation order as the reduction kernel
+      a.kcluster = nsplit;
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(ceil_div(d.N, G::BN), ceil_div(d.M, G::BM), nsplit);
+      cfg.blockDim = dim3(G::THREADS);
+      cfg.dynamicSmemBytes = S::BYTES;
+      cfg.stream = st;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = 1;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = nsplit;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      DMRG2_CUDA(cudaLaunchKernelEx(&cfg, gemm_kernel<T, TA, TB, CA>, a));
+      DMRG2_CHECK_LAUNCH();
+      return;
+    }
+    // more slices than a portable cluster: partial products per K slice into ws[z]
+    // (M x N, ld N), then one reduction
     a.C = d.ws; a.ldc = d.N; a.sC1 = (ll)d.M * d.N; a.sC2 = 0;
     a.sA1 = a.sA2 = a.sB1 = a.sB2 = 0;
     a.nb2 = 1;

@@ -13,6 +13,8 @@
 // the strided views of the DMRG contractions map onto one launch each.
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 
 namespace dmrg2 {
@@ -29,6 +31,8 @@ struct GemmArgs {
   double alpha_re, alpha_im, beta_re, beta_im;
   const int* skip;  // optional device flag: when non-zero the launch does nothing
   int kchunk;       // split-K: blockIdx.z selects the K slice [z*kchunk, (z+1)*kchunk) (0 = off)
+  int kcluster;     // > 1: the K slices of a tile form one thread-block cluster and are summed
+                    // in it, C = alpha sum + beta C written by the cluster (0: partials to C)
 };
 
 __device__ __forceinline__ void cp_async_8(void* smem, const void* gmem, bool pred) {
@@ -215,8 +219,58 @@ __global__ void __launch_bounds__(GemmTile<T>::THREADS) gemm_kernel(GemmArgs g) 
   }
   cp_async_wait<0>();
 
-  // epilogue
   const bool use_beta = (g.beta_re != 0.0) || (g.beta_im != 0.0);
+  if (g.kcluster > 1) {
+    // split-K inside a cluster: each slice leaves its partial tile in shared memory (the
+    // pipeline buffers are free now), then each CTA sums a share of the tile's rows over
+    // the slices, in slice order, reading its peers' tiles (distributed shared memory)
+    constexpr int PP = BN + (CPLX ? 2 : 4);  // row pitch of the partial tile
+    static_assert(BM * PP <= G::STAGES * S::STAGE, "partial tile must fit the pipeline buffers");
+    __syncthreads();
+    T* part = smem;
+#pragma unroll
+    for (int i = 0; i < MI; ++i)
+#pragma unroll
+      for (int j = 0; j < NI; ++j)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int lr = wm * WM + i * 16 + gq + ((r & 2) ? 8 : 0);
+          const int lc = wn * WN + j * 8 + 2 * tq + (r & 1);
+          if constexpr (!CPLX) part[lr * PP + lc] = acc_re[i][j][r];
+          else part[lr * PP + lc] = mkz(acc_re[i][j][r], acc_im[i][j][r]);
+        }
+    cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+    cl.sync();
+    const int ns = g.kcluster, q = (int)cl.block_rank();
+    const int rows_per = (BM + ns - 1) / ns;
+    const int rb = q * rows_per, re = min(BM, rb + rows_per);
+    for (int e = tid; e < (re - rb) * BN; e += G::THREADS) {
+      const int lr = rb + e / BN, lc = e % BN;
+      const int row = m0 + lr, col = n0 + lc;
+      if (row < M && col < N) {
+        T sum = ST<T>::zero();
+        for (int z2 = 0; z2 < ns; ++z2) sum = sum + cl.map_shared_rank(part, z2)[lr * PP + lc];
+        T* dst = Cb + (ll)row * ldc + col;
+        if constexpr (!CPLX) {
+          double v = g.alpha_re * sum;
+          if (use_beta) v += g.beta_re * (*dst);
+          *dst = v;
+        } else {
+          zc v = mkz(g.alpha_re * sum.re - g.alpha_im * sum.im, g.alpha_re * sum.im + g.alpha_im * sum.re);
+          if (use_beta) {
+            zc o = *dst;
+            v.re += g.beta_re * o.re - g.beta_im * o.im;
+            v.im += g.beta_re * o.im + g.beta_im * o.re;
+          }
+          *dst = v;
+        }
+      }
+    }
+    cl.sync();  // no CTA leaves while a peer may still read its partial tile
+    return;
+  }
+
+  // epilogue
 #pragma unroll
   for (int i = 0; i < MI; ++i)
 #pragma unroll

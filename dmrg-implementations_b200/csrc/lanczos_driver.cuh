@@ -19,7 +19,7 @@ namespace dmrg2 {
 template <typename T>
 struct LanczosWork {
   static constexpr int POLL_RING = 8;
-  static constexpr int POLL_LOOK = 3;
+  static constexpr int POLL_LOOK = 2;
   T* krylov = nullptr;  // kcap vectors of length >= n
   T* w = nullptr;       // work vector
   int kcap = 0;
