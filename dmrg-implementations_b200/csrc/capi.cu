@@ -525,6 +525,7 @@ static void fill_reports(const std::vector<SweepStats>& st, dmrg2_sweep_report* 
     r.rsvd_splits = st[s].rsvd_splits;
     r.rsvd_fallbacks = st[s].rsvd_fallbacks;
     r.eig_fallbacks = st[s].eig_fallbacks;
+    r.phase = st[s].phase;
   }
 }
 
@@ -549,6 +550,22 @@ int dmrg2_resume(dmrg2_handle* h, const int* chi_schedule, int n_sweeps, dmrg2_s
   if (!h) return DMRG2_ERR_ARG;
   return guarded(h, [&] {
     fill_reports(h->eng->resume(make_schedule(h, chi_schedule, n_sweeps)), out, max_out, n_out);
+  });
+}
+
+int dmrg2_pdmrg_run(dmrg2_handle* h, const dmrg2_pdmrg_options* opt, dmrg2_sweep_report* out, int max_out,
+                    int* n_out) {
+  if (!h || !opt) return DMRG2_ERR_ARG;
+  return guarded(h, [&] {
+    PdmrgOptions o;
+    o.n_segments = opt->n_segments;
+    o.n_outer = opt->n_outer;
+    o.n_local = opt->n_local;
+    o.n_warmup = opt->n_warmup;
+    o.n_polish = opt->n_polish;
+    o.n_recal = opt->n_recal;
+    o.chi = opt->chi;
+    fill_reports(h->eng->pdmrg(o), out, max_out, n_out);
   });
 }
 

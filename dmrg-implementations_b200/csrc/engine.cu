@@ -14,9 +14,13 @@
 //  * per-sweep chi schedule, cutoff, Krylov cap and restarts;
 //  * per-sweep energy, truncation error (discarded weight) and timings.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstring>
+#include <functional>
+#include <memory>
 #include <random>
+#include <thread>
 #include <type_traits>
 
 #include "contract.cuh"
@@ -48,6 +52,10 @@ ll ipow_cap(int d, int e, ll cap) {
 }
 }  // namespace
 
+// the lane the calling host thread works on, per engine (see Engine::LaneScope)
+thread_local const void* tl_lane_engine = nullptr;
+thread_local void* tl_lane = nullptr;
+
 template <typename T>
 class Engine final : public EngineBase {
  public:
@@ -61,7 +69,8 @@ class Engine final : public EngineBase {
     L_ = cfg_.L;
     d_ = cfg_.d;
     reset_split_history();
-    DMRG2_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+    lanes_.emplace_back(new Lane());
+    DMRG2_CUDA(cudaStreamCreateWithFlags(&lanes_[0]->st, cudaStreamNonBlocking));
     cap_.resize(L_ + 1);
     for (int i = 0; i <= L_; ++i) cap_[i] = (int)ipow_cap(d_, std::min(i, L_ - i), cfg_.chi_max);
     dims_.assign(L_ + 1, 1);
@@ -89,57 +98,22 @@ class Engine final : public EngineBase {
       qmax_ = std::max(qmax_, std::max(m, n));
     }
     for (int i = 0; i < L_; ++i) qmax_ = std::max(qmax_, (ll)d_ * cap_[i + 1]);
-    theta_ = dalloc(nmax_);
-    svdX_ = dalloc(nmax_);
-    svdQ_ = dalloc(qmax_ * qmax_);
-    tmp_ = dalloc((ll)cfg_.chi_max * cfg_.chi_max);
-    lw_.init(cfg_.krylov_max, nmax_);
-    bytes_ += lw_.bytes(nmax_);
-    ew_.init((int)qmax_, cfg_.chi_max);
-    bytes_ += ew_.bytes;
-    if (warm_capable(cfg_)) {
-      wst_.init((int)qmax_, cfg_.chi_max);
-      bytes_ += wst_.bytes;
-    }
-    if (rsvd_capable(cfg_)) {
-      rsvd_.init((int)qmax_, cfg_.chi_max + RSVD_OVERSAMPLE);
-      bytes_ += rsvd_.bytes;
-    }
-    sigma_ = (double*)dalloc_bytes(sizeof(double) * qmax_);
-    perm_ = (int*)dalloc_bytes(sizeof(int) * qmax_);
-    svdout_ = (SvdOut*)dalloc_bytes(sizeof(SvdOut));
-    jctl_ = (JacobiCtl*)dalloc_bytes(sizeof(JacobiCtl));
-    dscal_ = (double*)dalloc_bytes(sizeof(double) * 16);
-    red_.nblk = vec_blocks(nmax_);
-    red_.part = (double*)dalloc_bytes(sizeof(double) * (size_t)red_.nblk * 2 * (KRYLOV_CAP + 2));
-    red_.counter = (unsigned*)dalloc_bytes(sizeof(unsigned) * 4);
-    DMRG2_CUDA(cudaMemset(red_.counter, 0, sizeof(unsigned) * 4));
-    DMRG2_CUDA(cudaMallocHost(&h_svd_, sizeof(SvdOut)));
+    init_lane(*lanes_[0], true);
     canon_flags_ = (int*)dalloc_bytes(sizeof(int) * (size_t)(L_ + 1));
     DMRG2_CUDA(cudaMallocHost(&h_flags_, sizeof(int) * (size_t)(L_ + 1)));
-    DMRG2_CUDA(cudaEventCreate(&ev_c_));
-    DMRG2_CUDA(cudaEventCreate(&ev_d_));
     DMRG2_CUDA(cudaEventCreate(&ev_s0_));
     DMRG2_CUDA(cudaEventCreate(&ev_s1_));
   }
 
   ~Engine() override {
-    cudaStreamSynchronize(st_);
+    cudaStreamSynchronize(ln().st);
     free_tmp();
     free_mpo();
     for (void* p : allocs_) cudaFree(p);
-    cudaFreeHost(h_svd_);
     cudaFreeHost(h_flags_);
-    split_.release();
-    lw_.release();
-    ew_.release();
-    wst_.release();
-    rsvd_.release();
-    cudaEventDestroy(ev_c_);
-    cudaEventDestroy(ev_d_);
     cudaEventDestroy(ev_s0_);
     cudaEventDestroy(ev_s1_);
-    cudaStreamDestroy(st_);
+    for (auto& l : lanes_) release_lane(*l);
   }
 
   EngineConfig& config() override { return cfg_; }
@@ -160,7 +134,7 @@ class Engine final : public EngineBase {
     for (int i = 0; i < L_; ++i)
       if (Dl[i] < 1 || Dr[i] < 1 || Dl[i] > 4096 || Dr[i] > 4096)
         throw std::runtime_error("set_mpo: bad MPO bond dimension");
-    DMRG2_CUDA(cudaStreamSynchronize(st_));
+    DMRG2_CUDA(cudaStreamSynchronize(ln().st));
     free_mpo();
     Dl_ = Dl;
     Dr_ = Dr;
@@ -233,8 +207,8 @@ class Engine final : public EngineBase {
       lenv_[i] = carve(n);
       renv_[i] = carve(n);
     }
-    X_ = carve(xs);
-    Y_ = carve(xs);
+    lanes_[0]->X = carve(xs);
+    lanes_[0]->Y = carve(xs);
     xs_ = xs;
     mpo_set_ = true;
     envs_valid_ = false;
@@ -249,7 +223,7 @@ class Engine final : public EngineBase {
         throw std::runtime_error("set_mps: bond " + std::to_string(i) + " dimension " +
                                  std::to_string(dims[i]) + " exceeds min(chi_max, d^min(i,L-i)) = " +
                                  std::to_string(cap_[i]));
-    DMRG2_CUDA(cudaStreamSynchronize(st_));
+    DMRG2_CUDA(cudaStreamSynchronize(ln().st));
     dims_ = dims;
     for (int i = 0; i < L_; ++i) {
       size_t n = (size_t)dims[i] * d_ * dims[i + 1];
@@ -262,7 +236,7 @@ class Engine final : public EngineBase {
   }
 
   void get_mps(std::vector<void*>& out) override {
-    DMRG2_CUDA(cudaStreamSynchronize(st_));
+    DMRG2_CUDA(cudaStreamSynchronize(ln().st));
     for (int i = 0; i < L_; ++i) {
       size_t n = (size_t)dims_[i] * d_ * dims_[i + 1];
       DMRG2_CUDA(cudaMemcpy(out[i], mps_[i], n * sizeof(T), cudaMemcpyDeviceToHost));
@@ -279,7 +253,7 @@ class Engine final : public EngineBase {
     right_canonicalize();
     reset_split_history();
     build_right_envs();
-    DMRG2_CUDA(cudaStreamSynchronize(st_));
+    DMRG2_CUDA(cudaStreamSynchronize(ln().st));
     env_build_s_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 
     envs_valid_ = true;
@@ -293,6 +267,242 @@ class Engine final : public EngineBase {
     return sweeps(schedule, false);
   }
 
+  // ---------------------------------------------------------------- parallel sweep
+  // Segmented sweeps with boundary merges (the reference's PDMRGGPU, gpu-rocm/pdmrg-gpu/
+  // src/pdmrg_gpu_impl.h:2320-2725; Stoudenmire and White, New J. Phys. 15, 2013). The
+  // chain is cut into P segments (partition_chain, :582-601). After full-chain warm-up
+  // sweeps, each local iteration runs: even segments left-to-right and odd ones
+  // right-to-left, concurrently (one host thread and one lane, i.e. stream and scratch,
+  // per segment); then every even boundary is merged; then the segments sweep back the
+  // other way and the odd boundaries are merged. A merge optimises theta = psi_L diag(V)
+  // psi_R over the boundary bond, with V = 1/S from the last merge there (ones at first),
+  // splits it with the Jacobi SVD (the small singular values enter V with relative
+  // accuracy), stores V = 1/max(S, 1e-12), keeps U on the left site and S Vh on the right
+  // one, and rebuilds both boundary environments from the orthonormal factors U and Vh.
+  // The energy is the last merge's eigenvalue; the outer loop stops once it changes by less
+  // than tol. Warm-up, recalibration and polish sweeps are full-chain two-site sweeps.
+  // At the end V is put back into the boundaries that were swept from both sides after
+  // their last merge (psi = psi_L V psi_R) and the MPS is right-canonicalised, so get_mps
+  // and expect_local see one normalised state.
+  std::vector<SweepStats> pdmrg(const PdmrgOptions& o) override {
+    if (!mpo_set_) throw std::runtime_error("pdmrg: MPO not set");
+    if (!mps_set_) throw std::runtime_error("pdmrg: MPS not set");
+    if (cfg_.single_site) throw std::invalid_argument("pdmrg: the parallel sweep is two-site");
+    const int P = o.n_segments;
+    const int chi = o.chi > 0 ? o.chi : cfg_.chi_max;
+    if (chi > cfg_.chi_max) throw std::invalid_argument("pdmrg: chi above chi_max");
+    if (P < 2 || 2 * P > L_) throw std::invalid_argument("pdmrg: n_segments must lie in 2..L/2");
+    if (o.n_outer < 1 || o.n_local < 1 || o.n_warmup < 0 || o.n_polish < 0 || o.n_recal < 0)
+      throw std::invalid_argument("pdmrg: bad iteration counts");
+    int device = 0;
+    DMRG2_CUDA(cudaGetDevice(&device));
+    std::vector<SweepStats> out;
+    auto t0 = std::chrono::steady_clock::now();
+    right_canonicalize();
+    reset_split_history();
+    build_right_envs();
+    DMRG2_CUDA(cudaStreamSynchronize(ln().st));
+    env_build_s_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    envs_valid_ = true;
+    auto full_sweeps = [&](int n, int phase) {
+      if (n <= 0) return;
+      for (SweepStats& st : sweeps(std::vector<int>((size_t)n, chi), false)) {
+        st.phase = phase;
+        out.push_back(st);
+      }
+    };
+    full_sweeps(o.n_warmup, 1);
+    // segments: the first L % P take one site more (partition_chain)
+    std::vector<int> first(P), last(P);
+    for (int k = 0, pos = 0; k < P; ++k) {
+      const int len = L_ / P + (k < L_ % P ? 1 : 0);
+      first[k] = pos;
+      last[k] = pos + len - 1;
+      pos += len;
+    }
+    // lanes 1..P, the boundary vectors V on the device; both freed on every exit
+    struct Cleanup {
+      Engine* e;
+      std::vector<double*> v;
+      ~Cleanup() {
+        for (double* p : v) cudaFree(p);
+        while (e->lanes_.size() > 1) {
+          e->release_lane(*e->lanes_.back());
+          e->lanes_.pop_back();
+        }
+      }
+    } cleanup{this, {}};
+    while ((int)lanes_.size() < P + 1) {
+      lanes_.emplace_back(new Lane());
+      init_lane(*lanes_.back(), false);
+    }
+    std::vector<double*>& V = cleanup.v;
+    V.assign((size_t)(P - 1), nullptr);
+    const std::vector<double> ones((size_t)cfg_.chi_max, 1.0);
+    auto reset_v = [&]() {
+      for (double* p : V) DMRG2_CUDA(cudaMemcpy(p, ones.data(), sizeof(double) * ones.size(), cudaMemcpyHostToDevice));
+    };
+    for (auto& p : V) DMRG2_CUDA(cudaMalloc(&p, sizeof(double) * ones.size()));
+    reset_v();
+    // runs job(k, stats) for k < n on lanes 1..n, one host thread each, and waits
+    auto parallel = [&](int n, const std::function<void(int, SweepStats&)>& job) {
+      std::vector<SweepStats> st((size_t)n);
+      std::vector<std::exception_ptr> ex((size_t)n);
+      std::vector<std::thread> th;
+      for (int k = 0; k < n; ++k)
+        th.emplace_back([&, k] {
+          try {
+            DMRG2_CUDA(cudaSetDevice(device));
+            LaneScope scope(this, lanes_[(size_t)k + 1].get());
+            job(k, st[(size_t)k]);
+            DMRG2_CUDA(cudaStreamSynchronize(ln().st));
+          } catch (...) {
+            ex[(size_t)k] = std::current_exception();
+          }
+        });
+      for (auto& t : th) t.join();
+      for (auto& e : ex)
+        if (e) std::rethrow_exception(e);
+      return st;
+    };
+    // psi = psi_L V psi_R at the boundaries swept from both sides since their last merge
+    std::vector<char> needs_v((size_t)(P - 1), 0);
+    auto settle = [&]() {
+      for (int b = 0; b + 1 < P; ++b)
+        if (needs_v[(size_t)b]) {
+          const int bs = last[b];
+          row_scale<T>(mps_[bs + 1], V[(size_t)b], dims_[bs + 1], (ll)d_ * dims_[bs + 2], mps_[bs + 1], false,
+                       ln().st);
+          needs_v[(size_t)b] = 0;
+        }
+      DMRG2_CUDA(cudaStreamSynchronize(ln().st));
+    };
+    auto half_sweep = [&](int parity, SweepStats& acc) {
+      // parity 0: even segments left-to-right, odd right-to-left; parity 1 the reverse
+      for (const SweepStats& st : parallel(P, [&](int k, SweepStats& ss) {
+             const char dir = ((k & 1) == parity) ? 'R' : 'L';
+             if (dir == 'R')
+               for (int i = first[k]; i < last[k]; ++i) optimize_bond(i, 'R', chi, ss);
+             else
+               for (int i = last[k] - 1; i >= first[k]; --i) optimize_bond(i, 'L', chi, ss);
+           }))
+        add_stats(acc, st);
+      for (int b = 0; b + 1 < P; ++b) needs_v[(size_t)b] = 1;  // both neighbours moved
+    };
+    auto merge = [&](int parity, SweepStats& acc) {
+      std::vector<int> act;
+      for (int b = parity; b + 1 < P; b += 2) act.push_back(b);
+      if (act.empty()) return;
+      std::vector<double> e(act.size());
+      auto st = parallel((int)act.size(), [&](int j, SweepStats& ss) {
+        e[(size_t)j] = merge_boundary(last[act[(size_t)j]], V[(size_t)act[(size_t)j]], chi, ss);
+      });
+      for (const SweepStats& x : st) add_stats(acc, x);
+      for (int b : act) needs_v[(size_t)b] = 0;
+      energy_ = e.back();
+    };
+    double e_prev = energy_;
+    bool converged = false;
+    for (int outer = 0; outer < o.n_outer; ++outer) {
+      SweepStats so;
+      so.phase = 2;
+      so.sweep = outer;
+      so.chi_max = chi;
+      auto ts = std::chrono::steady_clock::now();
+      double e_local = energy_;
+      for (int loc = 0; loc < o.n_local; ++loc) {
+        half_sweep(0, so);
+        merge(0, so);
+        half_sweep(1, so);
+        merge(1, so);
+        if (std::fabs(energy_ - e_local) < cfg_.tol && loc > 0) break;
+        e_local = energy_;
+      }
+      so.wall_s = so.device_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - ts).count();
+      so.energy = energy_;
+      so.max_bond = *std::max_element(dims_.begin(), dims_.end());
+      out.push_back(so);
+      const double dE = std::fabs(energy_ - e_prev);
+      e_prev = energy_;
+      if (dE < cfg_.tol) {
+        converged = true;
+        break;
+      }
+      if (o.n_recal > 0 && (outer + 1) % o.n_recal == 0 && outer + 1 < o.n_outer) {
+        settle();
+        right_canonicalize();
+        build_right_envs();
+        full_sweeps(1, 3);
+        e_prev = energy_;
+        reset_v();
+      }
+    }
+    settle();
+    if (o.n_polish > 0 && !converged) {
+      right_canonicalize();
+      build_right_envs();
+      full_sweeps(o.n_polish, 4);
+    }
+    right_canonicalize();
+    DMRG2_CUDA(cudaStreamSynchronize(ln().st));
+    envs_valid_ = false;  // environments of the segmented state; run() rebuilds them
+    return out;
+  }
+
+  // one boundary merge on the calling thread's lane (see pdmrg); returns the eigenvalue
+  double merge_boundary(int bs, double* V, int chi, SweepStats& ss) {
+    Lane& l = ln();
+    const int cL = dims_[bs], cM = dims_[bs + 1], cR = dims_[bs + 2];
+    const ll m = (ll)cL * d_, nc = (ll)d_ * cR;
+    row_scale<T>(mps_[bs + 1], V, cM, nc, l.svdX, false, l.st);  // diag(V) psi_R
+    theta_form(mps_[bs], l.svdX, l.theta, cL, cM, cR, d_, l.st, l.X, xs_);
+    const double e = lanczos(bs, m * nc, ss);
+    DMRG2_CUDA(cudaEventRecord(l.ev_c, l.st));
+    DMRG2_CUDA(cudaMemcpyAsync(l.svdX, l.theta, sizeof(T) * (size_t)(m * nc), cudaMemcpyDeviceToDevice, l.st));
+    set_identity(l.svdQ, (int)m, l.st);
+    svd_jacobi(l.svdX, l.svdQ, (int)m, nc, l.jctl, cfg_.jacobi_max_sweeps, jacobi_tol(nc), nullptr, l.st);
+    svd_sort_truncate(l.svdX, (int)m, nc, l.sigma, l.perm, l.svdout, chi, cfg_.cutoff, false, l.jctl, l.st);
+    DMRG2_CUDA(cudaEventRecord(l.ev_d, l.st));
+    const SvdOut so = read_svd();
+    const int k = so.k;
+    svd_gather(l.svdX, l.svdQ, l.perm, (int)m, nc, k, 0, mps_[bs], mps_[bs + 1], l.st);  // U, S Vh
+    dims_[bs + 1] = k;
+    gather_sigma(l.sigma, l.perm, k, V, l.st);                   // V <- S
+    row_scale<T>(mps_[bs + 1], V, k, nc, l.svdQ, true, l.st);   // Vh = diag(1/S) S Vh
+    inv_clip(V, k, 1e-12, l.st);                                 // V <- 1 / max(S, 1e-12)
+    env_left(lenv_[bs], mps_[bs], wml_[bs], lenv_[bs + 1], l.X, l.Y, cL, k, d_, Dl_[bs], Dr_[bs], l.st);
+    env_right(renv_[bs + 2], l.svdQ, wmr_[bs + 1], renv_[bs + 1], l.X, l.Y, cR, k, d_, Dl_[bs + 1], Dr_[bs + 1],
+              l.st);
+    float ms = 0.f;
+    DMRG2_CUDA(cudaEventElapsedTime(&ms, l.ev_c, l.ev_d));
+    ss.svd_s += ms * 1e-3;
+    ss.jacobi_sweeps_max = std::max(ss.jacobi_sweeps_max, so.jacobi_sweeps);
+    ss.trunc_err_max = std::max(ss.trunc_err_max, so.trunc_err);
+    ss.trunc_err_sum += so.trunc_err;
+    te_ref_[bs] = so.trunc_err;
+    short_age_[bs] = 0;
+    return e;
+  }
+
+  static void add_stats(SweepStats& a, const SweepStats& b) {
+    a.trunc_err_max = std::max(a.trunc_err_max, b.trunc_err_max);
+    a.trunc_err_sum += b.trunc_err_sum;
+    a.matvecs += b.matvecs;
+    a.heff_s += b.heff_s;
+    a.heff_flops += b.heff_flops;
+    a.lanczos_iters += b.lanczos_iters;
+    a.lanczos_unconverged += b.lanczos_unconverged;
+    a.svd_s += b.svd_s;
+    a.jacobi_sweeps_max = std::max(a.jacobi_sweeps_max, b.jacobi_sweeps_max);
+    a.lowprec_matvecs += b.lowprec_matvecs;
+    a.warm_splits += b.warm_splits;
+    a.warm_fallbacks += b.warm_fallbacks;
+    a.eig_fallbacks += b.eig_fallbacks;
+    a.warm_short += b.warm_short;
+    a.rsvd_splits += b.rsvd_splits;
+    a.rsvd_fallbacks += b.rsvd_fallbacks;
+  }
+
   std::vector<SweepStats> sweeps(const std::vector<int>& schedule, bool stop_rule) {
     std::vector<SweepStats> out;
     double e_prev = energy_;
@@ -301,7 +511,7 @@ class Engine final : public EngineBase {
       ss.sweep = (int)sw;
       ss.chi_max = schedule[sw];
       auto ts = std::chrono::steady_clock::now();
-      DMRG2_CUDA(cudaEventRecord(ev_s0_, st_));
+      DMRG2_CUDA(cudaEventRecord(ev_s0_, ln().st));
       double e = 0.0;
       if (cfg_.single_site) {
         e = sweep1(schedule[sw], ss);
@@ -309,8 +519,8 @@ class Engine final : public EngineBase {
         for (int i = 0; i + 1 < L_; ++i) e = optimize_bond(i, 'R', schedule[sw], ss);
         for (int i = L_ - 2; i >= 0; --i) e = optimize_bond(i, 'L', schedule[sw], ss);
       }
-      DMRG2_CUDA(cudaEventRecord(ev_s1_, st_));
-      DMRG2_CUDA(cudaStreamSynchronize(st_));
+      DMRG2_CUDA(cudaEventRecord(ev_s1_, ln().st));
+      DMRG2_CUDA(cudaStreamSynchronize(ln().st));
       float ms = 0.f;
       DMRG2_CUDA(cudaEventElapsedTime(&ms, ev_s0_, ev_s1_));
       ss.device_s = ms * 1e-3;
@@ -341,21 +551,21 @@ class Engine final : public EngineBase {
     double* res = (double*)dalloc_tmp_bytes(sizeof(double) * 2 * (L_ + 1));
     std::vector<T> hid((size_t)d_ * d_, ST<T>::zero());
     for (int i = 0; i < d_; ++i) hid[(size_t)i * d_ + i] = ST<T>::one();
-    DMRG2_CUDA(cudaMemcpyAsync(opd, op, sizeof(T) * d_ * d_, cudaMemcpyHostToDevice, st_));
-    DMRG2_CUDA(cudaMemcpyAsync(idd, hid.data(), sizeof(T) * d_ * d_, cudaMemcpyHostToDevice, st_));
+    DMRG2_CUDA(cudaMemcpyAsync(opd, op, sizeof(T) * d_ * d_, cudaMemcpyHostToDevice, ln().st));
+    DMRG2_CUDA(cudaMemcpyAsync(idd, hid.data(), sizeof(T) * d_ * d_, cudaMemcpyHostToDevice, ln().st));
     T one = ST<T>::one();
-    DMRG2_CUDA(cudaMemcpyAsync(E, &one, sizeof(T), cudaMemcpyHostToDevice, st_));
+    DMRG2_CUDA(cudaMemcpyAsync(E, &one, sizeof(T), cudaMemcpyHostToDevice, ln().st));
     for (int i = 0; i < L_; ++i) {
       int a = dims_[i], b = dims_[i + 1];
-      env_left(E, mps_[i], opd, F, X_, Y_, a, b, d_, 1, 1, st_);
-      trace_real(F, b, b, res + 2 * i, res + 2 * i + 1, st_);
-      env_left(E, mps_[i], idd, E2, X_, Y_, a, b, d_, 1, 1, st_);
-      if (i == 0) trace_real(E2, b, b, res + 2 * L_, res + 2 * L_ + 1, st_);
+      env_left(E, mps_[i], opd, F, ln().X, ln().Y, a, b, d_, 1, 1, ln().st);
+      trace_real(F, b, b, res + 2 * i, res + 2 * i + 1, ln().st);
+      env_left(E, mps_[i], idd, E2, ln().X, ln().Y, a, b, d_, 1, 1, ln().st);
+      if (i == 0) trace_real(E2, b, b, res + 2 * L_, res + 2 * L_ + 1, ln().st);
       std::swap(E, E2);
     }
     std::vector<double> h(2 * (L_ + 1));
-    DMRG2_CUDA(cudaMemcpyAsync(h.data(), res, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st_));
-    DMRG2_CUDA(cudaStreamSynchronize(st_));
+    DMRG2_CUDA(cudaMemcpyAsync(h.data(), res, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, ln().st));
+    DMRG2_CUDA(cudaStreamSynchronize(ln().st));
     free_tmp();
     double nrm = h[2 * L_];
     re.resize(L_);
@@ -411,12 +621,12 @@ class Engine final : public EngineBase {
       g.M = cl; g.N = cl; g.K = nc;
       g.A = mps_[i]; g.lda = nc;
       g.B = mps_[i]; g.ldb = nc;
-      g.C = theta_; g.ldc = cl;
-      launch_gemm(g, st_);
-      identity_check(theta_, cl, 1e-12, canon_flags_ + i, st_);
+      g.C = ln().theta; g.ldc = cl;
+      launch_gemm(g, ln().st);
+      identity_check(ln().theta, cl, 1e-12, canon_flags_ + i, ln().st);
     }
-    DMRG2_CUDA(cudaMemcpyAsync(h_flags_, canon_flags_, sizeof(int) * (size_t)(L_ + 1), cudaMemcpyDeviceToHost, st_));
-    DMRG2_CUDA(cudaStreamSynchronize(st_));
+    DMRG2_CUDA(cudaMemcpyAsync(h_flags_, canon_flags_, sizeof(int) * (size_t)(L_ + 1), cudaMemcpyDeviceToHost, ln().st));
+    DMRG2_CUDA(cudaStreamSynchronize(ln().st));
     for (int i = L_ - 1; i >= 1; --i)
       if (!h_flags_[i]) return i;
     return 0;
@@ -433,71 +643,71 @@ class Engine final : public EngineBase {
       bool jacobi = (cfg_.svd_method == 1);
       if (!jacobi) {
         try {
-          SvdOut o = eig_split(ew_, mps_[i], cl, nc, 'L', chi, 1e-14, true, tmp_, mps_[i], st_);
+          SvdOut o = eig_split(ln().ew, mps_[i], cl, nc, 'L', chi, 1e-14, true, ln().tmp, mps_[i], ln().st);
           k = o.k;
-          scale_inplace(tmp_, (ll)cl * k, &ew_.out->sigma_max2, st_);
+          scale_inplace(ln().tmp, (ll)cl * k, &ln().ew.out->sigma_max2, ln().st);
         } catch (const NumericError&) {
           jacobi = true;  // eigenvectors not orthonormal: the Jacobi SVD splits this site
         }
       }
       if (jacobi) {
-        transpose(mps_[i], svdX_, cl, nc, st_);
-        norm2(svdX_, (ll)cl * nc, dscal_, red_, st_);
-        set_identity(svdQ_, nc, st_);
-        svd_jacobi(svdX_, svdQ_, nc, (ll)cl, jctl_, cfg_.jacobi_max_sweeps, jacobi_tol(cl), dscal_, st_);
-        svd_sort_truncate(svdX_, nc, (ll)cl, sigma_, perm_, svdout_, chi, 1e-14, true, jctl_, st_);
+        transpose(mps_[i], ln().svdX, cl, nc, ln().st);
+        norm2(ln().svdX, (ll)cl * nc, ln().dscal, ln().red, ln().st);
+        set_identity(ln().svdQ, nc, ln().st);
+        svd_jacobi(ln().svdX, ln().svdQ, nc, (ll)cl, ln().jctl, cfg_.jacobi_max_sweeps, jacobi_tol(cl), ln().dscal, ln().st);
+        svd_sort_truncate(ln().svdX, nc, (ll)cl, ln().sigma, ln().perm, ln().svdout, chi, 1e-14, true, ln().jctl, ln().st);
         k = read_svd().k;
-        svd_gather(svdX_, svdQ_, perm_, nc, (ll)cl, k, 1, tmp_, mps_[i], st_);
-        scale_inplace(tmp_, (ll)cl * k, &svdout_->sigma_max2, st_);
+        svd_gather(ln().svdX, ln().svdQ, ln().perm, nc, (ll)cl, k, 1, ln().tmp, mps_[i], ln().st);
+        scale_inplace(ln().tmp, (ll)cl * k, &ln().svdout->sigma_max2, ln().st);
       }
       {  // A[i-1] <- A[i-1] . (U S / sigma_max)
         Gemm<T> g;
         g.M = dims_[i - 1] * d_; g.N = k; g.K = cl;
         g.A = mps_[i - 1]; g.lda = cl;
-        g.B = tmp_; g.ldb = k;
-        g.C = theta_; g.ldc = k;
-        launch_gemm(g, st_);
+        g.B = ln().tmp; g.ldb = k;
+        g.C = ln().theta; g.ldc = k;
+        launch_gemm(g, ln().st);
       }
-      DMRG2_CUDA(cudaMemcpyAsync(mps_[i - 1], theta_, sizeof(T) * (size_t)dims_[i - 1] * d_ * k,
-                                 cudaMemcpyDeviceToDevice, st_));
+      DMRG2_CUDA(cudaMemcpyAsync(mps_[i - 1], ln().theta, sizeof(T) * (size_t)dims_[i - 1] * d_ * k,
+                                 cudaMemcpyDeviceToDevice, ln().st));
       dims_[i] = k;
     }
     const ll n0 = (ll)d_ * dims_[1];
-    norm2(mps_[0], n0, dscal_, red_, st_);
-    scale_inplace(mps_[0], n0, dscal_, st_);
+    norm2(mps_[0], n0, ln().dscal, ln().red, ln().st);
+    scale_inplace(mps_[0], n0, ln().dscal, ln().st);
     canonical_ = true;
   }
 
   void build_right_envs() {
     T one = ST<T>::one();
-    DMRG2_CUDA(cudaMemcpyAsync(lenv_[0], &one, sizeof(T), cudaMemcpyHostToDevice, st_));
-    DMRG2_CUDA(cudaMemcpyAsync(renv_[L_], &one, sizeof(T), cudaMemcpyHostToDevice, st_));
+    DMRG2_CUDA(cudaMemcpyAsync(lenv_[0], &one, sizeof(T), cudaMemcpyHostToDevice, ln().st));
+    DMRG2_CUDA(cudaMemcpyAsync(renv_[L_], &one, sizeof(T), cudaMemcpyHostToDevice, ln().st));
     const int lowest = cfg_.single_site ? 1 : 2;  // single-site sweeps start with R[1]
     for (int i = L_ - 1; i >= lowest; --i)
-      env_right(renv_[i + 1], mps_[i], wmr_[i], renv_[i], X_, Y_, dims_[i + 1], dims_[i], d_, Dl_[i],
-                Dr_[i], st_);
+      env_right(renv_[i + 1], mps_[i], wmr_[i], renv_[i], ln().X, ln().Y, dims_[i + 1], dims_[i], d_, Dl_[i],
+                Dr_[i], ln().st);
   }
 
   SvdOut read_svd() {
-    DMRG2_CUDA(cudaMemcpyAsync(h_svd_, svdout_, sizeof(SvdOut), cudaMemcpyDeviceToHost, st_));
-    DMRG2_CUDA(cudaStreamSynchronize(st_));
-    if (h_svd_->jacobi_err) throw std::runtime_error("Jacobi SVD barrier timed out");
-    return *h_svd_;
+    DMRG2_CUDA(cudaMemcpyAsync(ln().h_svd, ln().svdout, sizeof(SvdOut), cudaMemcpyDeviceToHost, ln().st));
+    DMRG2_CUDA(cudaStreamSynchronize(ln().st));
+    if (ln().h_svd->jacobi_err) throw std::runtime_error("Jacobi SVD barrier timed out");
+    return *ln().h_svd;
   }
 
   // ---------------------------------------------------------------- sweep
   double optimize_bond(int i, char dir, int chi, SweepStats& ss) {
     const int cL = dims_[i], cM = dims_[i + 1], cR = dims_[i + 2];
     const ll n = (ll)cL * d_ * d_ * cR;
-    theta_form(mps_[i], mps_[i + 1], theta_, cL, cM, cR, d_, st_, X_, xs_);
+    theta_form(mps_[i], mps_[i + 1], ln().theta, cL, cM, cR, d_, ln().st, ln().X, xs_);
     double e = lanczos(i, n, ss);
     svd_split(i, dir, chi, ss);
     if (dir == 'R')
-      env_left(lenv_[i], mps_[i], wml_[i], lenv_[i + 1], X_, Y_, dims_[i], dims_[i + 1], d_, Dl_[i],
-               Dr_[i], st_);
+      env_left(lenv_[i], mps_[i], wml_[i], lenv_[i + 1], ln().X, ln().Y, dims_[i], dims_[i + 1], d_, Dl_[i],
+               Dr_[i], ln().st);
     else
-      env_right(renv_[i + 2], mps_[i + 1], wmr_[i + 1], renv_[i + 1], X_, Y_, dims_[i + 2],
-                dims_[i + 1], d_, Dl_[i + 1], Dr_[i + 1], st_);
+      env_right(renv_[i + 2], mps_[i + 1], wmr_[i + 1], renv_[i + 1], ln().X, ln().Y, dims_[i + 2],
+                dims_[i + 1], d_, Dl_[i + 1], Dr_[i + 1], ln().st);
     return e;
   }
 
@@ -506,26 +716,26 @@ class Engine final : public EngineBase {
     const int Dl = Db_[i], Dr = Db_[i + 2];
     const double fl = heff_flops(cL, cR, d_, Dl, Dr, ST<T>::cplx);
     auto mv = [&](const T* in, T* out, const int* skip) {
-      heff_apply(lenv_[i], renv_[i + 2], wwt_[i], in, out, X_, Y_, cL, cR, d_, Dl, Dr, skip, st_);
+      heff_apply(lenv_[i], renv_[i + 2], wwt_[i], in, out, ln().X, ln().Y, cL, cR, d_, Dl, Dr, skip, ln().st);
     };
     LanczosResult r;
     if (cfg_.precision == 1) {
       // precision form: converge on the split-BF16 operator (FP32-level accuracy), then
       // refine the Ritz vector with FP64 matvecs; the energy is the FP64 one
       auto mv_lp = [&](const T* in, T* out, const int* skip) {
-        heff_apply_split(lenv_[i], renv_[i + 2], wwt_[i], in, out, X_, Y_, cL, cR, d_, Dl, Dr, split_, skip, st_);
+        heff_apply_split(lenv_[i], renv_[i + 2], wwt_[i], in, out, ln().X, ln().Y, cL, cR, d_, Dl, Dr, ln().split, skip, ln().st);
       };
-      LanczosResult lp = lanczos_solve<T>(lw_, theta_, n, cfg_.krylov_max, std::max(cfg_.lanczos_tol, 1e-9),
-                                          cfg_.max_restarts, cfg_.seed + 7919u * (unsigned)i, mv_lp, st_);
-      r = lanczos_solve<T>(lw_, theta_, n, std::min(cfg_.krylov_max, 16), cfg_.lanczos_tol, 1,
-                           cfg_.seed + 7919u * (unsigned)i + 1u, mv, st_);
+      LanczosResult lp = lanczos_solve<T>(ln().lw, ln().theta, n, cfg_.krylov_max, std::max(cfg_.lanczos_tol, 1e-9),
+                                          cfg_.max_restarts, cfg_.seed + 7919u * (unsigned)i, mv_lp, ln().st);
+      r = lanczos_solve<T>(ln().lw, ln().theta, n, std::min(cfg_.krylov_max, 16), cfg_.lanczos_tol, 1,
+                           cfg_.seed + 7919u * (unsigned)i + 1u, mv, ln().st);
       ss.lowprec_matvecs += lp.matvecs;
       r.matvecs += lp.matvecs;
       r.iters += lp.iters;
       r.matvec_s += lp.matvec_s;
     } else {
-      r = lanczos_solve<T>(lw_, theta_, n, cfg_.krylov_max, cfg_.lanczos_tol, cfg_.max_restarts,
-                           cfg_.seed + 7919u * (unsigned)i, mv, st_);
+      r = lanczos_solve<T>(ln().lw, ln().theta, n, cfg_.krylov_max, cfg_.lanczos_tol, cfg_.max_restarts,
+                           cfg_.seed + 7919u * (unsigned)i, mv, ln().st);
     }
     ss.heff_s += r.matvec_s;
     ss.matvecs += r.matvecs;
@@ -546,19 +756,19 @@ class Engine final : public EngineBase {
     for (int i = 0; i + 1 < L_; ++i) {
       e = lanczos1(i, ss);
       split1(i, 'R', chi, ss);
-      env_left(lenv_[i], mps_[i], wml_[i], lenv_[i + 1], X_, Y_, dims_[i], dims_[i + 1], d_, Dl_[i], Dr_[i], st_);
+      env_left(lenv_[i], mps_[i], wml_[i], lenv_[i + 1], ln().X, ln().Y, dims_[i], dims_[i + 1], d_, Dl_[i], Dr_[i], ln().st);
     }
     e = lanczos1(L_ - 1, ss);
-    DMRG2_CUDA(cudaMemcpyAsync(mps_[L_ - 1], theta_, sizeof(T) * (size_t)dims_[L_ - 1] * d_ * dims_[L_],
-                               cudaMemcpyDeviceToDevice, st_));
+    DMRG2_CUDA(cudaMemcpyAsync(mps_[L_ - 1], ln().theta, sizeof(T) * (size_t)dims_[L_ - 1] * d_ * dims_[L_],
+                               cudaMemcpyDeviceToDevice, ln().st));
     for (int i = L_ - 1; i >= 1; --i) {
       e = lanczos1(i, ss);
       split1(i, 'L', chi, ss);
-      env_right(renv_[i + 1], mps_[i], wmr_[i], renv_[i], X_, Y_, dims_[i + 1], dims_[i], d_, Dl_[i], Dr_[i], st_);
+      env_right(renv_[i + 1], mps_[i], wmr_[i], renv_[i], ln().X, ln().Y, dims_[i + 1], dims_[i], d_, Dl_[i], Dr_[i], ln().st);
     }
     e = lanczos1(0, ss);
-    DMRG2_CUDA(cudaMemcpyAsync(mps_[0], theta_, sizeof(T) * (size_t)dims_[0] * d_ * dims_[1],
-                               cudaMemcpyDeviceToDevice, st_));
+    DMRG2_CUDA(cudaMemcpyAsync(mps_[0], ln().theta, sizeof(T) * (size_t)dims_[0] * d_ * dims_[1],
+                               cudaMemcpyDeviceToDevice, ln().st));
     return e;
   }
 
@@ -566,12 +776,12 @@ class Engine final : public EngineBase {
     const int cL = dims_[i], cR = dims_[i + 1];
     const int Dl = Db_[i], Dr = Db_[i + 1];
     const ll n = (ll)cL * d_ * cR;
-    DMRG2_CUDA(cudaMemcpyAsync(theta_, mps_[i], sizeof(T) * (size_t)n, cudaMemcpyDeviceToDevice, st_));
+    DMRG2_CUDA(cudaMemcpyAsync(ln().theta, mps_[i], sizeof(T) * (size_t)n, cudaMemcpyDeviceToDevice, ln().st));
     auto mv = [&](const T* in, T* out, const int* skip) {
-      heff1_apply(lenv_[i], renv_[i + 1], wml_[i], in, out, X_, Y_, cL, cR, d_, Dl, Dr, skip, st_);
+      heff1_apply(lenv_[i], renv_[i + 1], wml_[i], in, out, ln().X, ln().Y, cL, cR, d_, Dl, Dr, skip, ln().st);
     };
-    LanczosResult r = lanczos_solve<T>(lw_, theta_, n, cfg_.krylov_max, cfg_.lanczos_tol, cfg_.max_restarts,
-                                       cfg_.seed + 7919u * (unsigned)i, mv, st_);
+    LanczosResult r = lanczos_solve<T>(ln().lw, ln().theta, n, cfg_.krylov_max, cfg_.lanczos_tol, cfg_.max_restarts,
+                                       cfg_.seed + 7919u * (unsigned)i, mv, ln().st);
     ss.heff_s += r.matvec_s;
     ss.matvecs += r.matvecs;
     ss.heff_flops += heff1_flops(cL, cR, d_, Dl, Dr, ST<T>::cplx) * r.matvecs;
@@ -582,37 +792,37 @@ class Engine final : public EngineBase {
 
   void split1(int i, char dir, int chi, SweepStats& ss) {
     const int cL = dims_[i], cR = dims_[i + 1];
-    DMRG2_CUDA(cudaEventRecord(ev_c_, st_));
+    DMRG2_CUDA(cudaEventRecord(ln().ev_c, ln().st));
     SvdOut o;
     if (dir == 'R') {  // theta (cL d) x cR: A[i] = U, then A[i+1] <- (S Vh) A[i+1]
-      o = eig_split(ew_, theta_, cL * d_, cR, 'R', chi, cfg_.cutoff, false, mps_[i], tmp_, st_);
+      o = eig_split(ln().ew, ln().theta, cL * d_, cR, 'R', chi, cfg_.cutoff, false, mps_[i], ln().tmp, ln().st);
       const int k = o.k, cR2 = dims_[i + 2];
       Gemm<T> g;
       g.M = k; g.N = d_ * cR2; g.K = cR;
-      g.A = tmp_; g.lda = cR;
+      g.A = ln().tmp; g.lda = cR;
       g.B = mps_[i + 1]; g.ldb = (ll)d_ * cR2;
-      g.C = svdX_; g.ldc = (ll)d_ * cR2;
-      launch_gemm(g, st_);
-      DMRG2_CUDA(cudaMemcpyAsync(mps_[i + 1], svdX_, sizeof(T) * (size_t)k * d_ * cR2, cudaMemcpyDeviceToDevice,
-                                 st_));
+      g.C = ln().svdX; g.ldc = (ll)d_ * cR2;
+      launch_gemm(g, ln().st);
+      DMRG2_CUDA(cudaMemcpyAsync(mps_[i + 1], ln().svdX, sizeof(T) * (size_t)k * d_ * cR2, cudaMemcpyDeviceToDevice,
+                                 ln().st));
       dims_[i + 1] = k;
     } else {  // theta cL x (d cR): A[i] = Vh, then A[i-1] <- A[i-1] (U S)
-      o = eig_split(ew_, theta_, cL, d_ * cR, 'L', chi, cfg_.cutoff, false, tmp_, mps_[i], st_);
+      o = eig_split(ln().ew, ln().theta, cL, d_ * cR, 'L', chi, cfg_.cutoff, false, ln().tmp, mps_[i], ln().st);
       const int k = o.k, cL2 = dims_[i - 1];
       Gemm<T> g;
       g.M = cL2 * d_; g.N = k; g.K = cL;
       g.A = mps_[i - 1]; g.lda = cL;
-      g.B = tmp_; g.ldb = k;
-      g.C = svdX_; g.ldc = k;
-      launch_gemm(g, st_);
-      DMRG2_CUDA(cudaMemcpyAsync(mps_[i - 1], svdX_, sizeof(T) * (size_t)cL2 * d_ * k, cudaMemcpyDeviceToDevice,
-                                 st_));
+      g.B = ln().tmp; g.ldb = k;
+      g.C = ln().svdX; g.ldc = k;
+      launch_gemm(g, ln().st);
+      DMRG2_CUDA(cudaMemcpyAsync(mps_[i - 1], ln().svdX, sizeof(T) * (size_t)cL2 * d_ * k, cudaMemcpyDeviceToDevice,
+                                 ln().st));
       dims_[i] = k;
     }
-    DMRG2_CUDA(cudaEventRecord(ev_d_, st_));
-    DMRG2_CUDA(cudaEventSynchronize(ev_d_));
+    DMRG2_CUDA(cudaEventRecord(ln().ev_d, ln().st));
+    DMRG2_CUDA(cudaEventSynchronize(ln().ev_d));
     float ms = 0.f;
-    DMRG2_CUDA(cudaEventElapsedTime(&ms, ev_c_, ev_d_));
+    DMRG2_CUDA(cudaEventElapsedTime(&ms, ln().ev_c, ln().ev_d));
     ss.svd_s += ms * 1e-3;
     ss.trunc_err_max = std::max(ss.trunc_err_max, o.trunc_err);
     ss.trunc_err_sum += o.trunc_err;
@@ -630,7 +840,7 @@ class Engine final : public EngineBase {
   // k-dimensional kept space)
   bool warm_split_applies(int i, int chi, ll m, ll nc) const {
     const int k = dims_[i + 1];
-    return prev_sweep_chi_ == chi && k <= chi && k <= wst_.kmax && std::min(m, nc) > k;
+    return prev_sweep_chi_ == chi && k <= chi && k <= ln().wst.kmax && std::min(m, nc) > k;
   }
 
   // A bond below the cap keeps its dimension only while the weight the warm split
@@ -658,21 +868,21 @@ class Engine final : public EngineBase {
   void svd_split(int i, char dir, int chi, SweepStats& ss) {
     const int cL = dims_[i], cR = dims_[i + 2];
     const ll m = (ll)cL * d_, nc = (ll)d_ * cR;
-    DMRG2_CUDA(cudaEventRecord(ev_c_, st_));
+    DMRG2_CUDA(cudaEventRecord(ln().ev_c, ln().st));
     if constexpr (std::is_same<T, double>::value) {
       if (warm_split_applies(i, chi, m, nc)) {
         double te = 0.0;
         const double* warm = (dir == 'R') ? mps_[i + 1] : mps_[i];
         const int k = dims_[i + 1];
         auto split = [&](WstMode mode) {
-          return wst_split(wst_, red_, theta_, (int)m, (int)nc, dir, k, warm, mps_[i], mps_[i + 1], te, st_, mode) &&
-                 warm_split_keeps_rank(k, chi, m, nc, te, wst_.h_buf[1]);
+          return wst_split(ln().wst, ln().red, ln().theta, (int)m, (int)nc, dir, k, warm, mps_[i], mps_[i + 1], te, ln().st, mode) &&
+                 warm_split_keeps_rank(k, chi, m, nc, te, ln().wst.h_buf[1]);
         };
         bool ok = false, short_kept = false;
         if (te_ref_[i] >= 0.0 && short_age_[i] < WARM_SHORT_RUN) {
           if (split(WST_SHORT)) {
             const double te_short = te;
-            short_kept = warm_short_accepts(i, te, wst_.h_buf[1]);
+            short_kept = warm_short_accepts(i, te, ln().wst.h_buf[1]);
             ok = short_kept;
             if (!short_kept || wst_debug()) {
               ok = split(WST_RESUME);  // the two remaining half-steps on the same theta
@@ -686,10 +896,10 @@ class Engine final : public EngineBase {
           ok = split(WST_FULL);
         }
         if (ok) {
-          DMRG2_CUDA(cudaEventRecord(ev_d_, st_));
-          DMRG2_CUDA(cudaEventSynchronize(ev_d_));
+          DMRG2_CUDA(cudaEventRecord(ln().ev_d, ln().st));
+          DMRG2_CUDA(cudaEventSynchronize(ln().ev_d));
           float ms = 0.f;
-          DMRG2_CUDA(cudaEventElapsedTime(&ms, ev_c_, ev_d_));
+          DMRG2_CUDA(cudaEventElapsedTime(&ms, ln().ev_c, ln().ev_d));
           ss.svd_s += ms * 1e-3;
           ss.warm_splits += 1;
           if (short_kept) {
@@ -706,22 +916,22 @@ class Engine final : public EngineBase {
         ss.warm_fallbacks += 1;
       }
     }
-    if (rsvd_.rmax > 0 && rsvd_applies(rsvd_, (int)m, (int)nc, dir, chi)) {
+    if (ln().rsvd.rmax > 0 && rsvd_applies(ln().rsvd, (int)m, (int)nc, dir, chi)) {
       // randomised split (truncation mode 2): a fresh test matrix per call
       SvdOut o;
       const unsigned long long seed = ((unsigned long long)cfg_.seed << 32) ^ (unsigned long long)(++rsvd_calls_);
       bool ok = false;
       try {
-        ok = rsvd_split(rsvd_, ew_, red_, theta_, (int)m, (int)nc, dir, chi, cfg_.cutoff, seed, mps_[i],
-                        mps_[i + 1], o, st_);
+        ok = rsvd_split(ln().rsvd, ln().ew, ln().red, ln().theta, (int)m, (int)nc, dir, chi, cfg_.cutoff, seed, mps_[i],
+                        mps_[i + 1], o, ln().st);
       } catch (const NumericError&) {
         ok = false;  // the small split's eigenvectors: the exact split below decides
       }
       if (ok) {
-        DMRG2_CUDA(cudaEventRecord(ev_d_, st_));
-        DMRG2_CUDA(cudaEventSynchronize(ev_d_));
+        DMRG2_CUDA(cudaEventRecord(ln().ev_d, ln().st));
+        DMRG2_CUDA(cudaEventSynchronize(ln().ev_d));
         float ms = 0.f;
-        DMRG2_CUDA(cudaEventElapsedTime(&ms, ev_c_, ev_d_));
+        DMRG2_CUDA(cudaEventElapsedTime(&ms, ln().ev_c, ln().ev_d));
         ss.svd_s += ms * 1e-3;
         ss.rsvd_splits += 1;
         dims_[i + 1] = o.k;
@@ -737,9 +947,9 @@ class Engine final : public EngineBase {
     bool jacobi = (cfg_.svd_method == 1);
     if (!jacobi) {
       try {
-        o = eig_split(ew_, theta_, (int)m, (int)nc, dir, chi, cfg_.cutoff, false, mps_[i], mps_[i + 1], st_);
-        DMRG2_CUDA(cudaEventRecord(ev_d_, st_));
-        DMRG2_CUDA(cudaEventSynchronize(ev_d_));
+        o = eig_split(ln().ew, ln().theta, (int)m, (int)nc, dir, chi, cfg_.cutoff, false, mps_[i], mps_[i + 1], ln().st);
+        DMRG2_CUDA(cudaEventRecord(ln().ev_d, ln().st));
+        DMRG2_CUDA(cudaEventSynchronize(ln().ev_d));
       } catch (const NumericError&) {
         // the eigenvectors of this density matrix could not be made orthonormal: split the
         // bond with the one-sided Jacobi SVD of theta instead (theta is unchanged)
@@ -753,21 +963,21 @@ class Engine final : public EngineBase {
       if (dir == 'R') {
         nvec = (int)m;
         len = nc;
-        DMRG2_CUDA(cudaMemcpyAsync(svdX_, theta_, sizeof(T) * m * nc, cudaMemcpyDeviceToDevice, st_));
+        DMRG2_CUDA(cudaMemcpyAsync(ln().svdX, ln().theta, sizeof(T) * m * nc, cudaMemcpyDeviceToDevice, ln().st));
       } else {
         nvec = (int)nc;
         len = m;
-        transpose(theta_, svdX_, m, nc, st_);
+        transpose(ln().theta, ln().svdX, m, nc, ln().st);
       }
-      set_identity(svdQ_, nvec, st_);
-      svd_jacobi(svdX_, svdQ_, nvec, len, jctl_, cfg_.jacobi_max_sweeps, jacobi_tol(len), nullptr, st_);
-      svd_sort_truncate(svdX_, nvec, len, sigma_, perm_, svdout_, chi, cfg_.cutoff, false, jctl_, st_);
-      DMRG2_CUDA(cudaEventRecord(ev_d_, st_));
+      set_identity(ln().svdQ, nvec, ln().st);
+      svd_jacobi(ln().svdX, ln().svdQ, nvec, len, ln().jctl, cfg_.jacobi_max_sweeps, jacobi_tol(len), nullptr, ln().st);
+      svd_sort_truncate(ln().svdX, nvec, len, ln().sigma, ln().perm, ln().svdout, chi, cfg_.cutoff, false, ln().jctl, ln().st);
+      DMRG2_CUDA(cudaEventRecord(ln().ev_d, ln().st));
       o = read_svd();
-      svd_gather(svdX_, svdQ_, perm_, nvec, len, o.k, dir == 'R' ? 0 : 1, mps_[i], mps_[i + 1], st_);
+      svd_gather(ln().svdX, ln().svdQ, ln().perm, nvec, len, o.k, dir == 'R' ? 0 : 1, mps_[i], mps_[i + 1], ln().st);
     }
     float ms = 0.f;
-    DMRG2_CUDA(cudaEventElapsedTime(&ms, ev_c_, ev_d_));
+    DMRG2_CUDA(cudaEventElapsedTime(&ms, ln().ev_c, ln().ev_d));
     ss.svd_s += ms * 1e-3;
     ss.jacobi_sweeps_max = std::max(ss.jacobi_sweeps_max, o.jacobi_sweeps);
     dims_[i + 1] = o.k;
@@ -777,40 +987,123 @@ class Engine final : public EngineBase {
     short_age_[i] = 0;
   }
 
+  // ---------------------------------------------------------------- lanes
+  // Scratch of one stream of bond work: a bond (theta, Lanczos, split, environment update)
+  // runs on the lane its host thread selected (LaneScope), lane 0 by default. Segment
+  // sweeps of the parallel sweep run on lanes 1..P concurrently; the bonds they touch are
+  // disjoint.
+  struct Lane {
+    cudaStream_t st = nullptr;
+    T *theta = nullptr, *X = nullptr, *Y = nullptr, *svdX = nullptr, *svdQ = nullptr, *tmp = nullptr;
+    LanczosWork<T> lw;
+    EigWork<T> ew;
+    WstWork wst;     // warm-started subspace split (real data)
+    RsvdWork<T> rsvd;  // randomised split (truncation mode 2)
+    double* sigma = nullptr;
+    int* perm = nullptr;
+    SvdOut* svdout = nullptr;
+    JacobiCtl* jctl = nullptr;
+    double* dscal = nullptr;
+    RedScratch red;
+    SvdOut* h_svd = nullptr;
+    SplitScratch split;  // BF16 pieces of the precision-form matvec
+    cudaEvent_t ev_c = nullptr, ev_d = nullptr;
+    std::vector<void*> owned;  // device buffers of lanes other than 0
+  };
+  Lane& ln() const {
+    return (tl_lane_engine == this) ? *static_cast<Lane*>(tl_lane) : *lanes_[0];
+  }
+  // selects lane l for the bond work of the calling thread while in scope
+  struct LaneScope {
+    LaneScope(const void* eng, Lane* l) {
+      tl_lane_engine = eng;
+      tl_lane = l;
+    }
+    ~LaneScope() {
+      tl_lane_engine = nullptr;
+      tl_lane = nullptr;
+    }
+  };
+  void init_lane(Lane& l, bool primary) {
+    if (!l.st) DMRG2_CUDA(cudaStreamCreateWithFlags(&l.st, cudaStreamNonBlocking));
+    auto al = [&](size_t b) -> void* {
+      b = std::max<size_t>(b, sizeof(T));
+      if (primary) return dalloc_bytes(b);
+      void* p = nullptr;
+      DMRG2_CUDA(cudaMalloc(&p, b));
+      l.owned.push_back(p);
+      return p;
+    };
+    l.theta = (T*)al(sizeof(T) * (size_t)nmax_);
+    l.svdX = (T*)al(sizeof(T) * (size_t)nmax_);
+    l.svdQ = (T*)al(sizeof(T) * (size_t)(qmax_ * qmax_));
+    l.tmp = (T*)al(sizeof(T) * (size_t)cfg_.chi_max * cfg_.chi_max);
+    l.lw.init(cfg_.krylov_max, nmax_);
+    l.ew.init((int)qmax_, cfg_.chi_max);
+    if (primary) bytes_ += l.lw.bytes(nmax_) + l.ew.bytes;
+    if (warm_capable(cfg_)) {
+      l.wst.init((int)qmax_, cfg_.chi_max);
+      if (primary) bytes_ += l.wst.bytes;
+    }
+    if (rsvd_capable(cfg_)) {
+      l.rsvd.init((int)qmax_, cfg_.chi_max + RSVD_OVERSAMPLE);
+      if (primary) bytes_ += l.rsvd.bytes;
+    }
+    l.sigma = (double*)al(sizeof(double) * (size_t)qmax_);
+    l.perm = (int*)al(sizeof(int) * (size_t)qmax_);
+    l.svdout = (SvdOut*)al(sizeof(SvdOut));
+    l.jctl = (JacobiCtl*)al(sizeof(JacobiCtl));
+    l.dscal = (double*)al(sizeof(double) * 16);
+    l.red.nblk = vec_blocks(nmax_);
+    l.red.part = (double*)al(sizeof(double) * (size_t)l.red.nblk * 2 * (KRYLOV_CAP + 2));
+    l.red.counter = (unsigned*)al(sizeof(unsigned) * 4);
+    DMRG2_CUDA(cudaMemset(l.red.counter, 0, sizeof(unsigned) * 4));
+    DMRG2_CUDA(cudaMallocHost(&l.h_svd, sizeof(SvdOut)));
+    DMRG2_CUDA(cudaEventCreate(&l.ev_c));
+    DMRG2_CUDA(cudaEventCreate(&l.ev_d));
+    if (!primary && mpo_set_) {  // lane 0's X, Y are carved from the MPO slab
+      l.X = (T*)al(sizeof(T) * (size_t)xs_);
+      l.Y = (T*)al(sizeof(T) * (size_t)xs_);
+    }
+  }
+  void release_lane(Lane& l) {
+    if (l.st) cudaStreamSynchronize(l.st);
+    l.split.release();
+    l.lw.release();
+    l.ew.release();
+    l.wst.release();
+    l.rsvd.release();
+    for (void* p : l.owned) cudaFree(p);
+    l.owned.clear();
+    if (l.h_svd) cudaFreeHost(l.h_svd);
+    l.h_svd = nullptr;
+    if (l.ev_c) cudaEventDestroy(l.ev_c);
+    if (l.ev_d) cudaEventDestroy(l.ev_d);
+    l.ev_c = l.ev_d = nullptr;
+    if (l.st) cudaStreamDestroy(l.st);
+    l.st = nullptr;
+  }
+
   // ---------------------------------------------------------------- state
   EngineConfig cfg_;
   int L_ = 0, d_ = 0;
-  cudaStream_t st_ = nullptr;
   std::vector<int> cap_, dims_, Dl_, Dr_, Db_;
   std::vector<std::vector<T>> hW_;
   std::vector<T*> mps_, lenv_, renv_, wwt_, wml_, wmr_;
-  T *theta_ = nullptr, *X_ = nullptr, *Y_ = nullptr, *svdX_ = nullptr,
-    *svdQ_ = nullptr, *tmp_ = nullptr;
-  LanczosWork<T> lw_;
-  EigWork<T> ew_;
-  WstWork wst_;                 // warm-started subspace split (real data)
-  RsvdWork<T> rsvd_;            // randomised split (truncation mode 2)
-  unsigned long long rsvd_calls_ = 0;
+  std::atomic<unsigned long long> rsvd_calls_{0};
   int prev_sweep_chi_ = 0;      // bond cap of the last completed sweep (0: none since the last set-up)
   std::vector<double> te_ref_;  // per bond: weight discarded by its last full split (< 0: none yet)
   std::vector<int> short_age_;  // per bond: short warm splits since that full split
-  double* sigma_ = nullptr;
-  int* perm_ = nullptr;
-  SvdOut* svdout_ = nullptr;
-  JacobiCtl* jctl_ = nullptr;
-  double* dscal_ = nullptr;
-  RedScratch red_;
-  SvdOut* h_svd_ = nullptr;
-  SplitScratch split_;  // BF16 pieces of the precision-form matvec
   int* canon_flags_ = nullptr;
   int* h_flags_ = nullptr;
-  cudaEvent_t ev_c_ = nullptr, ev_d_ = nullptr, ev_s0_ = nullptr, ev_s1_ = nullptr;
+  cudaEvent_t ev_s0_ = nullptr, ev_s1_ = nullptr;
+  std::vector<std::unique_ptr<Lane>> lanes_;  // lane 0: the engine's own stream and scratch
   bool envs_valid_ = false;
   std::vector<void*> allocs_, tmp_allocs_;
   void* mpo_slab_ = nullptr;  // every MPO-dependent buffer (mixing matrices, environments, scratch)
   size_t bytes_ = 0, bytes_mpo_ = 0;
   ll nmax_ = 0, qmax_ = 0;
-  ll xs_ = 0;  // elements of each contraction scratch buffer X_, Y_
+  ll xs_ = 0;  // elements of each contraction scratch buffer ln().X, ln().Y
   bool mpo_set_ = false, mps_set_ = false, canonical_ = false;
   double energy_ = 0.0, env_build_s_ = 0.0;
 };

@@ -35,8 +35,22 @@ struct EngineConfig {
   unsigned seed = 42;
 };
 
+// Parallel (segmented) sweep, the reference's PDMRGGPU::run(n_outer, n_local, n_warmup,
+// n_polish, n_recal) with n_segments from its constructor (gpu-rocm/pdmrg-gpu/src/
+// pdmrg_gpu.h:24-40)
+struct PdmrgOptions {
+  int n_segments = 2;  // P segments, each >= 2 sites
+  int n_outer = 20;    // outer iterations (stop when |dE| < tol after one)
+  int n_local = 2;     // local iterations per outer one: two staggered half-sweeps and merges each
+  int n_warmup = 1;    // full-chain sweeps before the segments start
+  int n_polish = 0;    // full-chain sweeps after the outer loop (unless it converged)
+  int n_recal = 0;     // a full-chain sweep every n_recal outer iterations (0: none)
+  int chi = 0;         // bond cap (0: chi_max)
+};
+
 struct SweepStats {
   int sweep = 0;
+  int phase = 0;             // 0 sweep; parallel sweep: 1 warm-up, 2 outer iteration, 3 recalibration, 4 polish
   int chi_max = 0;
   double energy = 0.0;
   double trunc_err_max = 0.0;
@@ -70,6 +84,8 @@ class EngineBase {
   virtual std::vector<SweepStats> run(const std::vector<int>& schedule) = 0;
   // continue sweeping from the current state (environments kept from the last run)
   virtual std::vector<SweepStats> resume(const std::vector<int>& schedule) = 0;
+  // segmented parallel sweeps with boundary merges (see PdmrgOptions)
+  virtual std::vector<SweepStats> pdmrg(const PdmrgOptions& opt) = 0;
   virtual void get_mps(std::vector<void*>& out) = 0;
   virtual void expect_local(const void* op, std::vector<double>& re, std::vector<double>& im) = 0;
   virtual double energy() const = 0;

@@ -87,6 +87,13 @@ template <typename T>
 void svd_gather(const T* X, const T* Q, const int* perm, int nvec, ll len, int k, int mode,
                 T* left, T* right, cudaStream_t s);
 
+// boundary merge of the parallel sweep: the k kept singular values in sorted order,
+// v <- 1 / max(v, floor), and out = diag(v) in (or diag(1/v) in) for a rows x cols block
+void gather_sigma(const double* sigma, const int* perm, int k, double* out, cudaStream_t s);
+void inv_clip(double* v, int k, double floor, cudaStream_t s);
+template <typename T>
+void row_scale(const T* in, const double* v, int rows, ll cols, T* out, bool invert, cudaStream_t s);
+
 // ---------------------------------------------------------------- eigen path (eig.cu)
 template <typename T>
 void hetrd_cluster(T* G, int n, ll ld, double* d, double* e, T* tau, cudaStream_t s);

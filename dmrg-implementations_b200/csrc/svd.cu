@@ -464,6 +464,47 @@ void trace_real(const T* M, int n, ll ld, double* out_re, double* out_im, cudaSt
   DMRG2_CHECK_LAUNCH();
 }
 
+// ---------------------------------------------------------------- boundary-merge helpers
+// out[j] = sigma[perm[j]], j < k: the kept singular values in sorted order
+__global__ void gather_sigma_kernel(const double* __restrict__ sigma, const int* __restrict__ perm, int k,
+                                    double* __restrict__ out) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < k; j += gridDim.x * blockDim.x) out[j] = sigma[perm[j]];
+}
+void gather_sigma(const double* sigma, const int* perm, int k, double* out, cudaStream_t s) {
+  if (k < 1) return;
+  gather_sigma_kernel<<<(k + 255) / 256, 256, 0, s>>>(sigma, perm, k, out);
+  DMRG2_CHECK_LAUNCH();
+}
+// v[j] <- 1 / max(v[j], floor)
+__global__ void inv_clip_kernel(double* __restrict__ v, int k, double floor) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < k; j += gridDim.x * blockDim.x) v[j] = 1.0 / fmax(v[j], floor);
+}
+void inv_clip(double* v, int k, double floor, cudaStream_t s) {
+  if (k < 1) return;
+  inv_clip_kernel<<<(k + 255) / 256, 256, 0, s>>>(v, k, floor);
+  DMRG2_CHECK_LAUNCH();
+}
+// out[r][c] = in[r][c] * v[r] (or / v[r] when invert), rows x cols row-major
+template <typename T>
+__global__ void row_scale_kernel(const T* __restrict__ in, const double* __restrict__ v, int rows, ll cols,
+                                 T* __restrict__ out, int invert) {
+  const ll tot = (ll)rows * cols;
+  for (ll t = (ll)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (ll)gridDim.x * blockDim.x) {
+    const double f = invert ? 1.0 / v[t / cols] : v[t / cols];
+    if constexpr (ST<T>::cplx) out[t] = mkz(f * in[t].re, f * in[t].im);
+    else out[t] = f * in[t];
+  }
+}
+template <typename T>
+void row_scale(const T* in, const double* v, int rows, ll cols, T* out, bool invert, cudaStream_t s) {
+  const ll tot = (ll)rows * cols;
+  if (tot < 1) return;
+  ll g = (tot + 255) / 256;
+  if (g > 148 * 8) g = 148 * 8;
+  row_scale_kernel<T><<<(int)g, 256, 0, s>>>(in, v, rows, cols, out, invert ? 1 : 0);
+  DMRG2_CHECK_LAUNCH();
+}
+
 #define INST(T)                                                                                 \
   template void svd_jacobi<T>(T*, T*, int, ll, JacobiCtl*, int, double, const double*,        \
                               cudaStream_t);   \
@@ -474,7 +515,8 @@ void trace_real(const T* M, int n, ll ld, double* out_re, double* out_im, cudaSt
   template void transpose<T>(const T*, T*, ll, ll, cudaStream_t);                                \
   template void set_identity<T>(T*, int, cudaStream_t);                                          \
   template void trace_real<T>(const T*, int, ll, double*, double*, cudaStream_t);                \
-  template void identity_check<T>(const T*, int, double, int*, cudaStream_t);
+  template void identity_check<T>(const T*, int, double, int*, cudaStream_t);                   \
+  template void row_scale<T>(const T*, const double*, int, ll, T*, bool, cudaStream_t);
 INST(double)
 INST(zc)
 #undef INST

@@ -34,7 +34,7 @@ EXPORTED = [
     "dmrg2_run", "dmrg2_get_energy", "dmrg2_get_env_build_seconds", "dmrg2_get_bond_dims",
     "dmrg2_get_mps", "dmrg2_expect_local", "dmrg2_get_device_bytes", "dmrg2_last_error",
     "dmrg2_abi_version", "dmrg2_op_heff", "dmrg2_op_env_left", "dmrg2_op_env_right",
-    "dmrg2_op_svd", "dmrg2_op_lanczos", "dmrg2_op_gemm", "dmrg2_resume", "dmrg2_get_launch_count",
+    "dmrg2_op_svd", "dmrg2_op_lanczos", "dmrg2_op_gemm", "dmrg2_resume", "dmrg2_pdmrg_run", "dmrg2_get_launch_count",
     "dmrg2_op_heff_noalloc", "dmrg2_server_create", "dmrg2_server_submit", "dmrg2_server_poll",
     "dmrg2_server_destroy", "dmrg2_op_gemm_bf16x3", "dmrg2_op_warm_split",
 ]
@@ -65,11 +65,17 @@ class SweepReport(ctypes.Structure):
         ("svd_s", ctypes.c_double), ("jacobi_sweeps_max", ctypes.c_int), ("device_s", ctypes.c_double),
         ("lowprec_matvecs", ctypes.c_longlong), ("warm_splits", ctypes.c_int), ("warm_fallbacks", ctypes.c_int),
         ("eig_fallbacks", ctypes.c_int), ("warm_short", ctypes.c_int), ("rsvd_splits", ctypes.c_int),
-        ("rsvd_fallbacks", ctypes.c_int),
+        ("rsvd_fallbacks", ctypes.c_int), ("phase", ctypes.c_int),
     ]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class PdmrgOptions(ctypes.Structure):
+    _fields_ = [("n_segments", ctypes.c_int), ("n_outer", ctypes.c_int), ("n_local", ctypes.c_int),
+                ("n_warmup", ctypes.c_int), ("n_polish", ctypes.c_int), ("n_recal", ctypes.c_int),
+                ("chi", ctypes.c_int)]
 
 
 class ServerConfig(ctypes.Structure):
@@ -121,6 +127,7 @@ def load_library(path: str | os.PathLike | None = None):
         "dmrg2_init_mps": (c_int, [vp, c_int, ctypes.c_uint64]),
         "dmrg2_run": (c_int, [vp, ip, c_int, ctypes.POINTER(SweepReport), c_int, ip]),
         "dmrg2_resume": (c_int, [vp, ip, c_int, ctypes.POINTER(SweepReport), c_int, ip]),
+        "dmrg2_pdmrg_run": (c_int, [vp, ctypes.POINTER(PdmrgOptions), ctypes.POINTER(SweepReport), c_int, ip]),
         "dmrg2_get_launch_count": (ctypes.c_longlong, []),
         "dmrg2_get_energy": (c_int, [vp, dp]),
         "dmrg2_get_env_build_seconds": (c_int, [vp, dp]),
@@ -320,6 +327,23 @@ class DMRG2GPU:
         self.reports += out
         return out
 
+    def pdmrg(self, n_segments=2, n_outer=20, n_local=2, n_warmup=1, n_polish=0, n_recal=0, chi=None):
+        """Parallel (segmented) sweeps with boundary merges: PDMRGGPU::run(n_outer, n_local,
+        n_warmup, n_polish, n_recal) with n_segments segments (gpu-rocm/pdmrg-gpu/src/
+        pdmrg_gpu.h:24-40). Returns one report per full sweep and per outer iteration (phase
+        1 warm-up, 2 outer, 3 recalibration, 4 polish); energy() is the last merge's."""
+        opt = PdmrgOptions(n_segments=int(n_segments), n_outer=int(n_outer), n_local=int(n_local),
+                           n_warmup=int(n_warmup), n_polish=int(n_polish), n_recal=int(n_recal),
+                           chi=int(chi or 0))
+        cap = int(n_warmup) + int(n_outer) * (1 + int(n_recal > 0)) + int(n_polish) + 1
+        rep = (SweepReport * cap)()
+        nout = ctypes.c_int(0)
+        _check(self._lib.dmrg2_pdmrg_run(self._h, ctypes.byref(opt), rep, cap, ctypes.byref(nout)), self._h,
+               "pdmrg")
+        out = [rep[i].as_dict() for i in range(min(nout.value, cap))]
+        self.reports += out
+        return out
+
     # -- outputs
     def get_energy(self):
         e = ctypes.c_double()
@@ -368,6 +392,23 @@ class DMRG2GPU:
 # ----------------------------------------------------------------------------
 # primitives (same signatures as the reference's numpy functions)
 # ----------------------------------------------------------------------------
+
+class PDMRGGPU(DMRG2GPU):
+    """Parallel DMRG on one B200 (mirror of PDMRGGPU<Scalar>, gpu-rocm/pdmrg-gpu/src/
+    pdmrg_gpu.h:24-62): the chain in n_segments segments swept concurrently (one stream and
+    scratch lane each), coupled by boundary merges with V = 1/S. tol is the outer stop rule."""
+
+    def __init__(self, L, d, chi_max, D_mpo=None, n_segments=2, tol=1e-10, dtype=np.float64, **kw):
+        super().__init__(L, d, chi_max, D_mpo, tol=tol, dtype=dtype, **kw)
+        self.n_segments = int(n_segments)
+
+    def run(self, n_outer_sweeps=20, n_local_sweeps=2, n_warmup=1, n_polish=0, n_recal=0):
+        """PDMRGGPU::run(n_outer_sweeps, n_local_sweeps, n_warmup, n_polish, n_recal)
+        (pdmrg_gpu_impl.h:2585-2760); returns the energy."""
+        self.pdmrg(self.n_segments, n_outer_sweeps, n_local_sweeps, n_warmup, n_polish, n_recal)
+        return self.get_energy()
+
+
 def apply_heff(L_env, R_env, W_left, W_right, theta):
     code = _dtype_code(L_env, R_env, W_left, W_right, theta)
     L_env, R_env, W_left, W_right, theta = (_prep(a, code) for a in (L_env, R_env, W_left, W_right, theta))

@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define DMRG2_ABI_VERSION 5
+#define DMRG2_ABI_VERSION 6
 
 enum dmrg2_status {
   DMRG2_OK = 0,
@@ -119,6 +119,8 @@ typedef struct dmrg2_sweep_report {
   int warm_short;            /* warm splits kept after one power half-step (of warm_splits) */
   int rsvd_splits;           /* bonds split by the randomised split (truncation 2) */
   int rsvd_fallbacks;        /* bonds where it could not orthonormalise its sketch */
+  int phase;                 /* 0 = sweep (dmrg2_run / dmrg2_resume); dmrg2_pdmrg_run: 1 = warm-up
+                                sweep, 2 = outer iteration, 3 = recalibration sweep, 4 = polish */
 } dmrg2_sweep_report;
 
 /* ---------------------------------------------------------------- solver */
@@ -152,6 +154,24 @@ int dmrg2_run(dmrg2_handle* h, const int* chi_schedule, int n_sweeps, dmrg2_swee
  * run() always rebuilds environments (impl:1427-1436). */
 int dmrg2_resume(dmrg2_handle* h, const int* chi_schedule, int n_sweeps, dmrg2_sweep_report* out,
                  int max_out, int* n_out);
+
+/* Parallel (segmented) DMRG: PDMRGGPU<Scalar>(L, d, chi_max, D_mpo, n_segments, tol) and
+ * PDMRGGPU::run(n_outer, n_local, n_warmup, n_polish, n_recal) (gpu-rocm/pdmrg-gpu/src/
+ * pdmrg_gpu.h:24-40, pdmrg_gpu_impl.h:2585-2760). The handle's tol is the outer stop rule.
+ * Warm-up, recalibration and polish sweeps are full-chain two-site sweeps at chi (the
+ * reference's warm-up and polish are single-site). One report per full sweep and per
+ * outer iteration (phase); the final MPS is right-canonical (dmrg2_get_mps). */
+typedef struct dmrg2_pdmrg_options {
+  int n_segments; /* >= 2, each segment >= 2 sites */
+  int n_outer;    /* outer iterations (reference default 20) */
+  int n_local;    /* local iterations per outer one (2) */
+  int n_warmup;   /* full-chain sweeps first (1) */
+  int n_polish;   /* full-chain sweeps at the end unless the outer loop converged (0) */
+  int n_recal;    /* a full-chain sweep every n_recal outer iterations (0 = never) */
+  int chi;        /* bond cap, <= chi_max (0 = chi_max) */
+} dmrg2_pdmrg_options;
+int dmrg2_pdmrg_run(dmrg2_handle* h, const dmrg2_pdmrg_options* opt, dmrg2_sweep_report* out, int max_out,
+                    int* n_out);
 
 /* get_energy() (dmrg2_gpu.h:40) */
 int dmrg2_get_energy(const dmrg2_handle* h, double* energy);
