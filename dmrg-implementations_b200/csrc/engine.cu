@@ -294,6 +294,9 @@ class Engine final : public EngineBase {
     if (P < 2 || 2 * P > L_) throw std::invalid_argument("pdmrg: n_segments must lie in 2..L/2");
     if (o.n_outer < 1 || o.n_local < 1 || o.n_warmup < 0 || o.n_polish < 0 || o.n_recal < 0)
       throw std::invalid_argument("pdmrg: bad iteration counts");
+    // the left-to-right half of a full sweep builds the left environments the segments
+    // start from (the right ones come from the canonical form below)
+    if (o.n_warmup < 1) throw std::invalid_argument("pdmrg: at least one warm-up sweep is needed");
     int device = 0;
     DMRG2_CUDA(cudaGetDevice(&device));
     std::vector<SweepStats> out;

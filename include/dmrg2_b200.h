@@ -165,7 +165,8 @@ typedef struct dmrg2_pdmrg_options {
   int n_segments; /* >= 2, each segment >= 2 sites */
   int n_outer;    /* outer iterations (reference default 20) */
   int n_local;    /* local iterations per outer one (2) */
-  int n_warmup;   /* full-chain sweeps first (1) */
+  int n_warmup;   /* full-chain sweeps first (1; at least 1: its left-to-right half builds
+                     the left environments the segments start from) */
   int n_polish;   /* full-chain sweeps at the end unless the outer loop converged (0) */
   int n_recal;    /* a full-chain sweep every n_recal outer iterations (0 = never) */
   int chi;        /* bond cap, <= chi_max (0 = chi_max) */

@@ -85,3 +85,12 @@ def test_pdmrg_polish_and_recalibration_run():
     assert 3 in phases and phases[-1] in (2, 4)
     assert abs(e - (-6.911737145575)) < 1e-8
     check_state(eng, mpo, e)
+
+
+def test_pdmrg_needs_a_warmup_sweep():
+    L = 8
+    eng = dmrg2.PDMRGGPU(L, 2, 16, n_segments=2)
+    eng.set_mpo(M.heisenberg_mpo(L))
+    eng.set_mps(O.random_mps(L, 2, 4, seed=0))
+    with pytest.raises(dmrg2.Dmrg2Error):
+        eng.run(n_outer_sweeps=2, n_warmup=0)
