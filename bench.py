@@ -566,9 +566,10 @@ def run_server_workload(args):
         timed = False
         metric = "solves/s (64 XXZ chains, L in {24..64}, chi_max in {64,128}, FP64, continuous admission)"
     else:
-        reqs = served_requests(args.requests or 512)
+        reqs = served_requests(args.requests or 512, rate=args.rate)
         timed = True
-        metric = "solves/s (J1-J2 D=8 request stream, Poisson 20 req/s, L in 16..96, chi_max in {32..256}, FP64)"
+        metric = ("solves/s (J1-J2 D=8 request stream, Poisson %g req/s, L in 16..96, chi_max in {32..256}, FP64)"
+                  % args.rate)
     n_plain = min(len(reqs), args.plain_sample)
     # the plain form: the same requests one at a time, back to back (no arrival gaps)
     plain, plain_wall = serve(reqs[:n_plain], 1, local, False)
@@ -586,6 +587,7 @@ def run_server_workload(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded MPOs and N(0,1) initial MPS)", "impl": "ours",
         "config": {"workload": args.workload, "requests": len(res), "max_active": args.max_active,
+                   "arrival_rate_per_s": args.rate if args.workload == "served" else None,
                    "schedule": "ramp 16,32,.. to chi_max then chi_max x8, stop |dE| < 1e-10",
                    "krylov_max": KRYLOV, "cutoff": 1e-12},
         "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
@@ -722,6 +724,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["sweep", "batched", "served", "precision", "pdmrg"], default="sweep")
     ap.add_argument("--requests", type=int, default=0)
+    ap.add_argument("--rate", type=float, default=20.0, help="served workload: Poisson arrivals per second")
     ap.add_argument("--max-active", type=int, default=12)
     ap.add_argument("--plain-sample", type=int, default=24)
     args = ap.parse_args()

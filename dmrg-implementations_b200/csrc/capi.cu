@@ -69,12 +69,12 @@ int guarded(dmrg2_handle* h, F&& f) {
 struct DBuf {
   void* p = nullptr;
   DBuf() = default;
-  explicit DBuf(size_t b) { DMRG2_CUDA(cudaMalloc(&p, b ? b : 16)); }
+  explicit DBuf(size_t b) { p = dev_alloc(b ? b : 16); }
   DBuf(const void* host, size_t b) : DBuf(b) {
     if (host && b) DMRG2_CUDA(cudaMemcpy(p, host, b, cudaMemcpyHostToDevice));
   }
   ~DBuf() {
-    if (p) cudaFree(p);
+    if (p) dev_free(p);
   }
   DBuf(const DBuf&) = delete;
   DBuf& operator=(const DBuf&) = delete;

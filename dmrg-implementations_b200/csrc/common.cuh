@@ -97,6 +97,15 @@ inline int ceil_div(ll a, ll b) { return (int)((a + b - 1) / b); }
 // DMRG2_ERR_NUMERIC while the device stays usable.
 bool test_unsignalled_waits();
 
+// Device memory of the library, from the device's stream-ordered pool (cudaMallocAsync
+// on a private stream of the calling thread, which the call then waits for). Unlike
+// cudaMalloc / cudaFree, neither call synchronises the device, so an engine that is created
+// or destroyed while others run (the served form) does not stall their streams; the pool
+// keeps released memory for the next allocation. dev_free requires that no stream still
+// uses the memory (owners synchronise their stream first).
+void* dev_alloc(size_t bytes);
+void dev_free(void* p);
+
 // cudaFuncSetAttribute acts on the current device only; `done` records, one bit
 // per device ordinal (mod 64), where the attribute was already set.
 inline void func_attr_once(std::atomic<unsigned long long>& done, const void* func, cudaFuncAttribute attr,

@@ -83,7 +83,7 @@ class Engine final : public EngineBase {
         tot += round256(sizeof(T) * (size_t)std::max<ll>((ll)cap_[i] * d_ * cap_[i + 1], 1));
       }
       void* p = nullptr;
-      DMRG2_CUDA(cudaMalloc(&p, tot));
+      p = dev_alloc(tot);
       allocs_.push_back(p);
       for (int i = 0; i < L_; ++i) {
         mps_[i] = (T*)((char*)p + off[i]);
@@ -109,7 +109,7 @@ class Engine final : public EngineBase {
     cudaStreamSynchronize(ln().st);
     free_tmp();
     free_mpo();
-    for (void* p : allocs_) cudaFree(p);
+    for (void* p : allocs_) dev_free(p);
     cudaFreeHost(h_flags_);
     cudaEventDestroy(ev_s0_);
     cudaEventDestroy(ev_s1_);
@@ -178,7 +178,7 @@ class Engine final : public EngineBase {
     for (auto& h : hww) up += round256(el((ll)h.size()));
     size_t total = up + 2 * round256(el(xs));
     for (int i = 0; i <= L_; ++i) total += 2 * round256(el((ll)cap_[i] * cap_[i] * Db_[i]));
-    DMRG2_CUDA(cudaMalloc(&mpo_slab_, total));
+    mpo_slab_ = dev_alloc(total);
     std::vector<char> stage(up);
     size_t off = 0;
     auto carve = [&](ll n) {
@@ -328,11 +328,12 @@ class Engine final : public EngineBase {
       Engine* e;
       std::vector<double*> v;
       ~Cleanup() {
-        for (double* p : v) cudaFree(p);
-        while (e->lanes_.size() > 1) {
+        while (e->lanes_.size() > 1) {  // synchronises each lane's stream first
           e->release_lane(*e->lanes_.back());
           e->lanes_.pop_back();
         }
+        cudaStreamSynchronize(e->ln().st);
+        for (double* p : v) dev_free(p);
       }
     } cleanup{this, {}};
     while ((int)lanes_.size() < P + 1) {
@@ -345,7 +346,7 @@ class Engine final : public EngineBase {
     auto reset_v = [&]() {
       for (double* p : V) DMRG2_CUDA(cudaMemcpy(p, ones.data(), sizeof(double) * ones.size(), cudaMemcpyHostToDevice));
     };
-    for (auto& p : V) DMRG2_CUDA(cudaMalloc(&p, sizeof(double) * ones.size()));
+    for (auto& p : V) p = (double*)dev_alloc(sizeof(double) * ones.size());
     reset_v();
     // runs job(k, stats) for k < n on lanes 1..n, one host thread each, and waits
     auto parallel = [&](int n, const std::function<void(int, SweepStats&)>& job) {
@@ -584,7 +585,7 @@ class Engine final : public EngineBase {
   T* dalloc(ll n) { return (T*)dalloc_bytes(sizeof(T) * (size_t)std::max<ll>(n, 1)); }
   void* dalloc_bytes(size_t b) {
     void* p = nullptr;
-    DMRG2_CUDA(cudaMalloc(&p, b));
+    p = dev_alloc(b);
     allocs_.push_back(p);
     bytes_ += b;
     return p;
@@ -593,16 +594,16 @@ class Engine final : public EngineBase {
   T* dalloc_tmp(ll n) { return (T*)dalloc_tmp_bytes(sizeof(T) * (size_t)std::max<ll>(n, 1)); }
   void* dalloc_tmp_bytes(size_t b) {
     void* p = nullptr;
-    DMRG2_CUDA(cudaMalloc(&p, b));
+    p = dev_alloc(b);
     tmp_allocs_.push_back(p);
     return p;
   }
   void free_tmp() {
-    for (void* p : tmp_allocs_) cudaFree(p);
+    for (void* p : tmp_allocs_) dev_free(p);
     tmp_allocs_.clear();
   }
   void free_mpo() {
-    if (mpo_slab_) cudaFree(mpo_slab_);
+    if (mpo_slab_) dev_free(mpo_slab_);
     mpo_slab_ = nullptr;
     bytes_mpo_ = 0;
   }
@@ -1033,7 +1034,7 @@ class Engine final : public EngineBase {
       b = std::max<size_t>(b, sizeof(T));
       if (primary) return dalloc_bytes(b);
       void* p = nullptr;
-      DMRG2_CUDA(cudaMalloc(&p, b));
+      p = dev_alloc(b);
       l.owned.push_back(p);
       return p;
     };
@@ -1076,7 +1077,7 @@ class Engine final : public EngineBase {
     l.ew.release();
     l.wst.release();
     l.rsvd.release();
-    for (void* p : l.owned) cudaFree(p);
+    for (void* p : l.owned) dev_free(p);
     l.owned.clear();
     if (l.h_svd) cudaFreeHost(l.h_svd);
     l.h_svd = nullptr;

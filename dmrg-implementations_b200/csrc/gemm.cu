@@ -10,6 +10,43 @@ std::atomic<long long>& launch_counter() {
   return c;
 }
 
+namespace {
+// the calling thread's private stream for pool calls on the current device
+cudaStream_t pool_stream(int& device) {
+  constexpr int kMaxDev = 64;
+  thread_local cudaStream_t streams[kMaxDev] = {};
+  static std::atomic<unsigned long long> pool_ready[kMaxDev];
+  DMRG2_CUDA(cudaGetDevice(&device));
+  if (device < 0 || device >= kMaxDev) throw std::runtime_error("dev_alloc: device index out of range");
+  if (!pool_ready[device].load()) {
+    // keep freed blocks in the pool instead of returning them at each synchronisation
+    cudaMemPool_t pool;
+    DMRG2_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+    unsigned long long keep = ~0ull;
+    DMRG2_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    pool_ready[device].store(1);
+  }
+  if (!streams[device]) DMRG2_CUDA(cudaStreamCreateWithFlags(&streams[device], cudaStreamNonBlocking));
+  return streams[device];
+}
+}  // namespace
+
+void* dev_alloc(size_t bytes) {
+  int dev = 0;
+  cudaStream_t s = pool_stream(dev);
+  void* p = nullptr;
+  DMRG2_CUDA(cudaMallocAsync(&p, bytes ? bytes : 16, s));
+  DMRG2_CUDA(cudaStreamSynchronize(s));  // usable from any stream from here on
+  return p;
+}
+
+void dev_free(void* p) {
+  if (!p) return;
+  int dev = 0;
+  cudaStream_t s = pool_stream(dev);
+  cudaFreeAsync(p, s);
+}
+
 bool test_unsignalled_waits() {
   static const bool on = [] {
     const char* e = std::getenv("DMRG2_TEST_UNSIGNALLED_WAITS");

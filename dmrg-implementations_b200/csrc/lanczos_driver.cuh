@@ -49,7 +49,7 @@ struct LanczosWork {
   }
   void* alloc(size_t b) {
     void* p = nullptr;
-    DMRG2_CUDA(cudaMalloc(&p, b));
+    p = dev_alloc(b);
     owned.push_back(p);
     return p;
   }
@@ -58,7 +58,7 @@ struct LanczosWork {
            sizeof(double) * (size_t)red.nblk * 2 * (KRYLOV_CAP + 2);
   }
   void release() {
-    for (void* p : owned) cudaFree(p);
+    for (void* p : owned) dev_free(p);
     owned.clear();
     if (h_flags) cudaFreeHost(h_flags);
     if (h_st) cudaFreeHost(h_st);

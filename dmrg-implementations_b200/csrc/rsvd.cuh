@@ -69,7 +69,7 @@ struct RsvdWork {
   }
   void* alloc(size_t b) {
     void* p = nullptr;
-    DMRG2_CUDA(cudaMalloc(&p, std::max<size_t>(b, 16)));
+    p = dev_alloc(std::max<size_t>(b, 16));
     owned.push_back(p);
     bytes += b;
     return p;
@@ -93,7 +93,7 @@ struct RsvdWork {
     DMRG2_CUDA(cudaMallocHost(&h_status, sizeof(int)));
   }
   void release() {
-    for (void* p : owned) cudaFree(p);
+    for (void* p : owned) dev_free(p);
     owned.clear();
     if (h_nrm) cudaFreeHost(h_nrm);
     if (h_status) cudaFreeHost(h_status);

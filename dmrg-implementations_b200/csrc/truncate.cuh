@@ -44,7 +44,7 @@ struct EigWork {
 
   void* alloc(size_t b) {
     void* p = nullptr;
-    DMRG2_CUDA(cudaMalloc(&p, std::max<size_t>(b, 16)));
+    p = dev_alloc(std::max<size_t>(b, 16));
     owned.push_back(p);
     bytes += b;
     return p;
@@ -74,7 +74,7 @@ struct EigWork {
     DMRG2_CUDA(cudaEventCreateWithFlags(&ev_wy, cudaEventDisableTiming));
   }
   void release() {
-    for (void* p : owned) cudaFree(p);
+    for (void* p : owned) dev_free(p);
     owned.clear();
     if (h_out) cudaFreeHost(h_out);
     h_out = nullptr;
@@ -284,7 +284,7 @@ struct WstWork {
 
   void* alloc(size_t b) {
     void* p = nullptr;
-    DMRG2_CUDA(cudaMalloc(&p, std::max<size_t>(b, 16)));
+    p = dev_alloc(std::max<size_t>(b, 16));
     owned.push_back(p);
     bytes += b;
     return p;
@@ -311,7 +311,7 @@ struct WstWork {
     DMRG2_CUDA(cudaMallocHost(&h_status, sizeof(int)));
   }
   void release() {
-    for (void* p : owned) cudaFree(p);
+    for (void* p : owned) dev_free(p);
     owned.clear();
     if (h_buf) cudaFreeHost(h_buf);
     if (h_out) cudaFreeHost(h_out);

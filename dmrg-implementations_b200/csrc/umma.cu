@@ -24,22 +24,25 @@
 
 namespace dmrg2 {
 
-void SplitScratch::reserve(size_t b) {
+void SplitScratch::reserve(size_t b, cudaStream_t s) {
   if (!err) {
-    DMRG2_CUDA(cudaMalloc(&err, sizeof(int)));
+    err = (int*)dev_alloc(sizeof(int));
     DMRG2_CUDA(cudaMemset(err, 0, sizeof(int)));
   }
   if (b <= bytes) return;
-  if (p) DMRG2_CUDA(cudaFree(p));
+  if (p) {
+    DMRG2_CUDA(cudaStreamSynchronize(s));  // kernels queued on s may still read the old pieces
+    dev_free(p);
+  }
   p = nullptr;
   bytes = 0;
-  DMRG2_CUDA(cudaMalloc(&p, b));
+  p = dev_alloc(b);
   bytes = b;
 }
 
 void SplitScratch::release() {
-  if (p) cudaFree(p);
-  if (err) cudaFree(err);
+  if (p) dev_free(p);
+  if (err) dev_free(err);
   p = nullptr;
   err = nullptr;
   bytes = 0;
@@ -294,7 +297,7 @@ void gemm_bf16x3(int ta, int tb, int M, int N, int K, T alpha, const T* A, ll ld
   if (Mp / UM_BM > 65535 || nbatch > 65535) throw std::invalid_argument("gemm_bf16x3: grid too large");
   const int nbA = sA == 0 ? 1 : nbatch, nbB = sB == 0 ? 1 : nbatch;  // shared operands split once
   const size_t need = sizeof(__nv_bfloat16) * 3 * ((size_t)nbA * Mp + (size_t)nbB * Np) * (size_t)Kp;
-  ws.reserve(need);
+  ws.reserve(need, s);
   __nv_bfloat16* Ap = (__nv_bfloat16*)ws.p;
   __nv_bfloat16* Bp = Ap + 3 * (size_t)nbA * Mp * Kp;
   const int grid = 148 * 8;

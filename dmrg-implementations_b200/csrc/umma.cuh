@@ -18,7 +18,7 @@ struct SplitScratch {
   void* p = nullptr;
   size_t bytes = 0;
   int* err = nullptr;  // device flag: set when a tensor-core wait timed out
-  void reserve(size_t b);
+  void reserve(size_t b, cudaStream_t s);  // s: the stream the pieces are used on
   void release();
 };
 
