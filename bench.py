@@ -54,7 +54,7 @@ METRIC = "sweeps/s (two-site DMRG, Heisenberg L=100, chi=256, FP64 plain form)"
 # DRAM bytes of one H_eff application at chi = 256 (dram__bytes_read.sum + dram__bytes_write.sum
 # over its four kernels: step-1 GEMM, MPO mixing, split-K step-3 GEMM, split-K reduce), from one
 # ncu capture of `python -m dmrg2.microbench heff --chi 256`; the algorithmic bytes are 9.4 MB
-HEFF_TRAFFIC_BYTES_CHI256 = 38.9e6
+HEFF_TRAFFIC_BYTES_CHI256 = 28.4e6  # ncu DRAM read bytes of the three H_eff kernels at chi=256 (no DRAM writes)
 
 
 def workload_config(n_gpus, extra=None):
