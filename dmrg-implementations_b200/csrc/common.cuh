@@ -106,6 +106,12 @@ bool test_unsignalled_waits();
 void* dev_alloc(size_t bytes);
 void dev_free(void* p);
 
+// Page-locked host memory from a process-wide cache of blocks in power-of-two size
+// classes: a block is page-locked once and reused, never handed back to the driver
+// (cudaFreeHost synchronises the device, which would stall every other engine's stream).
+void* host_pinned(size_t bytes);
+void host_unpin(void* p);
+
 // cudaFuncSetAttribute acts on the current device only; `done` records, one bit
 // per device ordinal (mod 64), where the attribute was already set.
 inline void func_attr_once(std::atomic<unsigned long long>& done, const void* func, cudaFuncAttribute attr,

@@ -100,7 +100,7 @@ class Engine final : public EngineBase {
     for (int i = 0; i < L_; ++i) qmax_ = std::max(qmax_, (ll)d_ * cap_[i + 1]);
     init_lane(*lanes_[0], true);
     canon_flags_ = (int*)dalloc_bytes(sizeof(int) * (size_t)(L_ + 1));
-    DMRG2_CUDA(cudaMallocHost(&h_flags_, sizeof(int) * (size_t)(L_ + 1)));
+    h_flags_ = (int*)host_pinned(sizeof(int) * (size_t)(L_ + 1));
     DMRG2_CUDA(cudaEventCreate(&ev_s0_));
     DMRG2_CUDA(cudaEventCreate(&ev_s1_));
   }
@@ -110,7 +110,7 @@ class Engine final : public EngineBase {
     free_tmp();
     free_mpo();
     for (void* p : allocs_) dev_free(p);
-    cudaFreeHost(h_flags_);
+    host_unpin(h_flags_);
     cudaEventDestroy(ev_s0_);
     cudaEventDestroy(ev_s1_);
     for (auto& l : lanes_) release_lane(*l);
@@ -1062,7 +1062,7 @@ class Engine final : public EngineBase {
     l.red.part = (double*)al(sizeof(double) * (size_t)l.red.nblk * 2 * (KRYLOV_CAP + 2));
     l.red.counter = (unsigned*)al(sizeof(unsigned) * 4);
     DMRG2_CUDA(cudaMemset(l.red.counter, 0, sizeof(unsigned) * 4));
-    DMRG2_CUDA(cudaMallocHost(&l.h_svd, sizeof(SvdOut)));
+    l.h_svd = (SvdOut*)host_pinned(sizeof(SvdOut));
     DMRG2_CUDA(cudaEventCreate(&l.ev_c));
     DMRG2_CUDA(cudaEventCreate(&l.ev_d));
     if (!primary && mpo_set_) {  // lane 0's X, Y are carved from the MPO slab
@@ -1079,7 +1079,7 @@ class Engine final : public EngineBase {
     l.rsvd.release();
     for (void* p : l.owned) dev_free(p);
     l.owned.clear();
-    if (l.h_svd) cudaFreeHost(l.h_svd);
+    if (l.h_svd) host_unpin(l.h_svd);
     l.h_svd = nullptr;
     if (l.ev_c) cudaEventDestroy(l.ev_c);
     if (l.ev_d) cudaEventDestroy(l.ev_d);

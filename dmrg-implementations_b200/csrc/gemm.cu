@@ -1,5 +1,9 @@
 // Host launcher and instantiations of the DMMA GEMM.
 #include <cstdlib>
+#include <map>
+#include <mutex>
+#include <unordered_map>
+#include <vector>
 
 #include "gemm.cuh"
 
@@ -45,6 +49,47 @@ void dev_free(void* p) {
   int dev = 0;
   cudaStream_t s = pool_stream(dev);
   cudaFreeAsync(p, s);
+}
+
+namespace {
+struct PinnedCache {
+  std::mutex mu;
+  std::map<size_t, std::vector<void*>> free_blocks;  // size class -> idle blocks
+  std::unordered_map<void*, size_t> cls;             // block -> its size class
+};
+PinnedCache& pinned_cache() {
+  static PinnedCache* c = new PinnedCache();  // lives to process exit (blocks may outlive statics)
+  return *c;
+}
+}  // namespace
+
+void* host_pinned(size_t bytes) {
+  size_t c = 64;
+  while (c < bytes) c <<= 1;
+  PinnedCache& pc = pinned_cache();
+  {
+    std::lock_guard<std::mutex> lk(pc.mu);
+    auto& v = pc.free_blocks[c];
+    if (!v.empty()) {
+      void* p = v.back();
+      v.pop_back();
+      return p;
+    }
+  }
+  void* p = nullptr;
+  DMRG2_CUDA(cudaMallocHost(&p, c));
+  std::lock_guard<std::mutex> lk(pc.mu);
+  pc.cls[p] = c;
+  return p;
+}
+
+void host_unpin(void* p) {
+  if (!p) return;
+  PinnedCache& pc = pinned_cache();
+  std::lock_guard<std::mutex> lk(pc.mu);
+  auto it = pc.cls.find(p);
+  if (it == pc.cls.end()) return;  // not from this cache
+  pc.free_blocks[it->second].push_back(p);
 }
 
 bool test_unsignalled_waits() {

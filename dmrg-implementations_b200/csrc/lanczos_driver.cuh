@@ -40,8 +40,8 @@ struct LanczosWork {
     red.counter = (unsigned*)alloc(sizeof(unsigned) * 4);
     DMRG2_CUDA(cudaMemset(red.counter, 0, sizeof(unsigned) * 4));
     DMRG2_CUDA(cudaMemset(st, 0, sizeof(LanczosDev)));
-    DMRG2_CUDA(cudaMallocHost(&h_flags, sizeof(int) * POLL_RING));
-    DMRG2_CUDA(cudaMallocHost(&h_st, sizeof(LanczosDev)));
+    h_flags = (int*)host_pinned(sizeof(int) * POLL_RING);
+    h_st = (LanczosDev*)host_pinned(sizeof(LanczosDev));
     ev_poll.resize(POLL_RING);
     for (auto& e : ev_poll) DMRG2_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     ev_mv.resize(2 * KRYLOV_CAP);
@@ -60,8 +60,8 @@ struct LanczosWork {
   void release() {
     for (void* p : owned) dev_free(p);
     owned.clear();
-    if (h_flags) cudaFreeHost(h_flags);
-    if (h_st) cudaFreeHost(h_st);
+    if (h_flags) host_unpin(h_flags);
+    if (h_st) host_unpin(h_st);
     h_flags = nullptr;
     h_st = nullptr;
     for (auto e : ev_poll) cudaEventDestroy(e);

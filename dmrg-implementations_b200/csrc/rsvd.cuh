@@ -89,14 +89,14 @@ struct RsvdWork {
     cpart = (double*)alloc(sizeof(double) * (size_t)COLNORM_MAX_CHUNKS * C * rmax);
     nrm = (double*)alloc(sizeof(double) * 2);
     status = (int*)alloc(sizeof(int));
-    DMRG2_CUDA(cudaMallocHost(&h_nrm, sizeof(double) * 2));
-    DMRG2_CUDA(cudaMallocHost(&h_status, sizeof(int)));
+    h_nrm = (double*)host_pinned(sizeof(double) * 2);
+    h_status = (int*)host_pinned(sizeof(int));
   }
   void release() {
     for (void* p : owned) dev_free(p);
     owned.clear();
-    if (h_nrm) cudaFreeHost(h_nrm);
-    if (h_status) cudaFreeHost(h_status);
+    if (h_nrm) host_unpin(h_nrm);
+    if (h_status) host_unpin(h_status);
     h_nrm = nullptr;
     h_status = nullptr;
   }

@@ -68,7 +68,7 @@ struct EigWork {
     counter = (unsigned*)alloc(sizeof(unsigned) * 4);
     DMRG2_CUDA(cudaMemset(counter, 0, sizeof(unsigned) * 4));
     out = (SvdOut*)alloc(sizeof(SvdOut));
-    DMRG2_CUDA(cudaMallocHost(&h_out, sizeof(SvdOut)));
+    h_out = (SvdOut*)host_pinned(sizeof(SvdOut));
     DMRG2_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
     DMRG2_CUDA(cudaEventCreateWithFlags(&ev_refl, cudaEventDisableTiming));
     DMRG2_CUDA(cudaEventCreateWithFlags(&ev_wy, cudaEventDisableTiming));
@@ -76,7 +76,7 @@ struct EigWork {
   void release() {
     for (void* p : owned) dev_free(p);
     owned.clear();
-    if (h_out) cudaFreeHost(h_out);
+    if (h_out) host_unpin(h_out);
     h_out = nullptr;
     if (side) cudaStreamDestroy(side);
     if (ev_refl) cudaEventDestroy(ev_refl);
@@ -306,16 +306,16 @@ struct WstWork {
     status = (int*)alloc(sizeof(int) * 4);
     out = (SvdOut*)alloc(sizeof(SvdOut));
     DMRG2_CUDA(cudaMemset(counter, 0, sizeof(unsigned) * 4));
-    DMRG2_CUDA(cudaMallocHost(&h_buf, sizeof(double) * 4));
-    DMRG2_CUDA(cudaMallocHost(&h_out, sizeof(SvdOut)));
-    DMRG2_CUDA(cudaMallocHost(&h_status, sizeof(int)));
+    h_buf = (double*)host_pinned(sizeof(double) * 4);
+    h_out = (SvdOut*)host_pinned(sizeof(SvdOut));
+    h_status = (int*)host_pinned(sizeof(int));
   }
   void release() {
     for (void* p : owned) dev_free(p);
     owned.clear();
-    if (h_buf) cudaFreeHost(h_buf);
-    if (h_out) cudaFreeHost(h_out);
-    if (h_status) cudaFreeHost(h_status);
+    if (h_buf) host_unpin(h_buf);
+    if (h_out) host_unpin(h_out);
+    if (h_status) host_unpin(h_status);
     h_buf = nullptr;
     h_out = nullptr;
     h_status = nullptr;
