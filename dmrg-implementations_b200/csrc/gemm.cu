@@ -18,7 +18,16 @@ namespace {
 // the calling thread's private stream for pool calls on the current device
 cudaStream_t pool_stream(int& device) {
   constexpr int kMaxDev = 64;
-  thread_local cudaStream_t streams[kMaxDev] = {};
+  // the thread's private streams, destroyed when the thread ends
+  struct Streams {
+    cudaStream_t s[kMaxDev] = {};
+    ~Streams() {
+      for (cudaStream_t x : s)
+        if (x) (void)cudaStreamDestroy(x);
+    }
+  };
+  thread_local Streams own;
+  cudaStream_t* streams = own.s;
   static std::atomic<unsigned long long> pool_ready[kMaxDev];
   DMRG2_CUDA(cudaGetDevice(&device));
   if (device < 0 || device >= kMaxDev) throw std::runtime_error("dev_alloc: device index out of range");
