@@ -139,12 +139,11 @@ static void splitk_reduce(const T* ws, int ns, int M, int N, T alpha, T beta, T*
   DMRG2_CHECK_LAUNCH();
 }
 
-template <typename T, bool TA, bool TB, bool CA>
-static void launch_impl(const Gemm<T>& d, cudaStream_t st) {
-  using G = GemmTile<T>;
-  using S = GemmSmem<T, TA, TB>;
+template <typename T, typename G, bool TA, bool TB, bool CA>
+static void launch_impl(const Gemm<T>& d, int splitk, cudaStream_t st) {
+  using S = GemmSmem<T, G, TA, TB>;
   static std::atomic<unsigned long long> attr{0};  // per instantiation, per device
-  set_smem_attr_once(attr, (const void*)gemm_kernel<T, TA, TB, CA>, (int)S::BYTES);
+  set_smem_attr_once(attr, (const void*)gemm_kernel<T, G, TA, TB, CA>, (int)S::BYTES);
   GemmArgs a;
   a.M = d.M; a.N = d.N; a.K = d.K;
   a.A = d.A; a.lda = d.lda; a.sA1 = d.sA1; a.sA2 = d.sA2;
@@ -156,8 +155,8 @@ static void launch_impl(const Gemm<T>& d, cudaStream_t st) {
   a.skip = d.skip;
   a.kchunk = 0;
   a.kcluster = 0;
-  if (d.splitk > 1) {
-    const int chunk = ceil_div(ceil_div(d.K, d.splitk), G::BK) * G::BK;
+  if (splitk > 1) {
+    const int chunk = ceil_div(ceil_div(d.K, splitk), G::BK) * G::BK;
     const int nsplit = ceil_div(d.K, chunk);
     a.kchunk = chunk;
     a.sA1 = a.sA2 = a.sB1 = a.sB2 = a.sC1 = a.sC2 = 0;
@@ -178,45 +177,148 @@ static void launch_impl(const Gemm<T>& d, cudaStream_t st) {
       at[0].val.clusterDim.z = nsplit;
       cfg.attrs = at;
       cfg.numAttrs = 1;
-      DMRG2_CUDA(cudaLaunchKernelEx(&cfg, gemm_kernel<T, TA, TB, CA>, a));
+      DMRG2_CUDA(cudaLaunchKernelEx(&cfg, gemm_kernel<T, G, TA, TB, CA>, a));
       DMRG2_CHECK_LAUNCH();
       return;
     }
-    // more slices than a portable cluster: partial products per K slice into ws[z]
-    // (M x N, ld N), then one reduction
-    a.C = d.ws; a.ldc = d.N; a.sC1 = (ll)d.M * d.N; a.sC2 = 0;
-    a.sA1 = a.sA2 = a.sB1 = a.sB2 = 0;
-    a.nb2 = 1;
-    a.alpha_re = 1.0; a.alpha_im = 0.0; a.beta_re = 0.0; a.beta_im = 0.0;
-    dim3 grid(ceil_div(d.N, G::BN), ceil_div(d.M, G::BM), nsplit);
-    gemm_kernel<T, TA, TB, CA><<<grid, G::THREADS, S::BYTES, st>>>(a);
-    DMRG2_CHECK_LAUNCH();
-    splitk_reduce<T>(d.ws, nsplit, d.M, d.N, d.alpha, d.beta, d.C, d.ldc, d.skip, st);
-    return;
+    if (nsplit > 8) {
+      // more slices than a portable cluster: partial products per K slice into ws[z]
+      // (M x N, ld N), then one reduction
+      if (!d.ws) throw std::runtime_error("gemm: more than 8 K slices need a workspace");
+      a.C = d.ws; a.ldc = d.N; a.sC1 = (ll)d.M * d.N; a.sC2 = 0;
+      a.alpha_re = 1.0; a.alpha_im = 0.0; a.beta_re = 0.0; a.beta_im = 0.0;
+      dim3 grid(ceil_div(d.N, G::BN), ceil_div(d.M, G::BM), nsplit);
+      gemm_kernel<T, G, TA, TB, CA><<<grid, G::THREADS, S::BYTES, st>>>(a);
+      DMRG2_CHECK_LAUNCH();
+      splitk_reduce<T>(d.ws, nsplit, d.M, d.N, d.alpha, d.beta, d.C, d.ldc, d.skip, st);
+      return;
+    }
+    a.kchunk = 0;  // one slice
   }
   dim3 grid(ceil_div(d.N, G::BN), ceil_div(d.M, G::BM), d.nb1 * d.nb2);
-  gemm_kernel<T, TA, TB, CA><<<grid, G::THREADS, S::BYTES, st>>>(a);
+  gemm_kernel<T, G, TA, TB, CA><<<grid, G::THREADS, S::BYTES, st>>>(a);
   DMRG2_CHECK_LAUNCH();
 }
+
+template <typename T, typename G>
+static void dispatch(const Gemm<T>& d, int splitk, cudaStream_t st) {
+  const bool ca = ST<T>::cplx && d.ca;
+  if (!d.ta && !d.tb && !ca) return launch_impl<T, G, false, false, false>(d, splitk, st);
+  if (!d.ta && d.tb && !ca) return launch_impl<T, G, false, true, false>(d, splitk, st);
+  if (d.ta && !d.tb && !ca) return launch_impl<T, G, true, false, false>(d, splitk, st);
+  if (d.ta && d.tb && !ca) return launch_impl<T, G, true, true, false>(d, splitk, st);
+  if constexpr (ST<T>::cplx) {
+    if (!d.ta && !d.tb) return launch_impl<T, G, false, false, true>(d, splitk, st);
+    if (!d.ta && d.tb) return launch_impl<T, G, false, true, true>(d, splitk, st);
+    if (d.ta && !d.tb) return launch_impl<T, G, true, false, true>(d, splitk, st);
+    return launch_impl<T, G, true, true, true>(d, splitk, st);
+  }
+}
+
+// ---------------------------------------------------------------- autotuner
+// A single real GEMM of at least TUNE_MIN_FLOP is run in each configuration (64 x 64
+// tiles with 1, 2, 4 or 8 K slices reduced in a cluster; 32 x 32 tiles with 1, 2 or 4)
+// the first time its shape (transposes, M, N, K) occurs in the process, on the caller's
+// stream and operands, writing into a scratch output (never the caller's C, no skip
+// flag); the fastest by CUDA events serves every later GEMM of that shape. Smaller GEMMs
+// are latency-bound and keep the default (64 x 64 tiles, the caller's K split): their
+// many distinct shapes (chain ends, bond-dimension ramps) would cost more to time than
+// a configuration can save. The tuning is off unless DMRG2_GEMM_TUNE=1: measured on the
+// L=100, chi=256 sweep it gains 2% on steady sweeps but loses 10% on a run that starts
+// from a fresh engine (the choices timed in isolation, on L2-resident operands, do not
+// carry over to the sweep's own cache state), and off, results do not depend on timing.
+namespace {
+struct TuneKey {
+  int ta, tb, M, N, K, dev;
+  bool operator==(const TuneKey& o) const {
+    return ta == o.ta && tb == o.tb && M == o.M && N == o.N && K == o.K && dev == o.dev;
+  }
+};
+struct TuneKeyHash {
+  size_t operator()(const TuneKey& k) const {
+    size_t h = (size_t)k.M * 1000003u ^ (size_t)k.N * 9176u ^ (size_t)k.K * 31u;
+    return h ^ (size_t)(k.ta * 2 + k.tb) ^ ((size_t)k.dev << 40);
+  }
+};
+struct TuneChoice {
+  int tile;   // 0: TileD64, 1: TileD32
+  int splitk;
+};
+constexpr double TUNE_MIN_FLOP = 1e8;
+std::mutex& tune_mutex() {
+  static std::mutex m;
+  return m;
+}
+std::unordered_map<TuneKey, TuneChoice, TuneKeyHash>& tune_cache() {
+  static auto* c = new std::unordered_map<TuneKey, TuneChoice, TuneKeyHash>();
+  return *c;
+}
+bool tune_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("DMRG2_GEMM_TUNE");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+
+TuneChoice tuned(const Gemm<double>& d, cudaStream_t st) {
+  int dev = 0;
+  DMRG2_CUDA(cudaGetDevice(&dev));
+  const TuneKey key{d.ta ? 1 : 0, d.tb ? 1 : 0, d.M, d.N, d.K, dev};
+  std::lock_guard<std::mutex> lk(tune_mutex());
+  auto it = tune_cache().find(key);
+  if (it != tune_cache().end()) return it->second;
+  Gemm<double> t = d;
+  t.skip = nullptr;
+  t.ldc = d.N;
+  t.sC1 = t.sC2 = 0;
+  t.C = (double*)dev_alloc(sizeof(double) * (size_t)d.M * d.N);
+  cudaEvent_t e0, e1;
+  DMRG2_CUDA(cudaEventCreate(&e0));
+  DMRG2_CUDA(cudaEventCreate(&e1));
+  TuneChoice best{0, 1};
+  float best_ms = 1e30f;
+  for (int tile = 0; tile < 2; ++tile)
+    for (int sk = 1; sk <= (tile == 0 ? 8 : 4); sk *= 2) {
+      if (sk > 1 && d.K < 32 * sk) continue;  // at least two k-tiles per slice
+      auto run = [&]() {
+        if (tile == 0) dispatch<double, TileD64>(t, sk, st);
+        else dispatch<double, TileD32>(t, sk, st);
+      };
+      run();  // first launch: attributes, instruction cache
+      DMRG2_CUDA(cudaEventRecord(e0, st));
+      for (int r = 0; r < 2; ++r) run();
+      DMRG2_CUDA(cudaEventRecord(e1, st));
+      DMRG2_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      DMRG2_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = {tile, sk};
+      }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  dev_free(t.C);  // the stream is idle after the last event
+  tune_cache()[key] = best;
+  return best;
+}
+}  // namespace
 
 template <typename T>
 void launch_gemm(const Gemm<T>& d, cudaStream_t st) {
   if (d.M <= 0 || d.N <= 0 || d.nb1 * d.nb2 <= 0) return;
   if (d.nb1 * d.nb2 > 65535) throw std::runtime_error("gemm: batch count exceeds 65535");
-  if (d.splitk > 1 && (d.nb1 * d.nb2 != 1 || !d.ws))
-    throw std::runtime_error("gemm: split-K needs a single GEMM and a workspace");
-  if (ceil_div(d.M, GemmTile<T>::BM) > 65535) throw std::runtime_error("gemm: M too large");
-  const bool ca = ST<T>::cplx && d.ca;
-  if (!d.ta && !d.tb && !ca) return launch_impl<T, false, false, false>(d, st);
-  if (!d.ta && d.tb && !ca) return launch_impl<T, false, true, false>(d, st);
-  if (d.ta && !d.tb && !ca) return launch_impl<T, true, false, false>(d, st);
-  if (d.ta && d.tb && !ca) return launch_impl<T, true, true, false>(d, st);
-  if constexpr (ST<T>::cplx) {
-    if (!d.ta && !d.tb) return launch_impl<T, false, false, true>(d, st);
-    if (!d.ta && d.tb) return launch_impl<T, false, true, true>(d, st);
-    if (d.ta && !d.tb) return launch_impl<T, true, false, true>(d, st);
-    return launch_impl<T, true, true, true>(d, st);
+  if (d.splitk > 1 && d.nb1 * d.nb2 != 1) throw std::runtime_error("gemm: split-K needs a single GEMM");
+  if (ceil_div(d.M, TileD32::BM) > 65535) throw std::runtime_error("gemm: M too large");
+  if constexpr (!ST<T>::cplx) {
+    if (d.nb1 * d.nb2 == 1 && 2.0 * d.M * d.N * d.K >= TUNE_MIN_FLOP && tune_enabled()) {
+      const TuneChoice c = tuned(d, st);
+      if (c.tile == 1) return dispatch<T, TileD32>(d, c.splitk, st);
+      return dispatch<T, TileD64>(d, c.splitk, st);
+    }
   }
+  dispatch<T, GemmTile<T>>(d, d.splitk, st);
 }
 
 template void launch_gemm<double>(const Gemm<double>&, cudaStream_t);

