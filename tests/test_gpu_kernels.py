@@ -382,3 +382,40 @@ def test_warm_split_gives_up_on_a_rank_deficient_factor():
     warm = _orth_rows(rng.standard_normal((k, n)))
     with pytest.raises(dmrg2.Dmrg2Error, match=f"status {dmrg2.ERR_NUMERIC}"):
         dmrg2.warm_split(M, warm, k, "R")
+
+
+TUNE_CHILD = r"""
+import numpy as np, dmrg2
+rng = np.random.default_rng(5)
+worst = 0.0
+for (m, n, k, ta, tb) in [(512, 256, 512, "N", "N"), (256, 256, 1024, "T", "N"), (1024, 256, 1280, "N", "T"),
+                          (300, 200, 700, "N", "N")]:
+    A = rng.standard_normal((k, m) if ta == "T" else (m, k))
+    B = rng.standard_normal((n, k) if tb == "T" else (k, n))
+    C0 = rng.standard_normal((m, n))
+    ref = 0.5 * ((A.T if ta == "T" else A) @ (B.T if tb == "T" else B)) - 2.0 * C0
+    for rep in range(2):  # the first call of a shape tunes it, the second uses the choice
+        out = dmrg2.gemm(A, B, ta, tb, alpha=0.5, beta=-2.0, C=C0.copy())
+        worst = max(worst, float(np.abs(out - ref).max() / np.abs(ref).max()))
+print("worst", worst)
+"""
+
+
+def test_gemm_autotuner_choices_match_numpy():
+    """DMRG2_GEMM_TUNE=1: GEMMs of at least 1e8 flop are timed in every configuration
+    (64x64 tiles with 1-8 K slices summed in a cluster, 32x32 tiles with 1-4) on their
+    first call and run with the fastest afterwards; whichever is chosen, the result
+    matches numpy to FP64 rounding (beta != 0 included: the timing writes a scratch
+    output, not the caller's C)."""
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+    repo = Path(__file__).resolve().parent.parent
+    env = dict(os.environ, DMRG2_GEMM_TUNE="1",
+               PYTHONPATH=os.pathsep.join([str(repo / "dmrg-implementations_b200"), str(repo)]))
+    r = subprocess.run([sys.executable, "-c", TUNE_CHILD], env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    worst = float(r.stdout.split("worst")[1])
+    print("autotuned GEMMs: worst relative error", worst)
+    assert worst < 1e-13
