@@ -271,7 +271,7 @@ __device__ inline void house_real1(double alpha, double xn2, double& tk, double&
 //     writes one block per step into its own slot of its inbox, [(p'_r, column
 //     (k+2)_r) of its rows][its warps' partials of s'], and copies that block
 //     into the same slot of every peer's inbox with cp.async.bulk (shared::cta to
-//     shared::cluster, no multicast), which counts the bytes on the receiver's
+//     shared::cluster, one copy per peer), which counts the bytes on the receiver's
 //     mbarrier; a CTA starts step k once its barrier has seen every peer's block
 //     of step k. Two parity inboxes (and barriers) carry consecutive steps. A
 //     slot is rewritten two steps after it was read, and its writer can only get
