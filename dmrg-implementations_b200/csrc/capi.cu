@@ -526,6 +526,7 @@ static void fill_reports(const std::vector<SweepStats>& st, dmrg2_sweep_report* 
     r.rsvd_fallbacks = st[s].rsvd_fallbacks;
     r.eig_fallbacks = st[s].eig_fallbacks;
     r.phase = st[s].phase;
+    r.device_loops = st[s].device_loops;
   }
 }
 

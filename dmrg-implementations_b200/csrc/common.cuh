@@ -82,11 +82,16 @@ struct NumericError : public std::runtime_error {
 // Every kernel launch of the library goes through DMRG2_CHECK_LAUNCH, which
 // also counts it (reported through dmrg2_get_launch_count).
 std::atomic<long long>& launch_counter();  // kernels launched by this library (all threads)
+long long& thread_launches();              // the same, by the calling thread
 #define DMRG2_CHECK_LAUNCH()            \
   do {                                  \
     DMRG2_CUDA(cudaGetLastError());     \
     ++::dmrg2::launch_counter();        \
+    ++::dmrg2::thread_launches();       \
   } while (0)
+
+// GEMMs pick their tile shapes by timing candidates (DMRG2_GEMM_TUNE=1)
+bool tune_enabled();
 
 inline int ceil_div(ll a, ll b) { return (int)((a + b - 1) / b); }
 

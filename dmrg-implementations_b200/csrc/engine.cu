@@ -176,7 +176,11 @@ class Engine final : public EngineBase {
     for (auto& h : hml) up += round256(el((ll)h.size()));
     for (auto& h : hmr) up += round256(el((ll)h.size()));
     for (auto& h : hww) up += round256(el((ll)h.size()));
-    size_t total = up + 2 * round256(el(xs));
+    ll opn = 1, opw = 1;  // staged operator slots
+    for (int i = 0; i <= L_; ++i) opn = std::max(opn, (ll)cap_[i] * cap_[i] * Db_[i]);
+    for (auto& h : hww) opw = std::max(opw, (ll)h.size());
+    for (auto& h : hml) opw = std::max(opw, (ll)h.size());
+    size_t total = up + 2 * round256(el(xs)) + 2 * round256(el(opn)) + round256(el(opw));
     for (int i = 0; i <= L_; ++i) total += 2 * round256(el((ll)cap_[i] * cap_[i] * Db_[i]));
     mpo_slab_ = dev_alloc(total);
     std::vector<char> stage(up);
@@ -209,7 +213,12 @@ class Engine final : public EngineBase {
     }
     lanes_[0]->X = carve(xs);
     lanes_[0]->Y = carve(xs);
+    lanes_[0]->opL = carve(opn);
+    lanes_[0]->opR = carve(opn);
+    lanes_[0]->opW = carve(opw);
     xs_ = xs;
+    opn_ = opn;
+    opw_ = opw;
     mpo_set_ = true;
     envs_valid_ = false;
   }
@@ -505,6 +514,7 @@ class Engine final : public EngineBase {
     a.warm_short += b.warm_short;
     a.rsvd_splits += b.rsvd_splits;
     a.rsvd_fallbacks += b.rsvd_fallbacks;
+    a.device_loops += b.device_loops;
   }
 
   std::vector<SweepStats> sweeps(const std::vector<int>& schedule, bool stop_rule) {
@@ -699,6 +709,12 @@ class Engine final : public EngineBase {
     return *ln().h_svd;
   }
 
+  // copies n elements of a bond's operator into a lane slot (on the lane's stream)
+  const T* stage_op(T* slot, const T* src, ll n) {
+    DMRG2_CUDA(cudaMemcpyAsync(slot, src, sizeof(T) * (size_t)n, cudaMemcpyDeviceToDevice, ln().st));
+    return slot;
+  }
+
   // ---------------------------------------------------------------- sweep
   double optimize_bond(int i, char dir, int chi, SweepStats& ss) {
     const int cL = dims_[i], cM = dims_[i + 1], cR = dims_[i + 2];
@@ -737,6 +753,18 @@ class Engine final : public EngineBase {
       r.matvecs += lp.matvecs;
       r.iters += lp.iters;
       r.matvec_s += lp.matvec_s;
+    } else if (lz_graphs_enabled()) {
+      // the device-looped solve: the bond's operator is staged into the lane's fixed slots,
+      // so the cached graph of this shape serves it
+      const ll dd = (ll)d_ * d_;
+      const T *sL = stage_op(ln().opL, lenv_[i], (ll)cL * Dl * cL), *sR = stage_op(ln().opR, renv_[i + 2], (ll)cR * Dr * cR),
+              *sW = stage_op(ln().opW, wwt_[i], Dl * dd * dd * Dr);
+      auto mvs = [&](const T* in, T* out, const int* skip) {
+        heff_apply(sL, sR, sW, in, out, ln().X, ln().Y, cL, cR, d_, Dl, Dr, skip, ln().st);
+      };
+      const LzKey key{2, cL, cR, Dl, Dr, d_, (ll)sL, (ll)sR, (ll)sW, (ll)ln().X, (ll)ln().Y, 0};
+      r = lanczos_solve<T>(ln().lw, ln().theta, n, cfg_.krylov_max, cfg_.lanczos_tol, cfg_.max_restarts,
+                           cfg_.seed + 7919u * (unsigned)i, mvs, ln().st, &key);
     } else {
       r = lanczos_solve<T>(ln().lw, ln().theta, n, cfg_.krylov_max, cfg_.lanczos_tol, cfg_.max_restarts,
                            cfg_.seed + 7919u * (unsigned)i, mv, ln().st);
@@ -745,6 +773,7 @@ class Engine final : public EngineBase {
     ss.matvecs += r.matvecs;
     ss.heff_flops += fl * r.matvecs;
     ss.lanczos_iters += r.iters;
+    ss.device_loops += r.device_loops;
     if (!r.converged) ss.lanczos_unconverged += 1;
     return r.energy;
   }
@@ -781,15 +810,21 @@ class Engine final : public EngineBase {
     const int Dl = Db_[i], Dr = Db_[i + 1];
     const ll n = (ll)cL * d_ * cR;
     DMRG2_CUDA(cudaMemcpyAsync(ln().theta, mps_[i], sizeof(T) * (size_t)n, cudaMemcpyDeviceToDevice, ln().st));
+    const bool graph = lz_graphs_enabled();  // staged operator, cached graph per shape
+    const T* sL = graph ? stage_op(ln().opL, lenv_[i], (ll)cL * Dl * cL) : lenv_[i];
+    const T* sR = graph ? stage_op(ln().opR, renv_[i + 1], (ll)cR * Dr * cR) : renv_[i + 1];
+    const T* sW = graph ? stage_op(ln().opW, wml_[i], (ll)d_ * Dr * Dl * d_) : wml_[i];
     auto mv = [&](const T* in, T* out, const int* skip) {
-      heff1_apply(lenv_[i], renv_[i + 1], wml_[i], in, out, ln().X, ln().Y, cL, cR, d_, Dl, Dr, skip, ln().st);
+      heff1_apply(sL, sR, sW, in, out, ln().X, ln().Y, cL, cR, d_, Dl, Dr, skip, ln().st);
     };
+    const LzKey key{1, cL, cR, Dl, Dr, d_, (ll)sL, (ll)sR, (ll)sW, (ll)ln().X, (ll)ln().Y, 0};
     LanczosResult r = lanczos_solve<T>(ln().lw, ln().theta, n, cfg_.krylov_max, cfg_.lanczos_tol, cfg_.max_restarts,
-                                       cfg_.seed + 7919u * (unsigned)i, mv, ln().st);
+                                       cfg_.seed + 7919u * (unsigned)i, mv, ln().st, graph ? &key : nullptr);
     ss.heff_s += r.matvec_s;
     ss.matvecs += r.matvecs;
     ss.heff_flops += heff1_flops(cL, cR, d_, Dl, Dr, ST<T>::cplx) * r.matvecs;
     ss.lanczos_iters += r.iters;
+    ss.device_loops += r.device_loops;
     if (!r.converged) ss.lanczos_unconverged += 1;
     return r.energy;
   }
@@ -999,6 +1034,9 @@ class Engine final : public EngineBase {
   struct Lane {
     cudaStream_t st = nullptr;
     T *theta = nullptr, *X = nullptr, *Y = nullptr, *svdX = nullptr, *svdQ = nullptr, *tmp = nullptr;
+    // the bond's operator (left and right environments, fused or single-site MPO) staged
+    // into fixed slots, so one cached device-looped Lanczos graph serves every bond of a shape
+    T *opL = nullptr, *opR = nullptr, *opW = nullptr;
     LanczosWork<T> lw;
     EigWork<T> ew;
     WstWork wst;     // warm-started subspace split (real data)
@@ -1068,6 +1106,9 @@ class Engine final : public EngineBase {
     if (!primary && mpo_set_) {  // lane 0's X, Y are carved from the MPO slab
       l.X = (T*)al(sizeof(T) * (size_t)xs_);
       l.Y = (T*)al(sizeof(T) * (size_t)xs_);
+      l.opL = (T*)al(sizeof(T) * (size_t)opn_);
+      l.opR = (T*)al(sizeof(T) * (size_t)opn_);
+      l.opW = (T*)al(sizeof(T) * (size_t)opw_);
     }
   }
   void release_lane(Lane& l) {
@@ -1108,6 +1149,7 @@ class Engine final : public EngineBase {
   size_t bytes_ = 0, bytes_mpo_ = 0;
   ll nmax_ = 0, qmax_ = 0;
   ll xs_ = 0;  // elements of each contraction scratch buffer ln().X, ln().Y
+  ll opn_ = 0, opw_ = 0;  // elements of the staged operator slots (environments, MPO)
   bool mpo_set_ = false, mps_set_ = false, canonical_ = false;
   double energy_ = 0.0, env_build_s_ = 0.0;
 };
@@ -1132,7 +1174,7 @@ size_t engine_footprint(const EngineConfig& c, const std::vector<int>& Dl, const
   b += 2 * el(nmax) + el(qmax * qmax) + el(chi * chi);
   const int kcap = std::min(std::max(c.krylov_max, 2), KRYLOV_CAP);
   const ll nblk = vec_blocks(nmax);
-  b += sb * ((size_t)kcap + 1) * (size_t)nmax + sizeof(LanczosDev) + sizeof(double) * (size_t)nblk * 2 * (KRYLOV_CAP + 2);
+  b += sb * ((size_t)kcap + 2) * (size_t)nmax + sizeof(LanczosDev) + sizeof(double) * (size_t)nblk * 2 * (KRYLOV_CAP + 2);
   {
     const size_t nn = (size_t)qmax, kk = (size_t)std::max<ll>(std::min<ll>(chi, qmax), 1);
     b += sb * nn * nn + 2 * sizeof(double) * nn + sb * nn + sizeof(double) * kk + 2 * sizeof(double) * nn * kk +
@@ -1152,7 +1194,14 @@ size_t engine_footprint(const EngineConfig& c, const std::vector<int>& Dl, const
   std::vector<ll> Db(L + 1, 1);
   for (int i = 0; i < L; ++i) Db[i] = Dl[i];
   Db[L] = Dr[L - 1];
-  for (int i = 0; i <= L; ++i) b += 2 * el(cap[i] * cap[i] * Db[i]);
+  ll opn = 1, opw = 1;
+  for (int i = 0; i <= L; ++i) {
+    b += 2 * el(cap[i] * cap[i] * Db[i]);
+    opn = std::max(opn, cap[i] * cap[i] * Db[i]);
+  }
+  for (int i = 0; i < L; ++i) opw = std::max(opw, (ll)d * Dr[i] * Dl[i] * d);
+  for (int i = 0; i + 1 < L; ++i) opw = std::max(opw, (ll)d * d * Dr[i + 1] * Dl[i] * d * d);
+  b += 2 * el(opn) + el(opw);
   ll xs = 1;
   const ll dd = (ll)d * d;
   for (int i = 0; i + 1 < L; ++i) {

@@ -73,6 +73,7 @@ struct SweepStats {
   int rsvd_fallbacks = 0;    // bonds where it gave up and the exact split ran
   int eig_fallbacks = 0;     // bonds where the density-matrix eigenvectors could not be made
                              // orthonormal and the Jacobi SVD split the bond
+  int device_loops = 0;      // Lanczos solves run as a device-looped graph (restarts counted)
 };
 
 class EngineBase {

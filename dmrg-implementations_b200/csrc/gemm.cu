@@ -14,6 +14,11 @@ std::atomic<long long>& launch_counter() {
   return c;
 }
 
+long long& thread_launches() {
+  thread_local long long c = 0;
+  return c;
+}
+
 namespace {
 // the calling thread's private stream for pool calls on the current device
 cudaStream_t pool_stream(int& device) {
@@ -253,6 +258,8 @@ std::unordered_map<TuneKey, TuneChoice, TuneKeyHash>& tune_cache() {
   static auto* c = new std::unordered_map<TuneKey, TuneChoice, TuneKeyHash>();
   return *c;
 }
+}  // namespace
+
 bool tune_enabled() {
   static const bool on = [] {
     const char* e = std::getenv("DMRG2_GEMM_TUNE");
@@ -261,6 +268,7 @@ bool tune_enabled() {
   return on;
 }
 
+namespace {
 TuneChoice tuned(const Gemm<double>& d, cudaStream_t st) {
   int dev = 0;
   DMRG2_CUDA(cudaGetDevice(&dev));

@@ -22,7 +22,11 @@ struct LanczosDev {
   int n_iter;                          // size of the tridiagonal matrix
   int randomized;
   int kmax;
-  int pad[3];
+  int j;                               // Krylov index of the device-looped solve's current step
+  int guard;                           // loop bodies run so far (bounds the device loop)
+  int pad;
+  unsigned long long t_mark;           // %globaltimer when the current matvec was issued
+  unsigned long long mv_ns;            // matvec time accumulated by the device-looped solve
 };
 
 // Reduction scratch shared by the vector kernels.
@@ -44,10 +48,18 @@ void lz_update_norm_check(const T* V, int nv, ll n, T* w, LanczosDev* st, RedScr
                           int kmax, cudaStream_t s);
 template <typename T>
 void lz_normalize_next(T* vnext, const T* w, ll n, LanczosDev* st, cudaStream_t s);
-// start: nrm(theta) -> (random fill if ~0) -> v0 = theta/|theta|
+// start: nrm(theta) -> (random fill if ~0) -> v0 = theta/|theta| (also into cur when given)
 template <typename T>
 void lz_start(T* theta, T* v0, ll n, LanczosDev* st, RedScratch& r, unsigned seed, double tol,
-              int kmax, cudaStream_t s);
+              int kmax, cudaStream_t s, T* cur = nullptr);
+// The same step with the Krylov index read on the device (st->j), for a loop that runs
+// without the host: the three passes over w = H v_j, then v_(j+1) into V and into cur
+// (the matvec's fixed input).
+template <typename T>
+void lz_step_dev(const T* V, ll n, T* w, T* cur, LanczosDev* st, RedScratch& r, int kmax, cudaStream_t s);
+// Ends one body of the device loop: advances st->j and sets the loop condition to
+// "not done and fewer than kmax bodies run".
+void lz_loop_next(LanczosDev* st, cudaGraphConditionalHandle h, int kmax, cudaStream_t s);
 // Ritz vector out = sum_i ritz_i V_i, normalised.
 template <typename T>
 void lz_ritz(const T* V, ll n, T* out, LanczosDev* st, RedScratch& r, cudaStream_t s);

@@ -209,17 +209,29 @@ __device__ void tridiag_vector(const double* a, const double* b, int k, double l
   }
 }
 
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 // ----------------------------------------------------------------------------
 // the fused streaming kernel
 //   PHASE 0: coef_i = <v_i, w>              (i < nv), nrm2 = |w|^2; alpha_j = Re coef_j
 //   PHASE 1: w -= sum coef_i v_i; coef_i = <v_i, w>; alpha_j += Re coef_j
 //   PHASE 2: w -= sum coef_i v_i; beta_j = |w|; convergence check
+// nv < 0: the device-looped solve; nv = st->j + 1, and PHASE 0 (the first kernel after
+// the matvec) adds the matvec's time since st->t_mark to st->mv_ns
 // ----------------------------------------------------------------------------
 template <typename T, int PHASE>
 __global__ void __launch_bounds__(VEC_THREADS)
     lz_pass_kernel(const T* __restrict__ V, int nv, ll n, T* __restrict__ w, LanczosDev* st,
                    double* part, unsigned* counter, int kmax) {
   if (*((volatile int*)&st->done)) return;
+  if (nv < 0) {
+    if (PHASE == 0 && blockIdx.x == 0 && threadIdx.x == 0) st->mv_ns += global_ns() - st->t_mark;
+    nv = st->j + 1;
+  }
   constexpr bool CPLX = ST<T>::cplx;
   constexpr int NW = VEC_THREADS / 32;
   __shared__ T ws[MAX_CHUNK];
@@ -329,6 +341,32 @@ __global__ void lz_normalize_kernel(T* __restrict__ vnext, const T* __restrict__
     vnext[x] = ST<T>::scale(inv, w[x]);
 }
 
+// device-looped form: v_(j+1) = w / |w| into V[j + 1] and into cur, j = st->j
+template <typename T>
+__global__ void lz_normalize_dev_kernel(T* __restrict__ V, T* __restrict__ cur, const T* __restrict__ w,
+                                        ll n, LanczosDev* st) {
+  if (*((volatile int*)&st->done)) return;
+  const int j1 = st->j + 1;
+  if (j1 >= st->kmax) return;
+  double inv = 1.0 / sqrt(st->nrm2);
+  T* vnext = V + (ll)j1 * n;
+  for (ll x = (ll)blockIdx.x * blockDim.x + threadIdx.x; x < n; x += (ll)gridDim.x * blockDim.x) {
+    const T v = ST<T>::scale(inv, w[x]);
+    vnext[x] = v;
+    cur[x] = v;
+  }
+}
+
+// last node of the device loop's body (one thread)
+__global__ void lz_loop_next_kernel(LanczosDev* st, cudaGraphConditionalHandle h, int kmax) {
+  const int g = st->guard + 1;
+  st->guard = g;
+  const int done = *((volatile int*)&st->done);
+  if (!done) st->j += 1;
+  st->t_mark = global_ns();
+  cudaGraphSetConditional(h, (!done && g < kmax) ? 1u : 0u);
+}
+
 // |x|^2 into st->nrm2 (or out), last-block finalize
 template <typename T>
 __global__ void norm2_kernel(const T* __restrict__ x, ll n, double* out, double* part,
@@ -379,14 +417,23 @@ __global__ void lz_reset_kernel(T* theta, ll n, LanczosDev* st, unsigned seed, d
     st->e_cur = 0.0;
     st->tol = tol;
     st->kmax = kmax;
+    st->j = 0;
+    st->guard = 0;
+    st->t_mark = 0ull;
+    st->mv_ns = 0ull;
   }
 }
 
 template <typename T>
-__global__ void lz_v0_kernel(const T* __restrict__ theta, T* __restrict__ v0, ll n, LanczosDev* st) {
+__global__ void lz_v0_kernel(const T* __restrict__ theta, T* __restrict__ v0, ll n, LanczosDev* st,
+                             T* __restrict__ cur) {
   double inv = 1.0 / sqrt(st->nrm2);
-  for (ll x = (ll)blockIdx.x * blockDim.x + threadIdx.x; x < n; x += (ll)gridDim.x * blockDim.x)
-    v0[x] = ST<T>::scale(inv, theta[x]);
+  for (ll x = (ll)blockIdx.x * blockDim.x + threadIdx.x; x < n; x += (ll)gridDim.x * blockDim.x) {
+    const T v = ST<T>::scale(inv, theta[x]);
+    v0[x] = v;
+    if (cur) cur[x] = v;
+  }
+  if (cur && blockIdx.x == 0 && threadIdx.x == 0) st->t_mark = global_ns();
 }
 
 template <typename T>
@@ -453,12 +500,29 @@ void norm2(const T* x, ll n, double* out_dev, RedScratch& r, cudaStream_t s) {
 
 template <typename T>
 void lz_start(T* theta, T* v0, ll n, LanczosDev* st, RedScratch& r, unsigned seed, double tol,
-              int kmax, cudaStream_t s) {
+              int kmax, cudaStream_t s, T* cur) {
   norm2<T>(theta, n, &st->nrm2, r, s);
   lz_reset_kernel<T><<<grid_for(n), VEC_THREADS, 0, s>>>(theta, n, st, seed, tol, kmax);
   DMRG2_CHECK_LAUNCH();
   norm2<T>(theta, n, &st->nrm2, r, s);
-  lz_v0_kernel<T><<<grid_for(n), VEC_THREADS, 0, s>>>(theta, v0, n, st);
+  lz_v0_kernel<T><<<grid_for(n), VEC_THREADS, 0, s>>>(theta, v0, n, st, cur);
+  DMRG2_CHECK_LAUNCH();
+}
+
+template <typename T>
+void lz_step_dev(const T* V, ll n, T* w, T* cur, LanczosDev* st, RedScratch& r, int kmax, cudaStream_t s) {
+  lz_pass_kernel<T, 0><<<vec_blocks(n), VEC_THREADS, 0, s>>>(V, -1, n, w, st, r.part, r.counter, 0);
+  DMRG2_CHECK_LAUNCH();
+  lz_pass_kernel<T, 1><<<vec_blocks(n), VEC_THREADS, 0, s>>>(V, -1, n, w, st, r.part, r.counter, 0);
+  DMRG2_CHECK_LAUNCH();
+  lz_pass_kernel<T, 2><<<vec_blocks(n), VEC_THREADS, 0, s>>>(V, -1, n, w, st, r.part, r.counter, kmax);
+  DMRG2_CHECK_LAUNCH();
+  lz_normalize_dev_kernel<T><<<grid_for(n), VEC_THREADS, 0, s>>>(const_cast<T*>(V), cur, w, n, st);
+  DMRG2_CHECK_LAUNCH();
+}
+
+void lz_loop_next(LanczosDev* st, cudaGraphConditionalHandle h, int kmax, cudaStream_t s) {
+  lz_loop_next_kernel<<<1, 1, 0, s>>>(st, h, kmax);
   DMRG2_CHECK_LAUNCH();
 }
 
@@ -484,7 +548,8 @@ void scale_inplace(T* x, ll n, const double* nrm2_dev, cudaStream_t s) {
                                         cudaStream_t);                                            \
   template void lz_normalize_next<T>(T*, const T*, ll, LanczosDev*, cudaStream_t);                \
   template void lz_start<T>(T*, T*, ll, LanczosDev*, RedScratch&, unsigned, double, int,      \
-                            cudaStream_t);        \
+                            cudaStream_t, T*);                                                    \
+  template void lz_step_dev<T>(const T*, ll, T*, T*, LanczosDev*, RedScratch&, int, cudaStream_t); \
   template void lz_ritz<T>(const T*, ll, T*, LanczosDev*, RedScratch&, cudaStream_t);             \
   template void norm2<T>(const T*, ll, double*, RedScratch&, cudaStream_t);                       \
   template void scale_inplace<T>(T*, ll, const double*, cudaStream_t);

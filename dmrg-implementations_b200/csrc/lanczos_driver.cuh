@@ -1,12 +1,26 @@
 // Host driver of one Lanczos ground-state solve on the device.
 //
-// The host enqueues Krylov iterations ahead of the device and polls the
-// device-side `done` flag through a small pinned ring with a lookahead of
-// POLL_LOOK iterations, so the GPU never idles on the host and at most
-// POLL_LOOK iterations of no-op launches are issued after convergence.
+// Two forms, the same arithmetic:
+//  - host-driven: the host enqueues Krylov iterations ahead of the device and polls the
+//    device-side `done` flag through a small pinned ring with a lookahead of POLL_LOOK
+//    iterations, so the GPU never idles on the host and at most POLL_LOOK iterations of
+//    no-op launches are issued after convergence;
+//  - device-looped: one CUDA graph per matvec identity (operator shapes and the fixed
+//    buffers it reads and writes) holds a conditional WHILE node whose body is one Krylov
+//    step (matvec, the three vector passes, the normalisation, and a one-thread kernel
+//    that advances the index and ends the loop on convergence or after kmax bodies). The
+//    host launches the graph once per restart and reads the result once; no flags cross
+//    to the host between steps and no no-op steps are issued. A call site opts in by
+//    passing a key; the first solve with a new key runs host-driven and then captures the
+//    graph, and at most LZ_GRAPH_CAP graphs per work area are kept (least recently used
+//    ones go first).
 #pragma once
 
 #include <algorithm>
+#include <array>
+#include <atomic>
+#include <cstdio>
+#include <cstdlib>
 #include <functional>
 #include <stdexcept>
 #include <vector>
@@ -16,12 +30,53 @@
 
 namespace dmrg2 {
 
+// identifies a matvec for the graph cache: operator shapes and device pointers, chosen by
+// the caller (unused entries 0); the solve adds n and kmax
+using LzKey = std::array<long long, 14>;
+
+inline std::atomic<bool>& lz_graphs_broken() {
+  static std::atomic<bool> b{false};
+  return b;
+}
+
+// on unless DMRG2_LANCZOS_GRAPH=0, or while GEMMs are being tuned (the tuner times
+// candidates, which a capture cannot hold), or after a capture failed in this process
+inline bool lz_graphs_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("DMRG2_LANCZOS_GRAPH");
+    return !(e && e[0] == '0') && !tune_enabled();
+  }();
+  return on && !lz_graphs_broken().load();
+}
+
+// a converged chi=256 sweep of 100 sites meets ~100 distinct (cL, cR) bond shapes (bonds
+// below the cap keep what the cutoff leaves); a graph is a few kilobytes
+constexpr int LZ_GRAPH_CAP = 512;
+
+struct LzGraph {
+  LzKey key{};
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ex = nullptr;
+  long long body_launches = 0;  // kernels in one loop body
+  unsigned long long last_use = 0;
+  void reset() {
+    if (ex) cudaGraphExecDestroy(ex);
+    if (g) cudaGraphDestroy(g);
+    ex = nullptr;
+    g = nullptr;
+    body_launches = 0;
+  }
+};
+
 template <typename T>
 struct LanczosWork {
   static constexpr int POLL_RING = 8;
   static constexpr int POLL_LOOK = 2;
   T* krylov = nullptr;  // kcap vectors of length >= n
   T* w = nullptr;       // work vector
+  T* cur = nullptr;     // the device-looped matvec's input (a copy of the current Krylov vector)
+  std::vector<LzGraph> graphs;  // device-looped solves, by key
+  unsigned long long uses = 0;
   int kcap = 0;
   LanczosDev* st = nullptr;
   RedScratch red;
@@ -34,6 +89,7 @@ struct LanczosWork {
     kcap = std::min(kcap_, KRYLOV_CAP);
     krylov = (T*)alloc(sizeof(T) * (size_t)kcap * std::max<ll>(nmax, 1));
     w = (T*)alloc(sizeof(T) * (size_t)std::max<ll>(nmax, 1));
+    cur = (T*)alloc(sizeof(T) * (size_t)std::max<ll>(nmax, 1));
     st = (LanczosDev*)alloc(sizeof(LanczosDev));
     red.nblk = vec_blocks(nmax);
     red.part = (double*)alloc(sizeof(double) * (size_t)red.nblk * 2 * (KRYLOV_CAP + 2));
@@ -54,10 +110,12 @@ struct LanczosWork {
     return p;
   }
   size_t bytes(ll nmax) const {
-    return sizeof(T) * ((size_t)kcap + 1) * (size_t)nmax + sizeof(LanczosDev) +
+    return sizeof(T) * ((size_t)kcap + 2) * (size_t)nmax + sizeof(LanczosDev) +
            sizeof(double) * (size_t)red.nblk * 2 * (KRYLOV_CAP + 2);
   }
   void release() {
+    for (auto& g : graphs) g.reset();
+    graphs.clear();
     for (void* p : owned) dev_free(p);
     owned.clear();
     if (h_flags) host_unpin(h_flags);
@@ -77,20 +135,103 @@ struct LanczosResult {
   int matvecs = 0;
   int converged = 0;
   double matvec_s = 0.0;  // device time of the matvecs
+  int device_loops = 0;   // restarts run as the device-looped graph
 };
+
+// Captures the device loop of W's buffers and this matvec into G. Nothing runs: the body's
+// kernels are recorded on s (which may still hold queued work), and the launch counters
+// drop them again (each run of the graph adds its executed bodies).
+template <typename T>
+void lz_build_graph(LanczosWork<T>& W, LzGraph& G, ll n, int kmax,
+                    const std::function<void(const T*, T*, const int*)>& matvec, cudaStream_t s) {
+  DMRG2_CUDA(cudaGraphCreate(&G.g, 0));
+  cudaGraphConditionalHandle h;
+  DMRG2_CUDA(cudaGraphConditionalHandleCreate(&h, G.g, 1, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams p{};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = h;
+  p.conditional.type = cudaGraphCondTypeWhile;
+  p.conditional.size = 1;
+  cudaGraphNode_t node;
+  DMRG2_CUDA(cudaGraphAddNode(&node, G.g, nullptr, 0, &p));
+  cudaGraph_t body = p.conditional.phGraph_out[0];
+  const long long t0 = thread_launches();
+  DMRG2_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  try {
+    matvec(W.cur, W.w, &W.st->done);
+    lz_step_dev(W.krylov, n, W.w, W.cur, W.st, W.red, kmax, s);
+    lz_loop_next(W.st, h, kmax, s);
+  } catch (...) {
+    cudaGraph_t t = nullptr;
+    cudaStreamEndCapture(s, &t);
+    const long long nb = thread_launches() - t0;
+    thread_launches() -= nb;
+    launch_counter() -= nb;
+    throw;
+  }
+  cudaGraph_t t = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(s, &t);
+  G.body_launches = thread_launches() - t0;
+  thread_launches() -= G.body_launches;
+  launch_counter() -= G.body_launches;
+  DMRG2_CUDA(e);
+  DMRG2_CUDA(cudaGraphInstantiate(&G.ex, G.g, 0));
+}
 
 // matvec(in, out, skip_flag) enqueues out = H in on stream s, doing nothing when
 // *skip_flag != 0 on the device. theta: start vector on entry, normalised Ritz
-// vector on exit.
+// vector on exit. With a key: the device-looped form, cached in W.graphs (the key must
+// identify everything the matvec reads and writes besides in and out).
 template <typename T>
 LanczosResult lanczos_solve(LanczosWork<T>& W, T* theta, ll n, int krylov_max, double tol,
                             int max_restarts, unsigned seed,
                             const std::function<void(const T*, T*, const int*)>& matvec,
-                            cudaStream_t s) {
+                            cudaStream_t s, const LzKey* key = nullptr) {
   LanczosResult res;
   const int kmax = (int)std::min<ll>(std::min(krylov_max, W.kcap), n);
   if (kmax < 1) throw std::runtime_error("lanczos: empty problem");
+  LzGraph* G = nullptr;
+  bool build = false;
+  if (key && lz_graphs_enabled()) {
+    LzKey k = *key;
+    k[12] = n;
+    k[13] = kmax;
+    for (auto& g : W.graphs)
+      if (g.ex && g.key == k) G = &g;
+    if (!G) {
+      if ((int)W.graphs.size() < LZ_GRAPH_CAP) {
+        W.graphs.emplace_back();
+        G = &W.graphs.back();
+      } else {
+        G = &*std::min_element(W.graphs.begin(), W.graphs.end(),
+                               [](const LzGraph& a, const LzGraph& b) { return a.last_use < b.last_use; });
+        G->reset();
+      }
+      G->key = k;
+      build = true;
+    }
+    G->last_use = ++W.uses;
+  }
   for (int rs = 0; rs <= max_restarts; ++rs) {
+    if (G && G->ex) {
+      lz_start(theta, W.krylov, n, W.st, W.red, seed + 104729u * (unsigned)rs, tol, kmax, s, W.cur);
+      DMRG2_CUDA(cudaGraphLaunch(G->ex, s));
+      lz_ritz(W.krylov, n, theta, W.st, W.red, s);
+      DMRG2_CUDA(cudaMemcpyAsync(W.h_st, W.st, sizeof(LanczosDev), cudaMemcpyDeviceToHost, s));
+      DMRG2_CUDA(cudaStreamSynchronize(s));
+      if (!W.h_st->done || W.h_st->n_iter < 1) throw std::runtime_error("Lanczos did not terminate");
+      const int bodies = W.h_st->guard;
+      launch_counter() += bodies * G->body_launches;
+      thread_launches() += bodies * G->body_launches;
+      res.matvecs += bodies;
+      res.iters += W.h_st->n_iter;
+      res.energy = W.h_st->e_cur;
+      res.matvec_s += (double)W.h_st->mv_ns * 1e-9;
+      res.converged = W.h_st->converged;
+      res.device_loops += 1;
+      if (res.converged) break;
+      continue;
+    }
     lz_start(theta, W.krylov, n, W.st, W.red, seed + 104729u * (unsigned)rs, tol, kmax, s);
     int issued = 0;
     for (int j = 0; j < kmax; ++j) {
@@ -127,6 +268,17 @@ LanczosResult lanczos_solve(LanczosWork<T>& W, T* theta, ll n, int krylov_max, d
     lz_ritz(W.krylov, n, theta, W.st, W.red, s);
     res.converged = W.h_st->converged;
     if (res.converged) break;
+  }
+  if (build) {
+    try {
+      lz_build_graph(W, *G, n, kmax, matvec, s);
+    } catch (const std::exception& e) {
+      // the host-driven form stays correct: use it from now on, and say why once
+      G->reset();
+      cudaGetLastError();
+      if (!lz_graphs_broken().exchange(true))
+        std::fprintf(stderr, "dmrg2: device-looped Lanczos disabled (graph capture failed: %s)\n", e.what());
+    }
   }
   return res;
 }

@@ -65,7 +65,7 @@ class SweepReport(ctypes.Structure):
         ("svd_s", ctypes.c_double), ("jacobi_sweeps_max", ctypes.c_int), ("device_s", ctypes.c_double),
         ("lowprec_matvecs", ctypes.c_longlong), ("warm_splits", ctypes.c_int), ("warm_fallbacks", ctypes.c_int),
         ("eig_fallbacks", ctypes.c_int), ("warm_short", ctypes.c_int), ("rsvd_splits", ctypes.c_int),
-        ("rsvd_fallbacks", ctypes.c_int), ("phase", ctypes.c_int),
+        ("rsvd_fallbacks", ctypes.c_int), ("phase", ctypes.c_int), ("device_loops", ctypes.c_int),
     ]
 
     def as_dict(self):

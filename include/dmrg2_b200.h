@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define DMRG2_ABI_VERSION 6
+#define DMRG2_ABI_VERSION 7
 
 enum dmrg2_status {
   DMRG2_OK = 0,
@@ -121,6 +121,9 @@ typedef struct dmrg2_sweep_report {
   int rsvd_fallbacks;        /* bonds where it could not orthonormalise its sketch */
   int phase;                 /* 0 = sweep (dmrg2_run / dmrg2_resume); dmrg2_pdmrg_run: 1 = warm-up
                                 sweep, 2 = outer iteration, 3 = recalibration sweep, 4 = polish */
+  int device_loops;          /* Lanczos solves (restarts counted) run as one cached CUDA graph
+                                whose conditional loop iterates the Krylov steps on the device
+                                (the rest: host-driven, e.g. the first solve of each bond shape) */
 } dmrg2_sweep_report;
 
 /* ---------------------------------------------------------------- solver */

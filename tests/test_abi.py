@@ -40,7 +40,7 @@ def test_python_mirror_binds_every_declared_symbol():
 
 
 def test_abi_version(lib):
-    assert lib.dmrg2_abi_version() == 6
+    assert lib.dmrg2_abi_version() == 7
 
 
 def test_null_arguments_are_rejected_without_touching_the_gpu(lib):

@@ -349,3 +349,65 @@ def test_rsvd_split_against_exact_split(model):
         a = A[k].reshape(A[k].shape[0], -1)
         np.testing.assert_allclose(a @ a.conj().T, np.eye(a.shape[0]), atol=1e-12)
     assert abs(O.mpo_expectation(A, mpo).real - rr[-1]["energy"]) < 1e-9
+
+
+LOOP_CHILD = r"""
+import hashlib, json
+import numpy as np
+import dmrg2
+from oracle import dmrg2_oracle as O
+from oracle import models as M
+out = {}
+def run(tag, mpo, mps, sched, **kw):
+    L, d = len(mpo), mpo[0].shape[2]
+    cplx = np.iscomplexobj(mpo[0]) or np.iscomplexobj(mps[0])
+    eng = dmrg2.DMRG2GPU(L, d, max(sched), dtype=np.complex128 if cplx else np.float64, tol=1e-300,
+                         min_sweeps=100, **kw)
+    eng.set_mpo(mpo)
+    eng.set_mps(mps)
+    c0 = dmrg2.launch_count()
+    rep = eng.run(schedule=sched)
+    launches = dmrg2.launch_count() - c0
+    h = hashlib.sha256()
+    for a in eng.get_mps():
+        h.update(np.ascontiguousarray(a).tobytes())
+    out[tag] = {"energies": [r["energy"].hex() for r in rep], "matvecs": [r["matvecs"] for r in rep],
+                "mps": h.hexdigest(), "launches": launches, "loops": sum(r["device_loops"] for r in rep),
+                "bonds": sum(1 for r in rep) * (L - 1) * 2}
+    eng.close()
+run("heis_L24", M.heisenberg_mpo(24), O.random_mps(24, 2, 16, seed=3), [16, 32, 64, 64, 64], krylov_max=30,
+    max_restarts=2, cutoff=1e-12)
+run("jos_L8_c128", M.josephson_mpo(8, n_max=1, E_J=2.0, E_C=1.0, n_g=0.25, phi=0.4, onsite="shifted"),
+    O.random_mps(8, 3, 16, seed=6, dtype=np.complex128), [32] * 4, krylov_max=30, max_restarts=2, cutoff=1e-14)
+run("heis_L12_single", M.heisenberg_mpo(12), O.random_mps(12, 2, 32, seed=5), [32] * 4, krylov_max=40,
+    max_restarts=4, cutoff=1e-14, single_site=True)
+print("RESULT" + json.dumps(out))
+"""
+
+
+def test_device_looped_lanczos_equals_host_driven():
+    """The device-looped Lanczos (one cached CUDA graph per operator shape: a conditional
+    WHILE node over matvec, vector passes and normalisation) does the same arithmetic as
+    the host-driven loop: per-sweep energies and the final MPS are bitwise equal for real
+    and complex two-site sweeps and for single-site sweeps, with the same matvec counts;
+    only the first solve of each operator shape runs host-driven."""
+    import os
+    import sys
+    res = {}
+    for mode in ("0", "1"):
+        env = dict(os.environ, DMRG2_LANCZOS_GRAPH=mode,
+                   PYTHONPATH=os.pathsep.join([str(REPO / "dmrg-implementations_b200"), str(REPO)]))
+        r = subprocess.run([sys.executable, "-c", LOOP_CHILD], env=env, capture_output=True, text=True,
+                           timeout=600)
+        assert r.returncode == 0, r.stderr
+        assert "Lanczos disabled" not in r.stderr, r.stderr
+        res[mode] = json.loads(r.stdout.split("RESULT")[1])
+    for tag in res["0"]:
+        host, dev = res["0"][tag], res["1"][tag]
+        print(tag, "launches host-driven", host["launches"], "device-looped", dev["launches"],
+              "device loops", dev["loops"], "of", dev["bonds"], "solves")
+        assert dev["energies"] == host["energies"], tag
+        assert dev["mps"] == host["mps"], tag
+        assert dev["matvecs"] == host["matvecs"], tag
+        assert host["loops"] == 0, tag
+        assert dev["loops"] >= dev["bonds"] // 2, tag
