@@ -1,0 +1,129 @@
+// Cached CUDA graphs of the per-bond launch sequences.
+//
+// A sequence that the host would otherwise launch kernel by kernel (a Lanczos solve, a
+// warm-started split) is captured once into a graph and replayed with one launch while
+// its key (shapes and the device buffers it reads and writes) stays the same. Replays do
+// the same arithmetic in the same order as the launches they stand for, so results are
+// bitwise the same with graphs on or off.
+#pragma once
+
+#include <array>
+#include <atomic>
+#include <cstdio>
+#include <cstdlib>
+#include <functional>
+#include <vector>
+
+#include "common.cuh"
+
+namespace dmrg2 {
+
+using GraphKey = std::array<long long, 16>;
+
+inline std::atomic<bool>& graphs_broken() {
+  static std::atomic<bool> b{false};
+  return b;
+}
+
+// on unless DMRG2_GRAPHS=0, or while GEMMs are being tuned (the tuner times candidates,
+// which a capture cannot hold), or after a capture failed in this process
+inline bool graphs_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("DMRG2_GRAPHS");
+    return !(e && e[0] == '0') && !tune_enabled();
+  }();
+  return on && !graphs_broken().load();
+}
+
+// the launch sequences stay correct without graphs: use them from now on, and say why once
+inline void graphs_disable(const char* why) {
+  cudaGetLastError();
+  if (!graphs_broken().exchange(true)) std::fprintf(stderr, "dmrg2: CUDA graphs disabled (capture failed: %s)\n", why);
+}
+
+struct GraphEntry {
+  GraphKey key{};
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ex = nullptr;
+  long long launches = 0;  // kernels one replay runs (per loop body for a looped graph)
+  unsigned long long last_use = 0;
+  void reset() {
+    if (ex) cudaGraphExecDestroy(ex);
+    if (g) cudaGraphDestroy(g);
+    ex = nullptr;
+    g = nullptr;
+    launches = 0;
+  }
+};
+
+// At most `cap` graphs; the least recently used goes first.
+struct GraphCache {
+  std::vector<GraphEntry> e;
+  unsigned long long uses = 0;
+  int cap = 256;
+
+  GraphEntry* find(const GraphKey& k) {
+    for (auto& g : e)
+      if (g.ex && g.key == k) {
+        g.last_use = ++uses;
+        return &g;
+      }
+    return nullptr;
+  }
+  // an empty entry carrying key k (evicting the least recently used one when full)
+  GraphEntry* slot(const GraphKey& k) {
+    GraphEntry* g = nullptr;
+    if ((int)e.size() < cap) {
+      e.emplace_back();
+      g = &e.back();
+    } else {
+      g = &e[0];
+      for (auto& x : e)
+        if (x.last_use < g->last_use) g = &x;
+      g->reset();
+    }
+    g->key = k;
+    g->last_use = ++uses;
+    return g;
+  }
+  void clear() {
+    for (auto& g : e) g.reset();
+    e.clear();
+  }
+};
+
+// Records what fn() enqueues on s into graph g (nothing runs; s may still hold queued
+// work) and returns the number of kernels recorded. The launch counters drop them
+// again: each replay adds what it runs.
+inline long long capture_to_graph(cudaStream_t s, cudaGraph_t g, const std::function<void()>& fn) {
+  const long long t0 = thread_launches();
+  auto undo = [&]() {
+    const long long nb = thread_launches() - t0;
+    thread_launches() -= nb;
+    launch_counter() -= nb;
+    return nb;
+  };
+  DMRG2_CUDA(cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  try {
+    fn();
+  } catch (...) {
+    cudaGraph_t t = nullptr;
+    cudaStreamEndCapture(s, &t);
+    undo();
+    throw;
+  }
+  cudaGraph_t t = nullptr;
+  const cudaError_t err = cudaStreamEndCapture(s, &t);
+  const long long nb = undo();
+  DMRG2_CUDA(err);
+  return nb;
+}
+
+// a replay of G on s: counts its kernels as launched
+inline void graph_replay(const GraphEntry& G, cudaStream_t s, long long bodies = 1) {
+  DMRG2_CUDA(cudaGraphLaunch(G.ex, s));
+  launch_counter() += bodies * G.launches;
+  thread_launches() += bodies * G.launches;
+}
+
+}  // namespace dmrg2

@@ -12,8 +12,7 @@
 //    host launches the graph once per restart and reads the result once; no flags cross
 //    to the host between steps and no no-op steps are issued. A call site opts in by
 //    passing a key; the first solve with a new key runs host-driven and then captures the
-//    graph, and at most LZ_GRAPH_CAP graphs per work area are kept (least recently used
-//    ones go first).
+//    graph (graphs.cuh holds the cache).
 #pragma once
 
 #include <algorithm>
@@ -26,6 +25,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "graphs.cuh"
 #include "kernels.cuh"
 
 namespace dmrg2 {
@@ -34,39 +34,9 @@ namespace dmrg2 {
 // the caller (unused entries 0); the solve adds n and kmax
 using LzKey = std::array<long long, 14>;
 
-inline std::atomic<bool>& lz_graphs_broken() {
-  static std::atomic<bool> b{false};
-  return b;
-}
-
-// on unless DMRG2_LANCZOS_GRAPH=0, or while GEMMs are being tuned (the tuner times
-// candidates, which a capture cannot hold), or after a capture failed in this process
-inline bool lz_graphs_enabled() {
-  static const bool on = [] {
-    const char* e = std::getenv("DMRG2_LANCZOS_GRAPH");
-    return !(e && e[0] == '0') && !tune_enabled();
-  }();
-  return on && !lz_graphs_broken().load();
-}
-
 // a converged chi=256 sweep of 100 sites meets ~100 distinct (cL, cR) bond shapes (bonds
 // below the cap keep what the cutoff leaves); a graph is a few kilobytes
 constexpr int LZ_GRAPH_CAP = 512;
-
-struct LzGraph {
-  LzKey key{};
-  cudaGraph_t g = nullptr;
-  cudaGraphExec_t ex = nullptr;
-  long long body_launches = 0;  // kernels in one loop body
-  unsigned long long last_use = 0;
-  void reset() {
-    if (ex) cudaGraphExecDestroy(ex);
-    if (g) cudaGraphDestroy(g);
-    ex = nullptr;
-    g = nullptr;
-    body_launches = 0;
-  }
-};
 
 template <typename T>
 struct LanczosWork {
@@ -75,8 +45,7 @@ struct LanczosWork {
   T* krylov = nullptr;  // kcap vectors of length >= n
   T* w = nullptr;       // work vector
   T* cur = nullptr;     // the device-looped matvec's input (a copy of the current Krylov vector)
-  std::vector<LzGraph> graphs;  // device-looped solves, by key
-  unsigned long long uses = 0;
+  GraphCache graphs;    // device-looped solves, by key
   int kcap = 0;
   LanczosDev* st = nullptr;
   RedScratch red;
@@ -86,6 +55,7 @@ struct LanczosWork {
   std::vector<void*> owned;
 
   void init(int kcap_, ll nmax) {
+    graphs.cap = LZ_GRAPH_CAP;
     kcap = std::min(kcap_, KRYLOV_CAP);
     krylov = (T*)alloc(sizeof(T) * (size_t)kcap * std::max<ll>(nmax, 1));
     w = (T*)alloc(sizeof(T) * (size_t)std::max<ll>(nmax, 1));
@@ -114,7 +84,6 @@ struct LanczosWork {
            sizeof(double) * (size_t)red.nblk * 2 * (KRYLOV_CAP + 2);
   }
   void release() {
-    for (auto& g : graphs) g.reset();
     graphs.clear();
     for (void* p : owned) dev_free(p);
     owned.clear();
@@ -138,11 +107,9 @@ struct LanczosResult {
   int device_loops = 0;   // restarts run as the device-looped graph
 };
 
-// Captures the device loop of W's buffers and this matvec into G. Nothing runs: the body's
-// kernels are recorded on s (which may still hold queued work), and the launch counters
-// drop them again (each run of the graph adds its executed bodies).
+// Captures the device loop of W's buffers and this matvec into G (nothing runs).
 template <typename T>
-void lz_build_graph(LanczosWork<T>& W, LzGraph& G, ll n, int kmax,
+void lz_build_graph(LanczosWork<T>& W, GraphEntry& G, ll n, int kmax,
                     const std::function<void(const T*, T*, const int*)>& matvec, cudaStream_t s) {
   DMRG2_CUDA(cudaGraphCreate(&G.g, 0));
   cudaGraphConditionalHandle h;
@@ -154,27 +121,11 @@ void lz_build_graph(LanczosWork<T>& W, LzGraph& G, ll n, int kmax,
   p.conditional.size = 1;
   cudaGraphNode_t node;
   DMRG2_CUDA(cudaGraphAddNode(&node, G.g, nullptr, 0, &p));
-  cudaGraph_t body = p.conditional.phGraph_out[0];
-  const long long t0 = thread_launches();
-  DMRG2_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-  try {
+  G.launches = capture_to_graph(s, p.conditional.phGraph_out[0], [&]() {
     matvec(W.cur, W.w, &W.st->done);
     lz_step_dev(W.krylov, n, W.w, W.cur, W.st, W.red, kmax, s);
     lz_loop_next(W.st, h, kmax, s);
-  } catch (...) {
-    cudaGraph_t t = nullptr;
-    cudaStreamEndCapture(s, &t);
-    const long long nb = thread_launches() - t0;
-    thread_launches() -= nb;
-    launch_counter() -= nb;
-    throw;
-  }
-  cudaGraph_t t = nullptr;
-  const cudaError_t e = cudaStreamEndCapture(s, &t);
-  G.body_launches = thread_launches() - t0;
-  thread_launches() -= G.body_launches;
-  launch_counter() -= G.body_launches;
-  DMRG2_CUDA(e);
+  });
   DMRG2_CUDA(cudaGraphInstantiate(&G.ex, G.g, 0));
 }
 
@@ -190,27 +141,18 @@ LanczosResult lanczos_solve(LanczosWork<T>& W, T* theta, ll n, int krylov_max, d
   LanczosResult res;
   const int kmax = (int)std::min<ll>(std::min(krylov_max, W.kcap), n);
   if (kmax < 1) throw std::runtime_error("lanczos: empty problem");
-  LzGraph* G = nullptr;
+  GraphEntry* G = nullptr;
   bool build = false;
-  if (key && lz_graphs_enabled()) {
-    LzKey k = *key;
-    k[12] = n;
-    k[13] = kmax;
-    for (auto& g : W.graphs)
-      if (g.ex && g.key == k) G = &g;
+  if (key && graphs_enabled()) {
+    GraphKey k{};
+    std::copy(key->begin(), key->end(), k.begin());
+    k[14] = n;
+    k[15] = kmax;
+    G = W.graphs.find(k);
     if (!G) {
-      if ((int)W.graphs.size() < LZ_GRAPH_CAP) {
-        W.graphs.emplace_back();
-        G = &W.graphs.back();
-      } else {
-        G = &*std::min_element(W.graphs.begin(), W.graphs.end(),
-                               [](const LzGraph& a, const LzGraph& b) { return a.last_use < b.last_use; });
-        G->reset();
-      }
-      G->key = k;
+      G = W.graphs.slot(k);
       build = true;
     }
-    G->last_use = ++W.uses;
   }
   for (int rs = 0; rs <= max_restarts; ++rs) {
     if (G && G->ex) {
@@ -221,8 +163,8 @@ LanczosResult lanczos_solve(LanczosWork<T>& W, T* theta, ll n, int krylov_max, d
       DMRG2_CUDA(cudaStreamSynchronize(s));
       if (!W.h_st->done || W.h_st->n_iter < 1) throw std::runtime_error("Lanczos did not terminate");
       const int bodies = W.h_st->guard;
-      launch_counter() += bodies * G->body_launches;
-      thread_launches() += bodies * G->body_launches;
+      launch_counter() += bodies * G->launches;
+      thread_launches() += bodies * G->launches;
       res.matvecs += bodies;
       res.iters += W.h_st->n_iter;
       res.energy = W.h_st->e_cur;
@@ -273,11 +215,8 @@ LanczosResult lanczos_solve(LanczosWork<T>& W, T* theta, ll n, int krylov_max, d
     try {
       lz_build_graph(W, *G, n, kmax, matvec, s);
     } catch (const std::exception& e) {
-      // the host-driven form stays correct: use it from now on, and say why once
       G->reset();
-      cudaGetLastError();
-      if (!lz_graphs_broken().exchange(true))
-        std::fprintf(stderr, "dmrg2: device-looped Lanczos disabled (graph capture failed: %s)\n", e.what());
+      graphs_disable(e.what());
     }
   }
   return res;

@@ -13,6 +13,7 @@
 #include "cholqr.cuh"
 #include "common.cuh"
 #include "gemm.cuh"
+#include "graphs.cuh"
 #include "kernels.cuh"
 
 namespace dmrg2 {
@@ -281,6 +282,9 @@ struct WstWork {
   int qmax = 0, kmax = 0;
   size_t bytes = 0;
   std::vector<void*> owned;
+  // the launch sequence of a split, by bond (direction, mode, shapes and the factors'
+  // buffers): a converged sweep of L sites replays ~4 L of them
+  GraphCache graphs;
 
   void* alloc(size_t b) {
     void* p = nullptr;
@@ -290,6 +294,7 @@ struct WstWork {
     return p;
   }
   void init(int qmax_, int kmax_) {
+    graphs.cap = 1024;
     qmax = std::max(qmax_, 1);
     kmax = std::max(std::min(kmax_, CHOL_MAX), 1);
     const size_t qk = (size_t)qmax * kmax;
@@ -311,6 +316,7 @@ struct WstWork {
     h_status = (int*)host_pinned(sizeof(int));
   }
   void release() {
+    graphs.clear();
     for (void* p : owned) dev_free(p);
     owned.clear();
     if (h_buf) host_unpin(h_buf);
@@ -360,7 +366,9 @@ enum WstMode { WST_FULL = 0, WST_SHORT = 1, WST_RESUME = 2 };
 // Warm-started split of theta (m x nt) at kept rank k; `warm` is B (k x nt) for 'R',
 // A (m x k) for 'L'. Writes left (m x k) and right (k x nt) and returns true, or returns
 // false (left / right undefined) when the warm start was not good enough. The host
-// waits once.
+// waits once. Everything between the status reset and that wait is one cached graph per
+// (direction, mode, shapes, buffers) when graphs are on: the first call of a key launches
+// the kernels and then captures them, later calls replay the capture.
 inline bool wst_split(WstWork& W, RedScratch& red, const double* theta, int m, int nt, char dir, int k,
                       const double* warm, double* left, double* right, double& trunc_err, cudaStream_t s,
                       WstMode mode = WST_FULL) {
@@ -427,6 +435,7 @@ inline bool wst_split(WstWork& W, RedScratch& red, const double* theta, int m, i
     chol_tiles(W.S, k, ldS, W.S, ldS, W.status, 1e-10, 0.0, s);  // factor in place of the Gram matrix
     trsm_rows(Z, rows, k, W.S, ldS, dst, W.status, s);
   };
+  auto body = [&]() {
   if (dir == 'R') {
     if (mode != WST_RESUME) {
       mul(false, theta, nt, m, k, nt, warm, nt, true, W.Ya, k, 1.0, 0.0, nullptr);  // theta B^T
@@ -462,6 +471,27 @@ inline bool wst_split(WstWork& W, RedScratch& red, const double* theta, int m, i
     norm2(left, (ll)m * k, W.nrm + 1, red, s);
   }
   norm2(theta, (ll)m * nt, W.nrm, red, s);
+  };
+  if (graphs_enabled() && !wst_debug()) {
+    const GraphKey key{dir, mode, m, nt, k, (ll)theta, (ll)warm, (ll)left, (ll)right, (ll)red.part, (ll)red.counter,
+                       0, 0, 0, 0, 0};
+    if (GraphEntry* G = W.graphs.find(key)) {
+      graph_replay(*G, s);
+    } else {
+      body();
+      GraphEntry* N = W.graphs.slot(key);
+      try {
+        DMRG2_CUDA(cudaGraphCreate(&N->g, 0));
+        N->launches = capture_to_graph(s, N->g, body);
+        DMRG2_CUDA(cudaGraphInstantiate(&N->ex, N->g, 0));
+      } catch (const std::exception& e) {
+        N->reset();
+        graphs_disable(e.what());
+      }
+    }
+  } else {
+    body();
+  }
   DMRG2_CUDA(cudaMemcpyAsync(W.h_buf + 1, W.nrm, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
   DMRG2_CUDA(cudaMemcpyAsync(W.h_out, W.out, sizeof(SvdOut), cudaMemcpyDeviceToHost, s));
   DMRG2_CUDA(cudaMemcpyAsync(W.h_status, W.status, sizeof(int), cudaMemcpyDeviceToHost, s));

@@ -375,7 +375,7 @@ def run(tag, mpo, mps, sched, **kw):
                 "mps": h.hexdigest(), "launches": launches, "loops": sum(r["device_loops"] for r in rep),
                 "bonds": sum(1 for r in rep) * (L - 1) * 2}
     eng.close()
-run("heis_L24", M.heisenberg_mpo(24), O.random_mps(24, 2, 16, seed=3), [16, 32, 64, 64, 64], krylov_max=30,
+run("heis_L24", M.heisenberg_mpo(24), O.random_mps(24, 2, 16, seed=3), [16, 32, 64, 64, 64, 64, 64], krylov_max=30,
     max_restarts=2, cutoff=1e-12)
 run("jos_L8_c128", M.josephson_mpo(8, n_max=1, E_J=2.0, E_C=1.0, n_g=0.25, phi=0.4, onsite="shifted"),
     O.random_mps(8, 3, 16, seed=6, dtype=np.complex128), [32] * 4, krylov_max=30, max_restarts=2, cutoff=1e-14)
@@ -385,22 +385,24 @@ print("RESULT" + json.dumps(out))
 """
 
 
-def test_device_looped_lanczos_equals_host_driven():
-    """The device-looped Lanczos (one cached CUDA graph per operator shape: a conditional
-    WHILE node over matvec, vector passes and normalisation) does the same arithmetic as
-    the host-driven loop: per-sweep energies and the final MPS are bitwise equal for real
-    and complex two-site sweeps and for single-site sweeps, with the same matvec counts;
-    only the first solve of each operator shape runs host-driven."""
+def test_cached_graphs_equal_host_launches():
+    """The cached CUDA graphs (the device-looped Lanczos: one graph per operator shape with
+    a conditional WHILE node over matvec, vector passes and normalisation; the warm split:
+    one graph per bond, direction and mode) do the same arithmetic as launching the kernels
+    from the host: per-sweep energies and the final MPS are bitwise equal for real and
+    complex two-site sweeps (the real run includes converged sweeps of short and full warm
+    splits) and for single-site sweeps, with the same matvec counts; only the first solve
+    of each operator shape runs host-driven."""
     import os
     import sys
     res = {}
     for mode in ("0", "1"):
-        env = dict(os.environ, DMRG2_LANCZOS_GRAPH=mode,
+        env = dict(os.environ, DMRG2_GRAPHS=mode,
                    PYTHONPATH=os.pathsep.join([str(REPO / "dmrg-implementations_b200"), str(REPO)]))
         r = subprocess.run([sys.executable, "-c", LOOP_CHILD], env=env, capture_output=True, text=True,
                            timeout=600)
         assert r.returncode == 0, r.stderr
-        assert "Lanczos disabled" not in r.stderr, r.stderr
+        assert "graphs disabled" not in r.stderr, r.stderr
         res[mode] = json.loads(r.stdout.split("RESULT")[1])
     for tag in res["0"]:
         host, dev = res["0"][tag], res["1"][tag]
