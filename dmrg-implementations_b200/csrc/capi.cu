@@ -381,7 +381,10 @@ int dmrg2_abi_version(void) { return DMRG2_ABI_VERSION; }
 
 const char* dmrg2_last_error(const dmrg2_handle* h) { return h ? h->err.c_str() : g_err.c_str(); }
 
-int dmrg2_create(const dmrg2_config* cfg, dmrg2_handle** out) {
+}  // extern "C"
+
+namespace {
+int create_handle(const dmrg2_config* cfg, dmrg2_handle** out, bool graphs) {
   if (!cfg || !out) { g_err = "null argument"; return DMRG2_ERR_ARG; }
   *out = nullptr;
   return guarded(nullptr, [&] {
@@ -389,7 +392,8 @@ int dmrg2_create(const dmrg2_config* cfg, dmrg2_handle** out) {
     check_pos({cfg->L, cfg->d, cfg->chi_max});
     if (cfg->L < 2) throw std::invalid_argument("L must be >= 2");
     DMRG2_CUDA(cudaSetDevice(cfg->device));
-    const EngineConfig c = engine_config(cfg);
+    EngineConfig c = engine_config(cfg);
+    c.graphs = graphs;
     std::unique_ptr<dmrg2_handle> h(new dmrg2_handle);
     h->cfg = c;
     h->dtype = cfg->dtype;
@@ -397,6 +401,11 @@ int dmrg2_create(const dmrg2_config* cfg, dmrg2_handle** out) {
     *out = h.release();
   });
 }
+}  // namespace
+
+extern "C" {
+
+int dmrg2_create(const dmrg2_config* cfg, dmrg2_handle** out) { return create_handle(cfg, out, true); }
 
 void dmrg2_destroy(dmrg2_handle* h) { delete h; }
 
@@ -832,7 +841,7 @@ struct dmrg2_server {
   // one solve through the public entry points, on this worker's own handle
   static void solve(ServedRequest* r) {
     dmrg2_handle* h = nullptr;
-    int rc = dmrg2_create(&r->cfg, &h);
+    int rc = create_handle(&r->cfg, &h, false);
     const int L = r->cfg.L;
     if (rc == DMRG2_OK) {
       std::vector<const void*> w(L);

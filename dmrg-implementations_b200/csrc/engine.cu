@@ -753,7 +753,7 @@ class Engine final : public EngineBase {
       r.matvecs += lp.matvecs;
       r.iters += lp.iters;
       r.matvec_s += lp.matvec_s;
-    } else if (graphs_enabled()) {
+    } else if (cfg_.graphs && graphs_enabled()) {
       // the device-looped solve: the bond's operator is staged into the lane's fixed slots,
       // so the cached graph of this shape serves it
       const ll dd = (ll)d_ * d_;
@@ -810,7 +810,7 @@ class Engine final : public EngineBase {
     const int Dl = Db_[i], Dr = Db_[i + 1];
     const ll n = (ll)cL * d_ * cR;
     DMRG2_CUDA(cudaMemcpyAsync(ln().theta, mps_[i], sizeof(T) * (size_t)n, cudaMemcpyDeviceToDevice, ln().st));
-    const bool graph = graphs_enabled();  // staged operator, cached graph per shape
+    const bool graph = cfg_.graphs && graphs_enabled();  // staged operator, cached graph per shape
     const T* sL = graph ? stage_op(ln().opL, lenv_[i], (ll)cL * Dl * cL) : lenv_[i];
     const T* sR = graph ? stage_op(ln().opR, renv_[i + 1], (ll)cR * Dr * cR) : renv_[i + 1];
     const T* sW = graph ? stage_op(ln().opW, wml_[i], (ll)d_ * Dr * Dl * d_) : wml_[i];
@@ -914,7 +914,8 @@ class Engine final : public EngineBase {
         const double* warm = (dir == 'R') ? mps_[i + 1] : mps_[i];
         const int k = dims_[i + 1];
         auto split = [&](WstMode mode) {
-          return wst_split(ln().wst, ln().red, ln().theta, (int)m, (int)nc, dir, k, warm, mps_[i], mps_[i + 1], te, ln().st, mode) &&
+          return wst_split(ln().wst, ln().red, ln().theta, (int)m, (int)nc, dir, k, warm, mps_[i], mps_[i + 1], te, ln().st, mode,
+                           cfg_.graphs) &&
                  warm_split_keeps_rank(k, chi, m, nc, te, ln().wst.h_buf[1]);
         };
         bool ok = false, short_kept = false;

@@ -33,6 +33,10 @@ struct EngineConfig {
                                //    2: randomised split where it applies (full_k > k + 10 and the
                                //    sketched side longer than 2k), exact otherwise
   unsigned seed = 42;
+  // cached CUDA graphs for the Lanczos solves and warm splits (also subject to DMRG2_GRAPHS);
+  // the server turns them off: with a dozen engines capturing concurrently a capture costs
+  // several times its single-engine time and short solves replay too few times to repay it
+  bool graphs = true;
 };
 
 // Parallel (segmented) sweep, the reference's PDMRGGPU::run(n_outer, n_local, n_warmup,

@@ -9,9 +9,12 @@
 
 #include <array>
 #include <atomic>
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <functional>
+#include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include "common.cuh"
@@ -56,39 +59,82 @@ struct GraphEntry {
   }
 };
 
+// DMRG2_GRAPH_STATS=1: each cache prints its builds, replays and build time when cleared
+inline bool graph_stats() {
+  static const bool on = [] {
+    const char* e = std::getenv("DMRG2_GRAPH_STATS");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+
+struct GraphKeyHash {
+  size_t operator()(const GraphKey& k) const {
+    unsigned long long h = 1469598103934665603ull;
+    for (long long v : k) h = (h ^ (unsigned long long)v) * 1099511628211ull;
+    return (size_t)h;
+  }
+};
+
 // At most `cap` graphs; the least recently used goes first.
 struct GraphCache {
   std::vector<GraphEntry> e;
+  std::unordered_map<GraphKey, size_t, GraphKeyHash> index;
+  std::unordered_set<GraphKey, GraphKeyHash> seen;
   unsigned long long uses = 0;
   int cap = 256;
+  const char* name = "graphs";
+  long long builds = 0, replays = 0;
+  double build_s = 0.0;  // host time spent capturing and instantiating
 
   GraphEntry* find(const GraphKey& k) {
-    for (auto& g : e)
-      if (g.ex && g.key == k) {
-        g.last_use = ++uses;
-        return &g;
-      }
-    return nullptr;
-  }
-  // an empty entry carrying key k (evicting the least recently used one when full)
-  GraphEntry* slot(const GraphKey& k) {
-    GraphEntry* g = nullptr;
-    if ((int)e.size() < cap) {
-      e.emplace_back();
-      g = &e.back();
-    } else {
-      g = &e[0];
-      for (auto& x : e)
-        if (x.last_use < g->last_use) g = &x;
-      g->reset();
-    }
-    g->key = k;
+    auto it = index.find(k);
+    if (it == index.end() || !e[it->second].ex) return nullptr;
+    GraphEntry* g = &e[it->second];
     g->last_use = ++uses;
     return g;
   }
+  // A key is captured on its second sighting: a capture costs about as much host time as
+  // a few replays save, so keys that occur once (shapes passed through while the bond
+  // dimensions grow) are not captured.
+  bool seen_before(const GraphKey& k) {
+    if (seen.count(k)) return true;
+    if (seen.size() >= 8192) seen.clear();
+    seen.insert(k);
+    return false;
+  }
+  // an empty entry carrying key k (evicting the least recently used one when full)
+  GraphEntry* slot(const GraphKey& k) {
+    size_t i;
+    auto it = index.find(k);
+    if (it != index.end()) {
+      i = it->second;
+      e[i].reset();
+    } else if ((int)e.size() < cap) {
+      e.emplace_back();
+      i = e.size() - 1;
+    } else {
+      i = 0;
+      for (size_t j = 1; j < e.size(); ++j)
+        if (e[j].last_use < e[i].last_use) i = j;
+      index.erase(e[i].key);
+      e[i].reset();
+    }
+    e[i].key = k;
+    e[i].last_use = ++uses;
+    index[k] = i;
+    return &e[i];
+  }
   void clear() {
+    if (graph_stats() && (builds || replays))
+      std::fprintf(stderr, "[graphs] %s: %lld builds (%.3f s), %lld replays, %zu cached\n", name, builds, build_s,
+                   replays, e.size());
     for (auto& g : e) g.reset();
     e.clear();
+    index.clear();
+    seen.clear();
+    builds = replays = 0;
+    build_s = 0.0;
   }
 };
 

@@ -11,8 +11,8 @@
 //    that advances the index and ends the loop on convergence or after kmax bodies). The
 //    host launches the graph once per restart and reads the result once; no flags cross
 //    to the host between steps and no no-op steps are issued. A call site opts in by
-//    passing a key; the first solve with a new key runs host-driven and then captures the
-//    graph (graphs.cuh holds the cache).
+//    passing a key; solves run host-driven until a key is met the second time, when the
+//    solve is followed by the capture (graphs.cuh holds the cache).
 #pragma once
 
 #include <algorithm>
@@ -36,7 +36,7 @@ using LzKey = std::array<long long, 14>;
 
 // a converged chi=256 sweep of 100 sites meets ~100 distinct (cL, cR) bond shapes (bonds
 // below the cap keep what the cutoff leaves); a graph is a few kilobytes
-constexpr int LZ_GRAPH_CAP = 512;
+constexpr int LZ_GRAPH_CAP = 1024;
 
 template <typename T>
 struct LanczosWork {
@@ -56,6 +56,7 @@ struct LanczosWork {
 
   void init(int kcap_, ll nmax) {
     graphs.cap = LZ_GRAPH_CAP;
+    graphs.name = "lanczos";
     kcap = std::min(kcap_, KRYLOV_CAP);
     krylov = (T*)alloc(sizeof(T) * (size_t)kcap * std::max<ll>(nmax, 1));
     w = (T*)alloc(sizeof(T) * (size_t)std::max<ll>(nmax, 1));
@@ -149,7 +150,7 @@ LanczosResult lanczos_solve(LanczosWork<T>& W, T* theta, ll n, int krylov_max, d
     k[14] = n;
     k[15] = kmax;
     G = W.graphs.find(k);
-    if (!G) {
+    if (!G && W.graphs.seen_before(k)) {
       G = W.graphs.slot(k);
       build = true;
     }
@@ -158,6 +159,7 @@ LanczosResult lanczos_solve(LanczosWork<T>& W, T* theta, ll n, int krylov_max, d
     if (G && G->ex) {
       lz_start(theta, W.krylov, n, W.st, W.red, seed + 104729u * (unsigned)rs, tol, kmax, s, W.cur);
       DMRG2_CUDA(cudaGraphLaunch(G->ex, s));
+      W.graphs.replays += 1;
       lz_ritz(W.krylov, n, theta, W.st, W.red, s);
       DMRG2_CUDA(cudaMemcpyAsync(W.h_st, W.st, sizeof(LanczosDev), cudaMemcpyDeviceToHost, s));
       DMRG2_CUDA(cudaStreamSynchronize(s));
@@ -213,7 +215,10 @@ LanczosResult lanczos_solve(LanczosWork<T>& W, T* theta, ll n, int krylov_max, d
   }
   if (build) {
     try {
+      const auto t0 = std::chrono::steady_clock::now();
       lz_build_graph(W, *G, n, kmax, matvec, s);
+      W.graphs.builds += 1;
+      W.graphs.build_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     } catch (const std::exception& e) {
       G->reset();
       graphs_disable(e.what());

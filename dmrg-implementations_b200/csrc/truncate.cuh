@@ -276,14 +276,16 @@ struct WstWork {
   unsigned* counter = nullptr;
   int* status = nullptr;
   SvdOut* out = nullptr;    // k and the Newton-Schulz convergence flag
+  // with graphs: the warm factor in, and both factors out, pass through these fixed slots
+  // (qmax x kmax each), so one graph serves every bond of a shape
+  double *Win = nullptr, *Lout = nullptr, *Rout = nullptr;
   double* h_buf = nullptr;  // pinned: |theta|^2, |kept|^2
   SvdOut* h_out = nullptr;  // pinned
   int* h_status = nullptr;  // pinned
   int qmax = 0, kmax = 0;
   size_t bytes = 0;
   std::vector<void*> owned;
-  // the launch sequence of a split, by bond (direction, mode, shapes and the factors'
-  // buffers): a converged sweep of L sites replays ~4 L of them
+  // the launch sequence of a split, by direction, mode and shapes
   GraphCache graphs;
 
   void* alloc(size_t b) {
@@ -294,13 +296,17 @@ struct WstWork {
     return p;
   }
   void init(int qmax_, int kmax_) {
-    graphs.cap = 1024;
+    graphs.cap = 2048;  // ~100 bond shapes x 2 directions x 3 modes in a chi=256 sweep of 100 sites
+    graphs.name = "warm split";
     qmax = std::max(qmax_, 1);
     kmax = std::max(std::min(kmax_, CHOL_MAX), 1);
     const size_t qk = (size_t)qmax * kmax;
     Ya = (double*)alloc(sizeof(double) * qk);
     Yb = (double*)alloc(sizeof(double) * qk);
     Yc = (double*)alloc(sizeof(double) * qk);
+    Win = (double*)alloc(sizeof(double) * qk);
+    Lout = (double*)alloc(sizeof(double) * qk);
+    Rout = (double*)alloc(sizeof(double) * qk);
     const size_t np = (size_t)chol_padded(kmax);
     S = (double*)alloc(sizeof(double) * np * np);
     cpart = (double*)alloc(sizeof(double) * (size_t)COLNORM_MAX_CHUNKS * kmax);
@@ -333,7 +339,7 @@ inline size_t wst_bytes(ll qmax, ll kmax) {
   qmax = std::max<ll>(qmax, 1);
   kmax = std::max<ll>(std::min<ll>(kmax, CHOL_MAX), 1);
   const ll np = chol_padded((int)kmax);
-  return sizeof(double) * (size_t)(11 * qmax * kmax + np * np + COLNORM_MAX_CHUNKS * kmax + 4 + 64) +
+  return sizeof(double) * (size_t)(14 * qmax * kmax + np * np + COLNORM_MAX_CHUNKS * kmax + 4 + 64) +
          sizeof(unsigned) * 4 + sizeof(int) * 4 + sizeof(SvdOut);
 }
 
@@ -366,12 +372,14 @@ enum WstMode { WST_FULL = 0, WST_SHORT = 1, WST_RESUME = 2 };
 // Warm-started split of theta (m x nt) at kept rank k; `warm` is B (k x nt) for 'R',
 // A (m x k) for 'L'. Writes left (m x k) and right (k x nt) and returns true, or returns
 // false (left / right undefined) when the warm start was not good enough. The host
-// waits once. Everything between the status reset and that wait is one cached graph per
-// (direction, mode, shapes, buffers) when graphs are on: the first call of a key launches
+// waits once. With graphs on (and a stream other than the legacy default one), the work
+// between the status reset and that wait is one cached graph per (direction, mode,
+// shapes): the warm factor is copied into W.Win and the factors come out of W.Lout and
+// W.Rout, so the graph's buffers do not depend on the bond; a key's second call launches
 // the kernels and then captures them, later calls replay the capture.
 inline bool wst_split(WstWork& W, RedScratch& red, const double* theta, int m, int nt, char dir, int k,
                       const double* warm, double* left, double* right, double& trunc_err, cudaStream_t s,
-                      WstMode mode = WST_FULL) {
+                      WstMode mode = WST_FULL, bool allow_graph = true) {
   if (k > W.kmax || m > W.qmax || nt > W.qmax) throw std::runtime_error("wst_split: workspace too small");
   if (std::max(m, nt) > 32 * COLNORM_MAX_CHUNKS) return false;  // beyond the column-scaling kernel
   DMRG2_CUDA(cudaMemsetAsync(W.status, 0, sizeof(int), s));
@@ -435,6 +443,18 @@ inline bool wst_split(WstWork& W, RedScratch& red, const double* theta, int m, i
     chol_tiles(W.S, k, ldS, W.S, ldS, W.status, 1e-10, 0.0, s);  // factor in place of the Gram matrix
     trsm_rows(Z, rows, k, W.S, ldS, dst, W.status, s);
   };
+  const bool graph = allow_graph && graphs_enabled() && !wst_debug() && s != nullptr;
+  double* const left_out = left;
+  double* const right_out = right;
+  if (graph) {
+    if (mode != WST_RESUME) {
+      DMRG2_CUDA(cudaMemcpyAsync(W.Win, warm, sizeof(double) * (size_t)(dir == 'R' ? (ll)k * nt : (ll)m * k),
+                                 cudaMemcpyDeviceToDevice, s));
+      warm = W.Win;
+    }
+    left = W.Lout;
+    right = W.Rout;
+  }
   auto body = [&]() {
   if (dir == 'R') {
     if (mode != WST_RESUME) {
@@ -472,23 +492,30 @@ inline bool wst_split(WstWork& W, RedScratch& red, const double* theta, int m, i
   }
   norm2(theta, (ll)m * nt, W.nrm, red, s);
   };
-  if (graphs_enabled() && !wst_debug()) {
-    const GraphKey key{dir, mode, m, nt, k, (ll)theta, (ll)warm, (ll)left, (ll)right, (ll)red.part, (ll)red.counter,
-                       0, 0, 0, 0, 0};
+  if (graph) {
+    const GraphKey key{dir, mode, m, nt, k, (ll)theta, (ll)&W, (ll)red.part, (ll)red.counter, 0, 0, 0, 0, 0, 0, 0};
     if (GraphEntry* G = W.graphs.find(key)) {
       graph_replay(*G, s);
+      W.graphs.replays += 1;
+    } else if (!W.graphs.seen_before(key)) {
+      body();
     } else {
       body();
       GraphEntry* N = W.graphs.slot(key);
       try {
+        const auto t0 = std::chrono::steady_clock::now();
         DMRG2_CUDA(cudaGraphCreate(&N->g, 0));
         N->launches = capture_to_graph(s, N->g, body);
         DMRG2_CUDA(cudaGraphInstantiate(&N->ex, N->g, 0));
+        W.graphs.builds += 1;
+        W.graphs.build_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
       } catch (const std::exception& e) {
         N->reset();
         graphs_disable(e.what());
       }
     }
+    DMRG2_CUDA(cudaMemcpyAsync(left_out, W.Lout, sizeof(double) * (size_t)m * k, cudaMemcpyDeviceToDevice, s));
+    DMRG2_CUDA(cudaMemcpyAsync(right_out, W.Rout, sizeof(double) * (size_t)k * nt, cudaMemcpyDeviceToDevice, s));
   } else {
     body();
   }
