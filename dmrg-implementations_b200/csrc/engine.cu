@@ -915,7 +915,7 @@ class Engine final : public EngineBase {
         const int k = dims_[i + 1];
         auto split = [&](WstMode mode) {
           return wst_split(ln().wst, ln().red, ln().theta, (int)m, (int)nc, dir, k, warm, mps_[i], mps_[i + 1], te, ln().st, mode,
-                           cfg_.graphs) &&
+                           cfg_.graphs, ln().ev_d) &&
                  warm_split_keeps_rank(k, chi, m, nc, te, ln().wst.h_buf[1]);
         };
         bool ok = false, short_kept = false;
@@ -936,8 +936,7 @@ class Engine final : public EngineBase {
           ok = split(WST_FULL);
         }
         if (ok) {
-          DMRG2_CUDA(cudaEventRecord(ln().ev_d, ln().st));
-          DMRG2_CUDA(cudaEventSynchronize(ln().ev_d));
+          // ev_d was recorded by the last wst_split call, which waited for the stream
           float ms = 0.f;
           DMRG2_CUDA(cudaEventElapsedTime(&ms, ln().ev_c, ln().ev_d));
           ss.svd_s += ms * 1e-3;

@@ -372,14 +372,14 @@ enum WstMode { WST_FULL = 0, WST_SHORT = 1, WST_RESUME = 2 };
 // Warm-started split of theta (m x nt) at kept rank k; `warm` is B (k x nt) for 'R',
 // A (m x k) for 'L'. Writes left (m x k) and right (k x nt) and returns true, or returns
 // false (left / right undefined) when the warm start was not good enough. The host
-// waits once. With graphs on (and a stream other than the legacy default one), the work
+// waits once; ev_end, when given, is recorded after the split's kernels. With graphs on (and a stream other than the legacy default one), the work
 // between the status reset and that wait is one cached graph per (direction, mode,
 // shapes): the warm factor is copied into W.Win and the factors come out of W.Lout and
 // W.Rout, so the graph's buffers do not depend on the bond; a key's second call launches
 // the kernels and then captures them, later calls replay the capture.
 inline bool wst_split(WstWork& W, RedScratch& red, const double* theta, int m, int nt, char dir, int k,
                       const double* warm, double* left, double* right, double& trunc_err, cudaStream_t s,
-                      WstMode mode = WST_FULL, bool allow_graph = true) {
+                      WstMode mode = WST_FULL, bool allow_graph = true, cudaEvent_t ev_end = nullptr) {
   if (k > W.kmax || m > W.qmax || nt > W.qmax) throw std::runtime_error("wst_split: workspace too small");
   if (std::max(m, nt) > 32 * COLNORM_MAX_CHUNKS) return false;  // beyond the column-scaling kernel
   DMRG2_CUDA(cudaMemsetAsync(W.status, 0, sizeof(int), s));
@@ -519,6 +519,7 @@ inline bool wst_split(WstWork& W, RedScratch& red, const double* theta, int m, i
   } else {
     body();
   }
+  if (ev_end) DMRG2_CUDA(cudaEventRecord(ev_end, s));  // the split's device work ends here
   DMRG2_CUDA(cudaMemcpyAsync(W.h_buf + 1, W.nrm, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
   DMRG2_CUDA(cudaMemcpyAsync(W.h_out, W.out, sizeof(SvdOut), cudaMemcpyDeviceToHost, s));
   DMRG2_CUDA(cudaMemcpyAsync(W.h_status, W.status, sizeof(int), cudaMemcpyDeviceToHost, s));
