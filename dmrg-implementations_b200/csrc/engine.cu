@@ -762,7 +762,7 @@ class Engine final : public EngineBase {
       auto mvs = [&](const T* in, T* out, const int* skip) {
         heff_apply(sL, sR, sW, in, out, ln().X, ln().Y, cL, cR, d_, Dl, Dr, skip, ln().st);
       };
-      const LzKey key{2, cL, cR, Dl, Dr, d_, (ll)sL, (ll)sR, (ll)sW, (ll)ln().X, (ll)ln().Y, 0};
+      const LzKey key{2, cL, cR, Dl, Dr, d_, (ll)sL, (ll)sR, (ll)sW, (ll)ln().X, (ll)ln().Y};
       r = lanczos_solve<T>(ln().lw, ln().theta, n, cfg_.krylov_max, cfg_.lanczos_tol, cfg_.max_restarts,
                            cfg_.seed + 7919u * (unsigned)i, mvs, ln().st, &key);
     } else {
@@ -817,7 +817,7 @@ class Engine final : public EngineBase {
     auto mv = [&](const T* in, T* out, const int* skip) {
       heff1_apply(sL, sR, sW, in, out, ln().X, ln().Y, cL, cR, d_, Dl, Dr, skip, ln().st);
     };
-    const LzKey key{1, cL, cR, Dl, Dr, d_, (ll)sL, (ll)sR, (ll)sW, (ll)ln().X, (ll)ln().Y, 0};
+    const LzKey key{1, cL, cR, Dl, Dr, d_, (ll)sL, (ll)sR, (ll)sW, (ll)ln().X, (ll)ln().Y};
     LanczosResult r = lanczos_solve<T>(ln().lw, ln().theta, n, cfg_.krylov_max, cfg_.lanczos_tol, cfg_.max_restarts,
                                        cfg_.seed + 7919u * (unsigned)i, mv, ln().st, graph ? &key : nullptr);
     ss.heff_s += r.matvec_s;

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <functional>
+#include <stdexcept>
 #include <unordered_map>
 #include <unordered_set>
 #include <vector>
@@ -49,6 +50,7 @@ struct GraphEntry {
   cudaGraph_t g = nullptr;
   cudaGraphExec_t ex = nullptr;
   long long launches = 0;  // kernels one replay runs (per loop body for a looped graph)
+  long long fixed = 0;     // a looped graph's kernels outside the loop
   unsigned long long last_use = 0;
   void reset() {
     if (ex) cudaGraphExecDestroy(ex);
@@ -56,6 +58,7 @@ struct GraphEntry {
     ex = nullptr;
     g = nullptr;
     launches = 0;
+    fixed = 0;
   }
 };
 
@@ -86,6 +89,7 @@ struct GraphCache {
   const char* name = "graphs";
   long long builds = 0, replays = 0;
   double build_s = 0.0;  // host time spent capturing and instantiating
+  double inst_s = 0.0;   // of which in cudaGraphInstantiate
 
   GraphEntry* find(const GraphKey& k) {
     auto it = index.find(k);
@@ -127,21 +131,23 @@ struct GraphCache {
   }
   void clear() {
     if (graph_stats() && (builds || replays))
-      std::fprintf(stderr, "[graphs] %s: %lld builds (%.3f s), %lld replays, %zu cached\n", name, builds, build_s,
-                   replays, e.size());
+      std::fprintf(stderr, "[graphs] %s: %lld builds (%.3f s, %.3f s instantiating), %lld replays, %zu cached\n",
+                   name, builds, build_s, inst_s, replays, e.size());
     for (auto& g : e) g.reset();
     e.clear();
     index.clear();
     seen.clear();
     builds = replays = 0;
-    build_s = 0.0;
+    build_s = inst_s = 0.0;
   }
 };
 
 // Records what fn() enqueues on s into graph g (nothing runs; s may still hold queued
 // work) and returns the number of kernels recorded. The launch counters drop them
 // again: each replay adds what it runs.
-inline long long capture_to_graph(cudaStream_t s, cudaGraph_t g, const std::function<void()>& fn) {
+// With dep, the recorded work follows that node of g.
+inline long long capture_to_graph(cudaStream_t s, cudaGraph_t g, const std::function<void()>& fn,
+                                  const cudaGraphNode_t* dep = nullptr) {
   const long long t0 = thread_launches();
   auto undo = [&]() {
     const long long nb = thread_launches() - t0;
@@ -149,7 +155,7 @@ inline long long capture_to_graph(cudaStream_t s, cudaGraph_t g, const std::func
     launch_counter() -= nb;
     return nb;
   };
-  DMRG2_CUDA(cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  DMRG2_CUDA(cudaStreamBeginCaptureToGraph(s, g, dep, nullptr, dep ? 1 : 0, cudaStreamCaptureModeThreadLocal));
   try {
     fn();
   } catch (...) {
@@ -163,6 +169,33 @@ inline long long capture_to_graph(cudaStream_t s, cudaGraph_t g, const std::func
   const long long nb = undo();
   DMRG2_CUDA(err);
   return nb;
+}
+
+// the one node of g that no other node depends on (g was recorded from one stream)
+inline cudaGraphNode_t graph_leaf(cudaGraph_t g) {
+  size_t n = 0;
+  DMRG2_CUDA(cudaGraphGetNodes(g, nullptr, &n));
+  std::vector<cudaGraphNode_t> nodes(n);
+  DMRG2_CUDA(cudaGraphGetNodes(g, nodes.data(), &n));
+  cudaGraphNode_t leaf = nullptr;
+  int leaves = 0;
+  for (auto v : nodes) {
+    size_t nd = 0;
+    DMRG2_CUDA(cudaGraphNodeGetDependentNodes(v, nullptr, &nd));
+    if (nd == 0) {
+      leaf = v;
+      ++leaves;
+    }
+  }
+  if (leaves != 1) throw std::runtime_error("graph_leaf: the recorded work does not end in one node");
+  return leaf;
+}
+
+// cudaGraphInstantiate, timed into the cache's statistics
+inline void graph_instantiate(GraphCache& c, GraphEntry& G) {
+  const auto t0 = std::chrono::steady_clock::now();
+  DMRG2_CUDA(cudaGraphInstantiate(&G.ex, G.g, 0));
+  c.inst_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
 // a replay of G on s: counts its kernels as launched

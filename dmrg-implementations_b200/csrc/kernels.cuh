@@ -24,7 +24,7 @@ struct LanczosDev {
   int kmax;
   int j;                               // Krylov index of the device-looped solve's current step
   int guard;                           // loop bodies run so far (bounds the device loop)
-  int pad;
+  unsigned seed_in;                    // the device-looped solve's seed (copied in per solve)
   unsigned long long t_mark;           // %globaltimer when the current matvec was issued
   unsigned long long mv_ns;            // matvec time accumulated by the device-looped solve
 };
@@ -51,7 +51,7 @@ void lz_normalize_next(T* vnext, const T* w, ll n, LanczosDev* st, cudaStream_t 
 // start: nrm(theta) -> (random fill if ~0) -> v0 = theta/|theta| (also into cur when given)
 template <typename T>
 void lz_start(T* theta, T* v0, ll n, LanczosDev* st, RedScratch& r, unsigned seed, double tol,
-              int kmax, cudaStream_t s, T* cur = nullptr);
+              int kmax, cudaStream_t s, T* cur = nullptr, const unsigned* seed_dev = nullptr);
 // The same step with the Krylov index read on the device (st->j), for a loop that runs
 // without the host: the three passes over w = H v_j, then v_(j+1) into V and into cur
 // (the matvec's fixed input).

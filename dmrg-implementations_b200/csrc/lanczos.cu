@@ -399,7 +399,9 @@ __device__ inline double hash_uniform(unsigned long long x) {
 
 // reset solver state; if |theta| is ~0, replace theta by a seeded random vector
 template <typename T>
-__global__ void lz_reset_kernel(T* theta, ll n, LanczosDev* st, unsigned seed, double tol, int kmax) {
+__global__ void lz_reset_kernel(T* theta, ll n, LanczosDev* st, unsigned seed, double tol, int kmax,
+                                const unsigned* seed_dev) {
+  if (seed_dev) seed = *seed_dev;
   const bool tiny = !(st->nrm2 >= 1e-28);
   if (tiny) {
     for (ll x = (ll)blockIdx.x * blockDim.x + threadIdx.x; x < n; x += (ll)gridDim.x * blockDim.x) {
@@ -500,9 +502,9 @@ void norm2(const T* x, ll n, double* out_dev, RedScratch& r, cudaStream_t s) {
 
 template <typename T>
 void lz_start(T* theta, T* v0, ll n, LanczosDev* st, RedScratch& r, unsigned seed, double tol,
-              int kmax, cudaStream_t s, T* cur) {
+              int kmax, cudaStream_t s, T* cur, const unsigned* seed_dev) {
   norm2<T>(theta, n, &st->nrm2, r, s);
-  lz_reset_kernel<T><<<grid_for(n), VEC_THREADS, 0, s>>>(theta, n, st, seed, tol, kmax);
+  lz_reset_kernel<T><<<grid_for(n), VEC_THREADS, 0, s>>>(theta, n, st, seed, tol, kmax, seed_dev);
   DMRG2_CHECK_LAUNCH();
   norm2<T>(theta, n, &st->nrm2, r, s);
   lz_v0_kernel<T><<<grid_for(n), VEC_THREADS, 0, s>>>(theta, v0, n, st, cur);
@@ -548,7 +550,7 @@ void scale_inplace(T* x, ll n, const double* nrm2_dev, cudaStream_t s) {
                                         cudaStream_t);                                            \
   template void lz_normalize_next<T>(T*, const T*, ll, LanczosDev*, cudaStream_t);                \
   template void lz_start<T>(T*, T*, ll, LanczosDev*, RedScratch&, unsigned, double, int,      \
-                            cudaStream_t, T*);                                                    \
+                            cudaStream_t, T*, const unsigned*);                                   \
   template void lz_step_dev<T>(const T*, ll, T*, T*, LanczosDev*, RedScratch&, int, cudaStream_t); \
   template void lz_ritz<T>(const T*, ll, T*, LanczosDev*, RedScratch&, cudaStream_t);             \
   template void norm2<T>(const T*, ll, double*, RedScratch&, cudaStream_t);                       \

@@ -20,6 +20,7 @@
 #include <atomic>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <functional>
 #include <stdexcept>
 #include <vector>
@@ -31,8 +32,8 @@
 namespace dmrg2 {
 
 // identifies a matvec for the graph cache: operator shapes and device pointers, chosen by
-// the caller (unused entries 0); the solve adds n and kmax
-using LzKey = std::array<long long, 14>;
+// the caller (unused entries 0); the solve adds n, kmax, the tolerance and its buffers
+using LzKey = std::array<long long, 11>;
 
 // a converged chi=256 sweep of 100 sites meets ~100 distinct (cL, cR) bond shapes (bonds
 // below the cap keep what the cutoff leaves); a graph is a few kilobytes
@@ -51,6 +52,7 @@ struct LanczosWork {
   RedScratch red;
   int* h_flags = nullptr;
   LanczosDev* h_st = nullptr;
+  unsigned* h_seed = nullptr;  // the device-looped solve's seed, copied to st->seed_in
   std::vector<cudaEvent_t> ev_poll, ev_mv;
   std::vector<void*> owned;
 
@@ -69,6 +71,7 @@ struct LanczosWork {
     DMRG2_CUDA(cudaMemset(st, 0, sizeof(LanczosDev)));
     h_flags = (int*)host_pinned(sizeof(int) * POLL_RING);
     h_st = (LanczosDev*)host_pinned(sizeof(LanczosDev));
+    h_seed = (unsigned*)host_pinned(sizeof(unsigned));
     ev_poll.resize(POLL_RING);
     for (auto& e : ev_poll) DMRG2_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     ev_mv.resize(2 * KRYLOV_CAP);
@@ -90,8 +93,10 @@ struct LanczosWork {
     owned.clear();
     if (h_flags) host_unpin(h_flags);
     if (h_st) host_unpin(h_st);
+    if (h_seed) host_unpin(h_seed);
     h_flags = nullptr;
     h_st = nullptr;
+    h_seed = nullptr;
     for (auto e : ev_poll) cudaEventDestroy(e);
     for (auto e : ev_mv) cudaEventDestroy(e);
     ev_poll.clear();
@@ -108,11 +113,17 @@ struct LanczosResult {
   int device_loops = 0;   // restarts run as the device-looped graph
 };
 
-// Captures the device loop of W's buffers and this matvec into G (nothing runs).
+// Captures one solve of W's buffers and this matvec into G (nothing runs): the start
+// (norms, reset with the seed read from st->seed_in, first vector), the WHILE node over
+// the Krylov steps, the Ritz vector and the copy of the solver state to W.h_st.
 template <typename T>
-void lz_build_graph(LanczosWork<T>& W, GraphEntry& G, ll n, int kmax,
+void lz_build_graph(LanczosWork<T>& W, GraphEntry& G, T* theta, ll n, int kmax, double tol,
                     const std::function<void(const T*, T*, const int*)>& matvec, cudaStream_t s) {
   DMRG2_CUDA(cudaGraphCreate(&G.g, 0));
+  G.fixed = capture_to_graph(s, G.g, [&]() {
+    lz_start(theta, W.krylov, n, W.st, W.red, 0u, tol, kmax, s, W.cur, &W.st->seed_in);
+  });
+  const cudaGraphNode_t start = graph_leaf(G.g);
   cudaGraphConditionalHandle h;
   DMRG2_CUDA(cudaGraphConditionalHandleCreate(&h, G.g, 1, cudaGraphCondAssignDefault));
   cudaGraphNodeParams p{};
@@ -120,14 +131,21 @@ void lz_build_graph(LanczosWork<T>& W, GraphEntry& G, ll n, int kmax,
   p.conditional.handle = h;
   p.conditional.type = cudaGraphCondTypeWhile;
   p.conditional.size = 1;
-  cudaGraphNode_t node;
-  DMRG2_CUDA(cudaGraphAddNode(&node, G.g, nullptr, 0, &p));
+  cudaGraphNode_t loop;
+  DMRG2_CUDA(cudaGraphAddNode(&loop, G.g, &start, 1, &p));
   G.launches = capture_to_graph(s, p.conditional.phGraph_out[0], [&]() {
     matvec(W.cur, W.w, &W.st->done);
     lz_step_dev(W.krylov, n, W.w, W.cur, W.st, W.red, kmax, s);
     lz_loop_next(W.st, h, kmax, s);
   });
-  DMRG2_CUDA(cudaGraphInstantiate(&G.ex, G.g, 0));
+  G.fixed += capture_to_graph(
+      s, G.g,
+      [&]() {
+        lz_ritz(W.krylov, n, theta, W.st, W.red, s);
+        DMRG2_CUDA(cudaMemcpyAsync(W.h_st, W.st, sizeof(LanczosDev), cudaMemcpyDeviceToHost, s));
+      },
+      &loop);
+  graph_instantiate(W.graphs, G);
 }
 
 // matvec(in, out, skip_flag) enqueues out = H in on stream s, doing nothing when
@@ -147,8 +165,14 @@ LanczosResult lanczos_solve(LanczosWork<T>& W, T* theta, ll n, int krylov_max, d
   if (key && graphs_enabled()) {
     GraphKey k{};
     std::copy(key->begin(), key->end(), k.begin());
-    k[14] = n;
-    k[15] = kmax;
+    double tol_key = tol;
+    long long tol_bits = 0;
+    std::memcpy(&tol_bits, &tol_key, sizeof(tol_bits));
+    k[11] = n;
+    k[12] = kmax;
+    k[13] = tol_bits;
+    k[14] = (ll)theta;
+    k[15] = (ll)&W;
     G = W.graphs.find(k);
     if (!G && W.graphs.seen_before(k)) {
       G = W.graphs.slot(k);
@@ -157,16 +181,16 @@ LanczosResult lanczos_solve(LanczosWork<T>& W, T* theta, ll n, int krylov_max, d
   }
   for (int rs = 0; rs <= max_restarts; ++rs) {
     if (G && G->ex) {
-      lz_start(theta, W.krylov, n, W.st, W.red, seed + 104729u * (unsigned)rs, tol, kmax, s, W.cur);
+      // the pinned seed is read by this copy before the host writes it again (the wait below)
+      *W.h_seed = seed + 104729u * (unsigned)rs;
+      DMRG2_CUDA(cudaMemcpyAsync(&W.st->seed_in, W.h_seed, sizeof(unsigned), cudaMemcpyHostToDevice, s));
       DMRG2_CUDA(cudaGraphLaunch(G->ex, s));
       W.graphs.replays += 1;
-      lz_ritz(W.krylov, n, theta, W.st, W.red, s);
-      DMRG2_CUDA(cudaMemcpyAsync(W.h_st, W.st, sizeof(LanczosDev), cudaMemcpyDeviceToHost, s));
       DMRG2_CUDA(cudaStreamSynchronize(s));
       if (!W.h_st->done || W.h_st->n_iter < 1) throw std::runtime_error("Lanczos did not terminate");
       const int bodies = W.h_st->guard;
-      launch_counter() += bodies * G->launches;
-      thread_launches() += bodies * G->launches;
+      launch_counter() += bodies * G->launches + G->fixed;
+      thread_launches() += bodies * G->launches + G->fixed;
       res.matvecs += bodies;
       res.iters += W.h_st->n_iter;
       res.energy = W.h_st->e_cur;
@@ -216,7 +240,7 @@ LanczosResult lanczos_solve(LanczosWork<T>& W, T* theta, ll n, int krylov_max, d
   if (build) {
     try {
       const auto t0 = std::chrono::steady_clock::now();
-      lz_build_graph(W, *G, n, kmax, matvec, s);
+      lz_build_graph(W, *G, theta, n, kmax, tol, matvec, s);
       W.graphs.builds += 1;
       W.graphs.build_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     } catch (const std::exception& e) {

@@ -506,7 +506,7 @@ inline bool wst_split(WstWork& W, RedScratch& red, const double* theta, int m, i
         const auto t0 = std::chrono::steady_clock::now();
         DMRG2_CUDA(cudaGraphCreate(&N->g, 0));
         N->launches = capture_to_graph(s, N->g, body);
-        DMRG2_CUDA(cudaGraphInstantiate(&N->ex, N->g, 0));
+        graph_instantiate(W.graphs, *N);
         W.graphs.builds += 1;
         W.graphs.build_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
       } catch (const std::exception& e) {
