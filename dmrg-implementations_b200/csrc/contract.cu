@@ -1,5 +1,9 @@
 #include "contract.cuh"
 
+#include <algorithm>
+#include <cstring>
+#include <stdexcept>
+
 namespace dmrg2 {
 
 // Y[a][o][e] = sum_k W[o][k] X[a][k][e] for Kin, Kout <= KM (the two-site MPO
@@ -33,12 +37,88 @@ __global__ void __launch_bounds__(128)
   }
 }
 
+// The same mixing with W in its nonzero form (row starts, ascending columns, values; Kin,
+// Kout <= 32 and at most MIX_SPARSE_NNZ nonzeros): each output sums only its row's
+// nonzeros, in the order of the dense loop above (whose other terms are exact zeros). A
+// thread first loads its Kin inputs together (a static loop, as the dense kernel does)
+// into its own column of shared memory, so the sums read shared memory, not L2.
+constexpr int MIX_SPARSE_NNZ = 512;
+constexpr int MIX_SPARSE_NT = 64;
+template <typename T>
+__global__ void __launch_bounds__(MIX_SPARSE_NT)
+    mpo_mix_sparse_kernel(const T* __restrict__ X, const T* __restrict__ val, const int* __restrict__ rowp,
+                          T* __restrict__ Y, int Kin, int Kout, int cR, ll sX, ll sY, const int* skip) {
+  if (skip && *((volatile const int*)skip)) return;
+  constexpr int KM = 32, NT = MIX_SPARSE_NT;
+  __shared__ int rp[KM + 1];
+  __shared__ int cs[MIX_SPARSE_NNZ];
+  __shared__ T vs[MIX_SPARSE_NNZ];
+  __shared__ T xs[KM * NT];  // xs[k][thread]
+  const int tid = threadIdx.x;
+  for (int i = tid; i <= Kout; i += NT) rp[i] = rowp[i];
+  __syncthreads();
+  const int nnz = min(rp[Kout], MIX_SPARSE_NNZ);
+  const int* col = rowp + Kout + 1;
+  for (int i = tid; i < nnz; i += NT) {
+    cs[i] = col[i];
+    vs[i] = val[i];
+  }
+  __syncthreads();
+  const int e = blockIdx.x * NT + tid;
+  if (e >= cR) return;
+  const ll a = blockIdx.y;
+  const T* xa = X + a * sX + e;
+  T* ya = Y + a * sY + e;
+#pragma unroll
+  for (int k = 0; k < KM; ++k)
+    if (k < Kin) xs[k * NT + tid] = xa[(ll)k * cR];
+  for (int o = 0; o < Kout; ++o) {
+    T acc = ST<T>::zero();
+    const int j1 = min(rp[o + 1], nnz);
+    for (int j = rp[o]; j < j1; ++j) acc = acc + ST<T>::mul(vs[j], xs[cs[j] * NT + tid]);
+    ya[(ll)o * cR] = acc;
+  }
+}
+
+template <typename T>
+int wwt_sparse_block(std::vector<T>& w, int Kin, int Kout) {
+  const ll kk = (ll)Kin * Kout;
+  if ((ll)w.size() != kk) throw std::invalid_argument("wwt_sparse_block: dense matrix of the wrong size");
+  std::vector<T> val((size_t)kk, ST<T>::zero());
+  std::vector<int> ints((size_t)(Kout + 1 + kk), 0);
+  int nnz = 0;
+  for (int o = 0; o < Kout; ++o) {
+    ints[(size_t)o] = nnz;
+    for (int k = 0; k < Kin; ++k) {
+      const T v = w[(size_t)o * Kin + k];
+      if (ST<T>::abs2(v) != 0.0) {
+        val[(size_t)nnz] = v;
+        ints[(size_t)(Kout + 1 + nnz)] = k;
+        ++nnz;
+      }
+    }
+  }
+  ints[(size_t)Kout] = nnz;
+  const ll total = wwt_block_elems(Kin, Kout, sizeof(T));
+  w.resize((size_t)total, ST<T>::zero());
+  std::copy(val.begin(), val.end(), w.begin() + kk);
+  std::memcpy(w.data() + 2 * kk, ints.data(), sizeof(int) * ints.size());
+  return nnz;
+}
+
 // step 2 of the matvec: Y[a] = W X[a] for every a (MPO mixing, FP64); X[a] is Kin x cR,
-// Y[a] is Kout x cR
+// Y[a] is Kout x cR; wsp: W's nonzero form (wwt_sparse_block), or null
 template <typename T>
 static void mix_rows(const T* X, const T* W, T* Y, int cL, int cR, int Kin, int Kout, const int* skip,
-                     cudaStream_t s) {
-  if (Kin <= 32 && Kout <= 32 && cL <= 65535) {
+                     cudaStream_t s, const T* wsp = nullptr) {
+  if (wsp && Kin <= 32 && Kout <= 32 && 2 * Kin * Kout <= 2 * MIX_SPARSE_NNZ && cL <= 65535) {
+    // (the engine uses the nonzero form only where nnz <= Kin Kout / 2 <= MIX_SPARSE_NNZ)
+    const ll kk = (ll)Kin * Kout;
+    dim3 grid(ceil_div(cR, MIX_SPARSE_NT), cL);
+    mpo_mix_sparse_kernel<T><<<grid, MIX_SPARSE_NT, 0, s>>>(X, wsp, (const int*)(wsp + kk), Y, Kin, Kout, cR,
+                                                            (ll)Kin * cR, (ll)Kout * cR, skip);
+    DMRG2_CHECK_LAUNCH();
+  } else if (Kin <= 32 && Kout <= 32 && cL <= 65535) {
     dim3 grid(ceil_div(cR, 128), cL);
     mpo_mix_kernel<T, 32><<<grid, 128, 0, s>>>(X, W, Y, Kin, Kout, cR, (ll)Kin * cR, (ll)Kout * cR, skip);
     DMRG2_CHECK_LAUNCH();
@@ -69,7 +149,7 @@ void heff_apply_split(const T* Lenv, const T* Renv, const T* WWt, const T* in, T
 
 template <typename T>
 void heff_apply(const T* Lenv, const T* Renv, const T* WWt, const T* in, T* out, T* X, T* Y, int cL,
-                int cR, int d, int Dl, int Dr, const int* skip, cudaStream_t s) {
+                int cR, int d, int Dl, int Dr, const int* skip, cudaStream_t s, const T* wsp) {
   const ll dd = (ll)d * d;
   {
     Gemm<T> g;
@@ -80,7 +160,7 @@ void heff_apply(const T* Lenv, const T* Renv, const T* WWt, const T* in, T* out,
     g.nb1 = Dl; g.skip = skip;
     launch_gemm(g, s);
   }
-  mix_rows(X, WWt, Y, cL, cR, (int)(Dl * dd), (int)(dd * Dr), skip, s);
+  mix_rows(X, WWt, Y, cL, cR, (int)(Dl * dd), (int)(dd * Dr), skip, s, wsp);
   {
     Gemm<T> g;
     g.tb = true;
@@ -299,7 +379,8 @@ void build_wmix_right(const T* W, int Dl, int Dr, int d, std::vector<T>& out) {
 
 #define INST(T)                                                                                 \
   template void heff_apply<T>(const T*, const T*, const T*, const T*, T*, T*, T*, int, int, int, \
-                              int, int, const int*, cudaStream_t);                               \
+                              int, int, const int*, cudaStream_t, const T*);                     \
+  template int wwt_sparse_block<T>(std::vector<T>&, int, int);                                  \
   template void heff1_apply<T>(const T*, const T*, const T*, const T*, T*, T*, T*, int, int, int,  \
                                int, int, const int*, cudaStream_t);                              \
   template void heff_apply_split<T>(const T*, const T*, const T*, const T*, T*, T*, T*, int, int,   \

@@ -21,9 +21,24 @@ namespace dmrg2 {
 //   step 1: X[a][w][s][r][e] = sum_c L[a][w][c] theta[c][s][r][e]      (Dl batches)
 //   step 2: Y[a][p][q][n][e] = sum_{w,s,r} WWt[(p,q,n)][(w,s,r)] X[a][w][s][r][e]  (cL batches)
 //   step 3: out[a][p][q][f]  = sum_{n,e} Y[a][p][q][n][e] R[f][n][e]  (one GEMM, K = Dr*cR)
+//
+// wsp, when given, is the nonzero form of WWt (wwt_sparse_block below): step 2 then sums
+// only the nonzero entries, in the same column order, so the result is the same.
 template <typename T>
 void heff_apply(const T* Lenv, const T* Renv, const T* WWt, const T* in, T* out, T* X, T* Y, int cL,
-                int cR, int d, int Dl, int Dr, const int* skip, cudaStream_t s);
+                int cR, int d, int Dl, int Dr, const int* skip, cudaStream_t s, const T* wsp = nullptr);
+
+// The fused two-site MPO of a bond as the engine stores it, one block: the dense Kout x Kin
+// matrix WWt, then its nonzeros row by row (Kout x Kin slots for values), then, as ints, the
+// Kout + 1 row starts and the Kout x Kin slots for column indices (ascending in each row).
+// The fused Heisenberg MPO (D = 5, d = 2) has 30 nonzeros of 400.
+inline ll wwt_block_elems(int Kin, int Kout, size_t elem_bytes) {
+  const ll kk = (ll)Kin * Kout;
+  return 2 * kk + (((ll)Kout + 1 + kk) * (ll)sizeof(int) + (ll)elem_bytes - 1) / (ll)elem_bytes;
+}
+// appends the nonzero form to a dense WWt (Kout x Kin) in place; returns the nonzero count
+template <typename T>
+int wwt_sparse_block(std::vector<T>& w, int Kin, int Kout);
 
 // The same matvec in the precision form: steps 1 and 3 as split-BF16 GEMMs on the
 // tcgen05 tensor cores (FP32 accumulation), step 2 in FP64.

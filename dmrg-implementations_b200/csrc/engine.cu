@@ -154,6 +154,18 @@ class Engine final : public EngineBase {
       build_wmix_right(hW_[i].data(), Dl[i], Dr[i], d_, hmr[i]);
     }
     for (int i = 0; i + 1 < L_; ++i) build_wwt(hW_[i].data(), hW_[i + 1].data(), Dl[i], Dr[i], Dr[i + 1], d_, hww[i]);
+    // each bond's fused MPO also in its nonzero form; the mixing step uses it where at
+    // most half the entries are nonzero (DMRG2_MIX_DENSE=1: always the dense form)
+    static const bool mix_dense = [] {
+      const char* e = std::getenv("DMRG2_MIX_DENSE");
+      return e && e[0] == '1';
+    }();
+    wwt_sparse_.assign(L_ - 1, 0);
+    for (int i = 0; i + 1 < L_; ++i) {
+      const int Kin = Dl[i] * d_ * d_, Kout = d_ * d_ * Dr[i + 1];
+      const int nnz = wwt_sparse_block(hww[i], Kin, Kout);
+      wwt_sparse_[i] = (!mix_dense && 2 * (ll)nnz <= (ll)Kin * Kout && Kin <= 32 && Kout <= 32) ? 1 : 0;
+    }
     // contraction scratch
     ll xs = 1;
     const ll dd = (ll)d_ * d_;
@@ -735,8 +747,11 @@ class Engine final : public EngineBase {
     const int cL = dims_[i], cR = dims_[i + 2];
     const int Dl = Db_[i], Dr = Db_[i + 2];
     const double fl = heff_flops(cL, cR, d_, Dl, Dr, ST<T>::cplx);
+    const ll kk = (ll)Dl * d_ * d_ * d_ * d_ * Dr;  // entries of the dense fused MPO
+    const bool sparse = wwt_sparse_[i] != 0;
     auto mv = [&](const T* in, T* out, const int* skip) {
-      heff_apply(lenv_[i], renv_[i + 2], wwt_[i], in, out, ln().X, ln().Y, cL, cR, d_, Dl, Dr, skip, ln().st);
+      heff_apply(lenv_[i], renv_[i + 2], wwt_[i], in, out, ln().X, ln().Y, cL, cR, d_, Dl, Dr, skip, ln().st,
+                 sparse ? wwt_[i] + kk : nullptr);
     };
     LanczosResult r;
     if (cfg_.precision == 1) {
@@ -758,11 +773,11 @@ class Engine final : public EngineBase {
       // so the cached graph of this shape serves it
       const ll dd = (ll)d_ * d_;
       const T *sL = stage_op(ln().opL, lenv_[i], (ll)cL * Dl * cL), *sR = stage_op(ln().opR, renv_[i + 2], (ll)cR * Dr * cR),
-              *sW = stage_op(ln().opW, wwt_[i], Dl * dd * dd * Dr);
+              *sW = stage_op(ln().opW, wwt_[i], wwt_block_elems(Dl * (int)dd, (int)dd * Dr, sizeof(T)));
       auto mvs = [&](const T* in, T* out, const int* skip) {
-        heff_apply(sL, sR, sW, in, out, ln().X, ln().Y, cL, cR, d_, Dl, Dr, skip, ln().st);
+        heff_apply(sL, sR, sW, in, out, ln().X, ln().Y, cL, cR, d_, Dl, Dr, skip, ln().st, sparse ? sW + kk : nullptr);
       };
-      const LzKey key{2, cL, cR, Dl, Dr, d_, (ll)sL, (ll)sR, (ll)sW, (ll)ln().X, (ll)ln().Y};
+      const LzKey key{sparse ? 3 : 2, cL, cR, Dl, Dr, d_, (ll)sL, (ll)sR, (ll)sW, (ll)ln().X, (ll)ln().Y};
       r = lanczos_solve<T>(ln().lw, ln().theta, n, cfg_.krylov_max, cfg_.lanczos_tol, cfg_.max_restarts,
                            cfg_.seed + 7919u * (unsigned)i, mvs, ln().st, &key);
     } else {
@@ -1135,6 +1150,7 @@ class Engine final : public EngineBase {
   std::vector<int> cap_, dims_, Dl_, Dr_, Db_;
   std::vector<std::vector<T>> hW_;
   std::vector<T*> mps_, lenv_, renv_, wwt_, wml_, wmr_;
+  std::vector<int> wwt_sparse_;  // bond uses the nonzero form of its fused MPO
   std::atomic<unsigned long long> rsvd_calls_{0};
   int prev_sweep_chi_ = 0;      // bond cap of the last completed sweep (0: none since the last set-up)
   std::vector<double> te_ref_;  // per bond: weight discarded by its last full split (< 0: none yet)
@@ -1190,7 +1206,7 @@ size_t engine_footprint(const EngineConfig& c, const std::vector<int>& Dl, const
        sizeof(int) * (size_t)(L + 1);
   // set_mpo
   for (int i = 0; i < L; ++i) b += 2 * el((ll)d * Dr[i] * Dl[i] * d);
-  for (int i = 0; i + 1 < L; ++i) b += el((ll)d * d * Dr[i + 1] * Dl[i] * d * d);
+  for (int i = 0; i + 1 < L; ++i) b += el(wwt_block_elems(Dl[i] * d * d, d * d * Dr[i + 1], sb));
   std::vector<ll> Db(L + 1, 1);
   for (int i = 0; i < L; ++i) Db[i] = Dl[i];
   Db[L] = Dr[L - 1];
@@ -1200,7 +1216,7 @@ size_t engine_footprint(const EngineConfig& c, const std::vector<int>& Dl, const
     opn = std::max(opn, cap[i] * cap[i] * Db[i]);
   }
   for (int i = 0; i < L; ++i) opw = std::max(opw, (ll)d * Dr[i] * Dl[i] * d);
-  for (int i = 0; i + 1 < L; ++i) opw = std::max(opw, (ll)d * d * Dr[i + 1] * Dl[i] * d * d);
+  for (int i = 0; i + 1 < L; ++i) opw = std::max(opw, wwt_block_elems(Dl[i] * d * d, d * d * Dr[i + 1], sb));
   b += 2 * el(opn) + el(opw);
   ll xs = 1;
   const ll dd = (ll)d * d;
