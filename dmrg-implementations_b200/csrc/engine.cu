@@ -756,14 +756,28 @@ class Engine final : public EngineBase {
     LanczosResult r;
     if (cfg_.precision == 1) {
       // precision form: converge on the split-BF16 operator (FP32-level accuracy), then
-      // refine the Ritz vector with FP64 matvecs; the energy is the FP64 one
+      // refine the Ritz vector with FP64 matvecs; the energy is the FP64 one. With graphs
+      // both solves run device-looped on the staged operator (the split's scratch pointer
+      // is part of the key: it moves when a larger shape grows it).
+      const bool graph = cfg_.graphs && graphs_enabled();
+      const ll dd = (ll)d_ * d_;
+      const T* sL = graph ? stage_op(ln().opL, lenv_[i], (ll)cL * Dl * cL) : lenv_[i];
+      const T* sR = graph ? stage_op(ln().opR, renv_[i + 2], (ll)cR * Dr * cR) : renv_[i + 2];
+      const T* sW = graph ? stage_op(ln().opW, wwt_[i], wwt_block_elems(Dl * (int)dd, (int)dd * Dr, sizeof(T)))
+                          : wwt_[i];
       auto mv_lp = [&](const T* in, T* out, const int* skip) {
-        heff_apply_split(lenv_[i], renv_[i + 2], wwt_[i], in, out, ln().X, ln().Y, cL, cR, d_, Dl, Dr, ln().split, skip, ln().st);
+        heff_apply_split(sL, sR, sW, in, out, ln().X, ln().Y, cL, cR, d_, Dl, Dr, ln().split, skip, ln().st);
       };
+      auto mv_hp = [&](const T* in, T* out, const int* skip) {
+        heff_apply(sL, sR, sW, in, out, ln().X, ln().Y, cL, cR, d_, Dl, Dr, skip, ln().st, sparse ? sW + kk : nullptr);
+      };
+      const LzKey key_lp{4, cL, cR, Dl, Dr, d_, (ll)sL, (ll)sR, (ll)sW, (ll)ln().X, (ll)ln().split.p};
+      const LzKey key_hp{sparse ? 3 : 2, cL, cR, Dl, Dr, d_, (ll)sL, (ll)sR, (ll)sW, (ll)ln().X, (ll)ln().Y};
       LanczosResult lp = lanczos_solve<T>(ln().lw, ln().theta, n, cfg_.krylov_max, std::max(cfg_.lanczos_tol, 1e-9),
-                                          cfg_.max_restarts, cfg_.seed + 7919u * (unsigned)i, mv_lp, ln().st);
+                                          cfg_.max_restarts, cfg_.seed + 7919u * (unsigned)i, mv_lp, ln().st,
+                                          graph ? &key_lp : nullptr);
       r = lanczos_solve<T>(ln().lw, ln().theta, n, std::min(cfg_.krylov_max, 16), cfg_.lanczos_tol, 1,
-                           cfg_.seed + 7919u * (unsigned)i + 1u, mv, ln().st);
+                           cfg_.seed + 7919u * (unsigned)i + 1u, mv_hp, ln().st, graph ? &key_hp : nullptr);
       ss.lowprec_matvecs += lp.matvecs;
       r.matvecs += lp.matvecs;
       r.iters += lp.iters;
