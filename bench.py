@@ -655,7 +655,9 @@ def run_precision_workload(args):
                  "trunc_err_max": z["trunc_err_max"],
                  "rel_dE_vs_fp64": abs(z["energy"] - p["energy"]) / abs(p["energy"]),
                  "what": "plain form with the randomised split (r = k + 10 sketch, shifted CholeskyQR3) "
-                         "where it applies; plain's truncation is the exact density-matrix split"},
+                         "where it applies; the plain form's truncation is the default one: the exact "
+                         "density-matrix split on the first sweep at a cap, the warm-started split "
+                         "(complex CholeskyQR on the real embedding) on sweeps that repeat it"},
         "plain_truncation_ms_per_bond": 1e3 * p["svd_s"] / bonds, "plain_trunc_err_max": p["trunc_err_max"],
         "rel_dE_split_vs_fp64": abs(q["energy"] - p["energy"]) / abs(p["energy"]),
         "max_abs_dn_split_vs_fp64": float(np.max(np.abs(np.asarray(q["n"]) - np.asarray(p["n"])))),

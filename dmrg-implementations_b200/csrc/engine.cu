@@ -28,14 +28,16 @@
 #include "lanczos_driver.cuh"
 #include "rsvd.cuh"
 #include "truncate.cuh"
+#include "truncate_c.cuh"
 
 namespace dmrg2 {
 
 namespace {
-// the warm-started subspace split is built for real data, the density-matrix route and
-// bond caps of at most 512
+// the warm-started subspace split goes with the density-matrix route; its Cholesky factor
+// has order k (real data) or 2k (complex data, on the real embedding), at most CHOL_MAX
 bool warm_capable(const EngineConfig& c) {
-  return !c.complex && c.truncation == 0 && c.svd_method == 0 && !c.single_site && c.chi_max <= CHOL_MAX;
+  return c.truncation == 0 && c.svd_method == 0 && !c.single_site &&
+         (c.complex ? 2 * c.chi_max : c.chi_max) <= CHOL_MAX;
 }
 // the randomised split is an option of two-site sweeps with the density-matrix split
 bool rsvd_capable(const EngineConfig& c) {
@@ -908,8 +910,11 @@ class Engine final : public EngineBase {
   // k-dimensional kept space)
   bool warm_split_applies(int i, int chi, ll m, ll nc) const {
     const int k = dims_[i + 1];
-    return prev_sweep_chi_ == chi && k <= chi && k <= ln().wst.kmax && std::min(m, nc) > k;
+    const int kmax = ST<T>::cplx ? ln().wstc.kmax : ln().wst.kmax;  // 0 where the split is not built
+    return prev_sweep_chi_ == chi && k <= chi && k <= kmax && std::min(m, nc) > k;
   }
+  // |theta|^2 of the last warm split
+  double warm_fro2() const { return ST<T>::cplx ? ln().wstc.h_buf[1] : ln().wst.h_buf[1]; }
 
   // A bond below the cap keeps its dimension only while the weight the warm split
   // discards could all lie below the exact split's threshold (cutoff^2, or the density
@@ -937,21 +942,26 @@ class Engine final : public EngineBase {
     const int cL = dims_[i], cR = dims_[i + 2];
     const ll m = (ll)cL * d_, nc = (ll)d_ * cR;
     DMRG2_CUDA(cudaEventRecord(ln().ev_c, ln().st));
-    if constexpr (std::is_same<T, double>::value) {
+    {
       if (warm_split_applies(i, chi, m, nc)) {
         double te = 0.0;
-        const double* warm = (dir == 'R') ? mps_[i + 1] : mps_[i];
+        const T* warm = (dir == 'R') ? mps_[i + 1] : mps_[i];
         const int k = dims_[i + 1];
         auto split = [&](WstMode mode) {
-          return wst_split(ln().wst, ln().red, ln().theta, (int)m, (int)nc, dir, k, warm, mps_[i], mps_[i + 1], te, ln().st, mode,
-                           cfg_.graphs, ln().ev_d) &&
-                 warm_split_keeps_rank(k, chi, m, nc, te, ln().wst.h_buf[1]);
+          bool done;
+          if constexpr (ST<T>::cplx)
+            done = wst_split_c(ln().wstc, ln().red, ln().theta, (int)m, (int)nc, dir, k, warm, mps_[i], mps_[i + 1], te,
+                               ln().st, mode, ln().ev_d);
+          else
+            done = wst_split(ln().wst, ln().red, ln().theta, (int)m, (int)nc, dir, k, warm, mps_[i], mps_[i + 1], te,
+                             ln().st, mode, cfg_.graphs, ln().ev_d);
+          return done && warm_split_keeps_rank(k, chi, m, nc, te, warm_fro2());
         };
         bool ok = false, short_kept = false;
         if (te_ref_[i] >= 0.0 && short_age_[i] < WARM_SHORT_RUN) {
           if (split(WST_SHORT)) {
             const double te_short = te;
-            short_kept = warm_short_accepts(i, te, ln().wst.h_buf[1]);
+            short_kept = warm_short_accepts(i, te, warm_fro2());
             ok = short_kept;
             if (!short_kept || wst_debug()) {
               ok = split(WST_RESUME);  // the two remaining half-steps on the same theta
@@ -1069,6 +1079,7 @@ class Engine final : public EngineBase {
     LanczosWork<T> lw;
     EigWork<T> ew;
     WstWork wst;     // warm-started subspace split (real data)
+    WstWorkC wstc;   // the same for complex data
     RsvdWork<T> rsvd;  // randomised split (truncation mode 2)
     double* sigma = nullptr;
     int* perm = nullptr;
@@ -1113,8 +1124,13 @@ class Engine final : public EngineBase {
     l.ew.init((int)qmax_, cfg_.chi_max);
     if (primary) bytes_ += l.lw.bytes(nmax_) + l.ew.bytes;
     if (warm_capable(cfg_)) {
-      l.wst.init((int)qmax_, cfg_.chi_max);
-      if (primary) bytes_ += l.wst.bytes;
+      if constexpr (ST<T>::cplx) {
+        l.wstc.init((int)qmax_, cfg_.chi_max);
+        if (primary) bytes_ += l.wstc.bytes;
+      } else {
+        l.wst.init((int)qmax_, cfg_.chi_max);
+        if (primary) bytes_ += l.wst.bytes;
+      }
     }
     if (rsvd_capable(cfg_)) {
       l.rsvd.init((int)qmax_, cfg_.chi_max + RSVD_OVERSAMPLE);
@@ -1146,6 +1162,7 @@ class Engine final : public EngineBase {
     l.lw.release();
     l.ew.release();
     l.wst.release();
+    l.wstc.release();
     l.rsvd.release();
     for (void* p : l.owned) dev_free(p);
     l.owned.clear();
@@ -1211,7 +1228,7 @@ size_t engine_footprint(const EngineConfig& c, const std::vector<int>& Dl, const
          sizeof(double) * kk * kk + sizeof(double) * 5 * nn * kk + sb * nn * kk + sb * 256 * (nn + 1) +
          sizeof(double) * 64 + sizeof(unsigned) * 4 + sizeof(SvdOut);
   }
-  if (warm_capable(c)) b += wst_bytes(qmax, chi);
+  if (warm_capable(c)) b += c.complex ? wstc_bytes(qmax, chi) : wst_bytes(qmax, chi);
   if (rsvd_capable(c))
     b += c.complex ? RsvdWork<zc>::bytes_for(qmax, chi + RSVD_OVERSAMPLE)
                    : RsvdWork<double>::bytes_for(qmax, chi + RSVD_OVERSAMPLE);
