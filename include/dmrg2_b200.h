@@ -78,10 +78,12 @@ typedef struct dmrg2_config {
                          dmrg-gpu driver (gpu-rocm/dmrg-gpu/src/dmrg_gpu_impl.h:1119-1450):
                          bond dimensions stay at those of the initial MPS (or shrink) */
   int truncation;     /* 0 = warm-started subspace split (default): on a sweep that repeats
-                         the previous sweep's bond cap, real data, cap <= 512, a bond keeps
-                         its dimension and the kept space comes from three power steps on theta
-                         from the MPS factor next to it (column-scaled, orthonormalised by
-                         CholeskyQR), exact for that space; the first sweep at a cap, a bond
+                         the previous sweep's bond cap (cap <= 512 for real data, <= 256 for
+                         complex data), a bond keeps its dimension, and the kept space
+                         comes from three power steps on theta starting from the MPS factor
+                         next to it (unit columns, orthonormalised by CholeskyQR; complex
+                         blocks on their real embedding). It is exact for that space. The
+                         first sweep at a cap, a bond
                          below the cap whose discarded weight exceeds the exact split's
                          threshold, or one where CholeskyQR gives up, takes the exact split of
                          svd_method.
