@@ -83,10 +83,9 @@ typedef struct dmrg2_config {
                          comes from three power steps on theta starting from the MPS factor
                          next to it (unit columns, orthonormalised by CholeskyQR; complex
                          blocks on their real embedding). It is exact for that space. The
-                         first sweep at a cap, a bond
-                         below the cap whose discarded weight exceeds the exact split's
-                         threshold, or one where CholeskyQR gives up, takes the exact split of
-                         svd_method.
+                         first sweep at a cap, a bond below the cap whose discarded weight
+                         exceeds the exact split's threshold, or one where CholeskyQR gives
+                         up, takes the exact split of svd_method.
                          1 = the exact split on every bond
                          2 = randomised split (the reference's RSVD option, dmrg2_gpu_impl.h:
                          1178-1266): r = k + 10 random sketch columns on the side that takes
