@@ -1,6 +1,7 @@
 """Timing of single sweep primitives on one GPU, on seeded random operands.
 
     python -m dmrg2.microbench heff --chi 256 [--d 2 --D 5 --complex --reps 50]
+    python -m dmrg2.microbench heffref --chi 256 [--d 2 --D 5 --reps 50]
     python -m dmrg2.microbench svd  --n 512   [--keep 256 --complex --reps 5]
     python -m dmrg2.microbench gemm --m 1024 --n 4096 --k 1024 [--complex --reps 5]
     python -m dmrg2.microbench lanczos --chi 256 [--reps 3]
@@ -9,7 +10,11 @@
 
 heff runs dmrg2_op_heff_noalloc on device-resident operands (torch tensors)
 and reports the device time per matvec (CUDA events) and its algorithmic
-TFLOP/s; svd runs the truncated split through dmrg2_op_svd (host buffers,
+TFLOP/s; heffref times the same three steps (real FP64) as cuBLAS calls through
+torch (a yardstick for the GEMM rate these shapes allow, not part of the library:
+step 1 one GEMM of (cL D) x cL by cL x (d^2 cR), step 2 the D d^2 square mixing
+matrix applied per row block, step 3 (cL d^2) x (D cR) by its transpose of R) and
+the library's matvec beside them; svd runs the truncated split through dmrg2_op_svd (host buffers,
 so the time includes the copies); gemm runs the FP64 DMMA GEMM and the
 split-BF16 tcgen05 GEMM of the precision form on the same operands (host
 buffers) and reports their difference. lanczos runs the
@@ -74,6 +79,51 @@ def bench_heff(chi, d, D, cplx, reps, seed=0):
     fl = heff_flops(chi, chi, d, D, cplx)
     return {"op": "heff", "chi": chi, "d": d, "D": D, "complex": cplx, "us_per_matvec": t * 1e6,
             "gflop_per_matvec": fl / 1e9, "tflops": fl / t / 1e12}
+
+
+def bench_heff_ref(chi, d, D, reps, seed=0):
+    import torch
+
+    dd = d * d
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    L = torch.randn(chi * D, chi, dtype=torch.float64, device="cuda", generator=g)
+    th = torch.randn(chi, dd * chi, dtype=torch.float64, device="cuda", generator=g)
+    W = torch.randn(D * dd, D * dd, dtype=torch.float64, device="cuda", generator=g)
+    R = torch.randn(chi, D * chi, dtype=torch.float64, device="cuda", generator=g)
+
+    def step1():
+        return L @ th                                  # (cL D) x (d^2 cR): X[a][w][.]
+
+    def step2(X):
+        return torch.matmul(W, X.view(chi, D * dd, chi))  # per a: (D d^2) x cR
+
+    def step3(Y):
+        return Y.view(chi * dd, D * chi) @ R.t()       # (cL d^2) x cR
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) * 1e-3 / reps
+
+    X = step1()
+    Y = step2(X).contiguous()
+    t1, t2, t3 = timed(step1), timed(lambda: step2(X)), timed(lambda: step3(Y))
+    f1 = 2.0 * chi * D * chi * dd * chi
+    f2 = 2.0 * chi * (D * dd) ** 2 * chi
+    f3 = 2.0 * chi * dd * D * chi * chi
+    ours = bench_heff(chi, d, D, False, reps)
+    return {"op": "heffref", "chi": chi, "d": d, "D": D,
+            "cublas_us": {"step1": t1 * 1e6, "step2": t2 * 1e6, "step3": t3 * 1e6, "total": (t1 + t2 + t3) * 1e6},
+            "cublas_tflops": {"step1": f1 / t1 / 1e12, "step3": f3 / t3 / 1e12,
+                              "matvec": (f1 + f2 + f3) / (t1 + t2 + t3) / 1e12},
+            "library_us_per_matvec": ours["us_per_matvec"], "library_tflops": ours["tflops"]}
 
 
 def bench_svd(n, keep, cplx, reps, seed=0):
@@ -161,7 +211,7 @@ def bench_warm(n, keep, reps, seed=1):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("op", choices=["heff", "svd", "gemm", "lanczos", "env", "warm"])
+    ap.add_argument("op", choices=["heff", "heffref", "svd", "gemm", "lanczos", "env", "warm"])
     ap.add_argument("--m", type=int, default=1024)
     ap.add_argument("--k", type=int, default=1024)
     ap.add_argument("--chi", type=int, default=256)
@@ -174,6 +224,8 @@ def main():
     a = ap.parse_args()
     if a.op == "heff":
         r = bench_heff(a.chi, a.d, a.D, a.complex, a.reps or 50)
+    elif a.op == "heffref":
+        r = bench_heff_ref(a.chi, a.d, a.D, a.reps or 50)
     elif a.op == "svd":
         n = a.n or 512
         r = bench_svd(n, a.keep or n // 2, a.complex, a.reps or 5)
