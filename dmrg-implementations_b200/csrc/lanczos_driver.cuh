@@ -6,20 +6,19 @@
 //    iterations, so the GPU never idles on the host and at most POLL_LOOK iterations of
 //    no-op launches are issued after convergence;
 //  - device-looped: one CUDA graph per matvec identity (operator shapes and the fixed
-//    buffers it reads and writes) holds a conditional WHILE node whose body is one Krylov
-//    step (matvec, the three vector passes, the normalisation, and a one-thread kernel
-//    that advances the index and ends the loop on convergence or after kmax bodies). The
-//    host launches the graph once per restart and reads the result once; no flags cross
-//    to the host between steps and no no-op steps are issued. A call site opts in by
-//    passing a key; solves run host-driven until a key is met the second time, when the
-//    solve is followed by the capture (graphs.cuh holds the cache).
+//    buffers it reads and writes) holds the whole solve: the start (norms, reset, first
+//    vector), a conditional WHILE node whose body is one Krylov step (matvec, the three
+//    vector passes, the normalisation, and a one-thread kernel that advances the index
+//    and ends the loop on convergence or after kmax bodies), then the Ritz vector and a
+//    copy of the solver state to pinned host memory. The host copies in a seed, launches
+//    the graph once per restart and waits once; no flags cross to the host between steps
+//    and no no-op steps are issued. A call site opts in by passing a key; solves run
+//    host-driven until a key is met the second time, when the solve is followed by the
+//    capture (graphs.cuh holds the cache).
 #pragma once
 
 #include <algorithm>
 #include <array>
-#include <atomic>
-#include <cstdio>
-#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <stdexcept>
