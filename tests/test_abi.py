@@ -65,3 +65,32 @@ def test_cli_binary_built():
     assert cli.exists()
     r = subprocess.run([str(cli), "8", "16", "2", "--bogus"], capture_output=True, text=True)
     assert r.returncode == 1 and "Unknown flag" in r.stderr
+
+
+def _c_layout(struct, fields, tmp_path):
+    """sizeof and field offsets of a header struct, from a C program compiled with gcc."""
+    prog = ["#include <stddef.h>", "#include <stdio.h>", f'#include "{HEADER}"', "int main(void) {",
+            f'  printf("%zu\\n", sizeof({struct}));']
+    prog += [f'  printf("%zu\\n", offsetof({struct}, {f}));' for f in fields]
+    prog += ["  return 0;", "}"]
+    src = tmp_path / f"{struct}.c"
+    exe = tmp_path / f"{struct}.out"
+    src.write_text("\n".join(prog) + "\n")
+    subprocess.run(["gcc", "-std=c11", "-o", str(exe), str(src)], check=True, capture_output=True)
+    vals = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    return vals[0], vals[1:]
+
+
+@pytest.mark.parametrize("name,struct", [("Config", "dmrg2_config"), ("SweepReport", "dmrg2_sweep_report"),
+                                         ("PdmrgOptions", "dmrg2_pdmrg_options"),
+                                         ("ServerConfig", "dmrg2_server_config"), ("Request", "dmrg2_request"),
+                                         ("Result", "dmrg2_result")])
+def test_python_structs_match_the_header_layout(name, struct, tmp_path):
+    """Every ctypes mirror of a header struct has the C compiler's size and field offsets
+    (a field added on one side only, or in another order, fails here without a GPU)."""
+    import dmrg2
+    cls = getattr(dmrg2, name)
+    fields = [f[0] for f in cls._fields_]
+    size, offsets = _c_layout(struct, fields, tmp_path)
+    assert ctypes.sizeof(cls) == size, (name, ctypes.sizeof(cls), size)
+    assert [getattr(cls, f).offset for f in fields] == offsets, name
