@@ -5,7 +5,7 @@
  * reference driver (gpu-rocm/dmrg2-gpu/src/dmrg2_gpu.h:24-203) with plain C
  * functions: integer status codes instead of exceptions, caller-owned host
  * buffers, handle-owned device memory. The op-level entry points replace the
- * reference's numpy two-site primitives (cpu/pdmrg/pdmrg/numerics/*.py,
+ * reference's numpy two-site primitives (the modules of cpu/pdmrg/pdmrg/numerics/ and
  * cpu/pdmrg/pdmrg/environments/update.py) one for one and run them on the GPU.
  *
  * Scalars: DMRG2_F64 = double, DMRG2_C128 = interleaved (re, im) doubles,
