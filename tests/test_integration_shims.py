@@ -32,3 +32,26 @@ template class PDMRGGPU<std::complex<double>>;
     r = subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", f"-I{REPO / 'include'}", str(src)],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_integration_python_snippets_name_real_entry_points():
+    """The Python snippets of INTEGRATION.md use names and signatures the package and the
+    header have: the op-level drop-ins, dmrg2_op_heff's 7 ints and 6 pointers, and the
+    Server's submit / result."""
+    import inspect
+
+    import dmrg2
+    text = (REPO / "INTEGRATION.md").read_text()
+    snippets = "\n".join(re.findall(r"```python\n(.*?)```", text, flags=re.S))
+    imported = re.search(r"from dmrg2 import ([\w, ]+)", snippets).group(1)
+    for name in (n.strip() for n in imported.split(",")):
+        assert hasattr(dmrg2, name), name
+    header = (REPO / "include" / "dmrg2_b200.h").read_text()
+    params = re.search(r"int dmrg2_op_heff\((.*?)\);", header, flags=re.S).group(1).split(",")
+    kinds = ["int" if p.split()[0] == "int" else "ptr" for p in params]
+    assert kinds == ["int"] * 7 + ["ptr"] * 6
+    assert "[ctypes.c_int] * 7 + [ctypes.c_void_p] * 6" in snippets
+    assert "max_active" in inspect.signature(dmrg2.Server.__init__).parameters
+    sub = inspect.signature(dmrg2.Server.submit).parameters
+    assert list(sub)[1:3] == ["mpo", "schedule"] and "mps" in sub
+    assert hasattr(dmrg2.Server, "result")
