@@ -94,3 +94,15 @@ def test_python_structs_match_the_header_layout(name, struct, tmp_path):
     size, offsets = _c_layout(struct, fields, tmp_path)
     assert ctypes.sizeof(cls) == size, (name, ctypes.sizeof(cls), size)
     assert [getattr(cls, f).offset for f in fields] == offsets, name
+
+
+@pytest.mark.parametrize("compiler,std", [("gcc", "-std=c99"), ("gcc", "-std=c11"), ("g++", "-std=c++17")])
+def test_header_compiles_cleanly(compiler, std, tmp_path):
+    """include/dmrg2_b200.h is a plain C header: it compiles as C99, C11 and C++17 with
+    -Wall -Wextra -pedantic -Werror (what a cgo, JNI or C++ caller builds it with)."""
+    src = tmp_path / ("h.c" if compiler == "gcc" else "h.cpp")
+    src.write_text(f'#include "{HEADER}"\nint main(void) {{ return (int)(sizeof(dmrg2_config) + '
+                   f'sizeof(dmrg2_sweep_report) + sizeof(dmrg2_request) + sizeof(dmrg2_result)) == 0; }}\n')
+    r = subprocess.run([compiler, std, "-Wall", "-Wextra", "-pedantic", "-Werror", "-fsyntax-only", str(src)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
