@@ -89,7 +89,7 @@ __device__ inline bool mbar_wait(uint32_t bar, uint32_t parity, int* err, int sp
         : "memory");
     if (ok) return true;
   }
-  atomicExch(err, 1);
+  if (err) atomicExch(err, 1);  // err: the device error flag, or null (no report)
   return false;
 }
 
@@ -238,10 +238,7 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
   if (!ok) {
     // timed out: let the MMAs of the last issued tile finish (bounded) before the
     // accumulator is released; the result is not read
-    if (tid == 0 && kt_issued == kt - 1) {
-      int dummy = 0;
-      (void)mbar_wait(sbar, (uint32_t)(kt_issued & 1), &dummy, UM_SPIN);
-    }
+    if (tid == 0 && kt_issued == kt - 1) (void)mbar_wait(sbar, (uint32_t)(kt_issued & 1), nullptr, UM_SPIN);
     __syncthreads();
   }
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
