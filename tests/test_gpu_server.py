@@ -120,3 +120,16 @@ def test_destroy_with_queued_requests_returns():
     t = time.perf_counter()
     srv.close()  # running solve finishes, queued ones are dropped
     assert time.perf_counter() - t < 120
+
+
+def test_complex_request_footprint_matches_the_engine(alone):
+    """The admission footprint of the complex Josephson request (its engine holds the
+    complex warm-split workspace) equals what an engine of the same configuration
+    allocates."""
+    reqs, ref = alone
+    r = reqs[5]
+    eng = dmrg2.DMRG2GPU(len(r["mpo"]), 3, 24, dtype=np.complex128, krylov_max=30, max_restarts=2, cutoff=1e-14,
+                         tol=1e-300, min_sweeps=100, seed=0)
+    eng.set_mpo(r["mpo"])
+    eng.set_mps(r["mps"])
+    assert ref[5]["footprint_bytes"] == eng.device_bytes()
