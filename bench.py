@@ -349,6 +349,7 @@ def run_ours(args):
     warm_fallbacks = sum(r["warm_fallbacks"] for r in timed)
     eig_fallbacks = sum(r["eig_fallbacks"] for r in timed)
     warm_short = sum(r["warm_short"] for r in timed)
+    device_loops = sum(r["device_loops"] for r in timed)
     mv = sum(r["matvecs"] for r in timed)
     n_sw = len(timed)
 
@@ -405,6 +406,9 @@ def run_ours(args):
                                     "dependent pivots in one 8-CTA cluster; no bandwidth or tensor roofline "
                                     "applies"},
         "matvecs_per_bond": mv_per_bond,
+        "lanczos_graphs": {"device_loops": device_loops, "solves": n_sw * 2 * (L_SITES - 1),
+                           "what": "Lanczos solves of the timed sweeps (restarts counted) that ran as one "
+                                   "cached CUDA graph looping over the Krylov steps on the device"},
         "cpu_baseline": {"value": cpu_value, "unit": "sweeps/s", "cores": cpu_threads(), "kind": "port",
                          "sample": f"the oracle's sweep loop (eigsh, SVD, environment update) run over the first "
                                    f"{cpu_info['bonds_run']} bonds of a chi={CHI} sweep from the warm-up's state "
