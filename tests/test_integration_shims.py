@@ -1,7 +1,7 @@
-"""The C++ shims that INTEGRATION.md gives the reference's callers (DMRG2GPU<Scalar> and
-PDMRGGPU<Scalar> over the C ABI) compile against include/dmrg2_b200.h, for double and
-std::complex<double>: the code blocks are extracted from the document and every member
-is instantiated (compile only; nothing runs, no GPU)."""
+"""The C++ shims that the integration guide gives the reference's callers (DMRG2GPU<Scalar>
+and PDMRGGPU<Scalar> over the C ABI) compile against include/dmrg2_b200.h, for double and
+std::complex<double>: the code blocks are extracted from the guide and every member is
+instantiated (compile only; nothing runs, no GPU)."""
 import re
 import shutil
 import subprocess
@@ -35,9 +35,9 @@ template class PDMRGGPU<std::complex<double>>;
 
 
 def test_integration_python_snippets_name_real_entry_points():
-    """The Python snippets of INTEGRATION.md use names and signatures the package and the
-    header have: the op-level drop-ins, dmrg2_op_heff's 7 ints and 6 pointers, and the
-    Server's submit / result."""
+    """The guide's Python snippets use names and signatures the package and the header
+    have: the op-level drop-ins, dmrg2_op_heff's 7 ints and 6 pointers, and the Server's
+    submit / result."""
     import inspect
 
     import dmrg2
